@@ -1,0 +1,85 @@
+/*
+ * CPU oracle for the molecular PM3 SCF single point of pm3-rs.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library restates, in C++, the reference's CPU algorithm
+ * (pm3-rs 0.2.5: src/params.rs, src/integrals.rs, src/overlap.rs, src/repulsion.rs,
+ * src/hamiltonian.rs, src/fock.rs, src/scf.rs, src/dipole.rs, src/gradient.rs) so that the
+ * GPU library can be checked against it. Only tests/, __graft_entry__.smoke() and the CPU
+ * baseline leg of bench.py load it; the product path never does.
+ *
+ * Units: positions in Bohr, energies in eV (as inside the reference core).
+ */
+#pragma once
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  double charge;
+  int multiplicity;
+  int max_scf;
+  double e_tol;
+  double p_tol;
+  int use_diis;
+  int accelerator;   /* 0 none, 1 CDIIS, 2 A-DIIS -> CDIIS (scf.rs ScfAccelerator) */
+  double adiis_switch;
+  int reference;     /* 0 auto, 1 RHF, 2 UHF (scf.rs Reference) */
+  int guess;         /* 0 auto, 1 SAD, 2 core, 3 symmetry-broken (scf.rs ScfGuess) */
+  int stability;     /* 0 off, 1 auto, 2 always (scf.rs ScfStability) */
+  double level_shift_ev;
+  double damping;
+  int scf_memory_mb;
+} oracle_options;
+
+typedef struct {
+  double electronic_ev, core_ev, total_ev, heat_of_formation_kcal;
+  double dipole_debye[3];
+  double homo_ev, lumo_ev;
+  int has_homo, has_lumo;
+  int iterations, converged, unrestricted, scf_paths_tried;
+  double scf_improvement_ev;
+  int n_occ, n_beta, nao;
+  double last_change;
+} oracle_result;
+
+void oracle_default_options(oracle_options* o);
+
+/* Optional LAPACK/BLAS entry points (Fortran ABI: dsyevd_, dgemm_). NULL restores the
+ * built-in Jacobi eigensolver and loop GEMMs. */
+void oracle_set_lapack(void* dsyevd, void* dgemm);
+
+int oracle_nao(int n_atoms, const int* z);
+
+/* Full single point (run_pm3). charges[n_atoms] required; density[nao*nao], mo_energies[nao],
+ * gradient[3*n_atoms] (eV/Bohr, closed-form Hellmann-Feynman) are optional (NULL = skip).
+ * Returns 0 on success or a status code (1 invalid input, 2 missing element, 4 SCF not
+ * converged, 5 linear algebra); err receives a message. */
+int oracle_single_point(int n_atoms, const int* z, const double* xyz_bohr,
+                        const oracle_options* opt, oracle_result* res, double* charges,
+                        double* density, double* mo_energies, double* gradient, char* err,
+                        int errlen);
+
+/* Derived element constants: out[0..21] = n_orb, uss, upp, zs, zp, betas, betap, gss, gsp,
+ * gpp, gp2, hsp, alpha, core, dd, qq, rho0, rho1, rho2, e_isol, eheat_ev, mass. */
+int oracle_element(int z, double* out);
+
+/* One ordered pair (a heavy-first, dvec = R_b - R_a in Bohr): packed two-electron table
+ * w[pa*pb] (row-major, pa = na(na+1)/2), electron-core blocks e1b[4*4], e2a[4*4] and the
+ * overlap s[4*4] (rows a, cols b). */
+int oracle_pair(int za, int zb, const double* dvec, double* w, double* e1b, double* e2a,
+                double* s, int* na, int* nb);
+
+int oracle_core_hamiltonian(int n_atoms, const int* z, const double* xyz, double* h);
+int oracle_fock(int n_atoms, const int* z, const double* xyz, const double* p_tot,
+                const double* p_spin, double* f);
+double oracle_core_core(int n_atoms, const int* z, const double* xyz);
+/* Hellmann-Feynman gradient at fixed densities (uhf=0: pa/pb ignored). */
+int oracle_fixed_density_gradient(int n_atoms, const int* z, const double* xyz,
+                                  const double* p_tot, const double* pa, const double* pb,
+                                  int uhf, double* grad);
+/* Symmetric eigensolver used by the oracle (ascending; vectors as columns, row-major). */
+int oracle_eigh(int n, const double* a, double* w, double* v);
+
+#ifdef __cplusplus
+}
+#endif
