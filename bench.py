@@ -1,0 +1,354 @@
+"""Benchmark: batched PM3 single points on B200 (pm3gpu) beside the CPU reference path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pm3gpu|reference] [--n-mol M]
+
+Workload (one step): 4096 seeded, neutral, closed-shell C/H/N/O/S organics of 5-60 atoms
+(uniform size), plain FP64 RHF PM3 with the reference's default options (A-DIIS -> CDIIS,
+e_tol 1e-8 eV, p_tol 1e-7, stability search on), every molecule to convergence. The metric is
+converged single points per second over the whole job. Under torchrun every rank solves its
+own 4096 molecules (seed offset by rank): weak scaling, no data-path collective.
+
+`value`: inputs (atom numbers and coordinates) already resident in HBM, CUDA-event time of the
+call on the stream the library launches on. `e2e`: the same through the host C ABI
+(pm3gpu_batch) from pinned host buffers, host<->device copies inside the timed region.
+L2 is flushed (a 512 MiB write) between timed steps, outside the timed region.
+`--impl reference` times the reference algorithm's CPU implementation (the C++ oracle that
+restates pm3-rs, linked to SciPy's OpenBLAS) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "pm3-rs_b200"))
+A2B = 1.0 / 0.529177210903
+METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] if os.path.exists(
+    os.path.join(ROOT, "BASELINE.json")) else "converged SCF/s (batched)"
+WORKLOAD = "organics-4096: seeded C/H/N/O/S trees, 5-60 atoms uniform, RHF PM3 FP64, reference default options"
+
+
+# ------------------------------------------------------------------------- CPU (oracle) side
+def _oracle_worker(args):
+    mols, opts = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    n_conv = 0
+    for z, xyz in mols:
+        try:
+            r = O.single_point(z, xyz, **opts)
+            n_conv += int(r["converged"])
+        except Exception:
+            pass
+    return n_conv
+
+
+def cpu_throughput(mols, cores, steps=1, warmup=0):
+    """Converged molecules/s of the oracle over `mols` on `cores` spawn workers (one thread each)."""
+    import multiprocessing as mp
+
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    os.environ["OMP_NUM_THREADS"] = "1"
+    ctx = mp.get_context("spawn")
+    chunks = [mols[i::cores] for i in range(cores)]
+    with ctx.Pool(cores) as pool:
+        pool.map(_oracle_worker, [(c[:1], {}) for c in chunks])  # start-up outside the timing
+        for _ in range(warmup):
+            pool.map(_oracle_worker, [(c, {}) for c in chunks])
+        rates = []
+        for _ in range(max(steps, 1)):
+            t0 = time.perf_counter()
+            n = sum(pool.map(_oracle_worker, [(c, {}) for c in chunks]))
+            rates.append((n, time.perf_counter() - t0))
+    return rates
+
+
+def molecules(n_mol, seed):
+    from pm3_rs import workloads
+
+    mols = workloads.organic_batch(n_mol, 5, 60, seed=seed)
+    return [(z, xyz * A2B) for z, xyz in mols]
+
+
+# --------------------------------------------------------------------------- GPU helpers
+def gpu_uuid(dev):
+    import torch
+
+    try:
+        return str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        try:
+            for line in open(self.f.name):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                if self.uuid and self.uuid not in parts[0]:
+                    continue
+                rows.append(parts)
+        finally:
+            os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def fp64_gemm_peak(dev):
+    """Measured FP64 dense peak of this GPU: cuBLAS DGEMM 8192^3, best of 3 (TFLOP/s)."""
+    import torch
+
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def scf_flops(nao, n_occ, iters):
+    """Algorithmic FP64 flops of the dense SCF algebra per molecule: per iteration
+    tridiagonalisation 4/3 n^3 + back-transformation 2 n^3 + commutator 2 n^3 + density
+    2 n^2 n_occ (the per-iteration formula of the hot-path measurement plan)."""
+    n = nao.astype(np.float64)
+    return float(np.sum(iters * ((4.0 / 3.0) * n ** 3 + 2.0 * n ** 3 + 2.0 * n ** 3 + 2.0 * n * n * n_occ)))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="pm3gpu", choices=["pm3gpu", "reference"])
+    ap.add_argument("--n-mol", type=int, default=4096)
+    ap.add_argument("--cpu-sample", type=int, default=1024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cores = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        mols = molecules(args.n_mol, seed=1234)[: args.cpu_sample]
+        rates = cpu_throughput(mols, cores, steps=args.steps, warmup=0)
+        n = sum(r[0] for r in rates)
+        t = sum(r[1] for r in rates)
+        value = n / t
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "SCF/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / len(rates),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "molecules_per_step": len(mols), "note": "CPU sample of the workload"},
+            "cpu_baseline": {"value": value, "unit": "SCF/s", "cores": cores, "kind": "port",
+                             "sample": f"first {len(mols)} of the {args.n_mol} molecules per step, one process per core"},
+            "e2e": {"value": value, "unit": "SCF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
+
+    import ctypes
+
+    import torch
+
+    from pm3_rs import _lib, native
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    mols = molecules(args.n_mol, seed=1234 + 7919 * rank)
+    from pm3_rs import workloads
+
+    offs, z, xyz = workloads.pack(mols)
+    n_mol, n_atoms = len(mols), len(z)
+    ctx = _lib.Context(local)
+    lib = ctx.lib
+    stream = torch.cuda.current_stream(dev)
+    lib.pm3gpu_set_stream(ctx.ptr, ctypes.c_void_p(stream.cuda_stream))
+    opts = native.options()
+    results = (_lib.Result * n_mol)()
+    charges = np.zeros(n_atoms)
+    d_z = torch.from_numpy(z).to(dev)
+    d_xyz = torch.from_numpy(np.ascontiguousarray(xyz)).to(dev)
+    d_off = torch.from_numpy(offs).to(dev)
+    h_z = np.ascontiguousarray(z)
+    h_off = np.ascontiguousarray(offs)
+    pz = torch.from_numpy(z).pin_memory()
+    pxyz = torch.from_numpy(np.ascontiguousarray(xyz)).pin_memory()
+    pq = torch.zeros(n_atoms, dtype=torch.float64).pin_memory()
+    I32 = ctypes.POINTER(ctypes.c_int32)
+    D = ctypes.POINTER(ctypes.c_double)
+
+    def run_device():
+        rc = lib.pm3gpu_batch_device_inputs(ctx.ptr, n_mol, ctypes.c_void_p(d_off.data_ptr()),
+                                            ctypes.c_void_p(d_z.data_ptr()), ctypes.c_void_p(d_xyz.data_ptr()),
+                                            h_off.ctypes.data_as(I32), h_z.ctypes.data_as(I32), ctypes.byref(opts),
+                                            results, charges.ctypes.data_as(D), None)
+        if rc != 0:
+            raise RuntimeError(ctx.last_error())
+
+    def run_host():
+        rc = lib.pm3gpu_batch(ctx.ptr, n_mol, h_off.ctypes.data_as(I32), ctypes.cast(pz.data_ptr(), I32),
+                              ctypes.cast(pxyz.data_ptr(), D), ctypes.byref(opts), 0, results,
+                              ctypes.cast(pq.data_ptr(), D), None)
+        if rc != 0:
+            raise RuntimeError(ctx.last_error())
+
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    peak = fp64_gemm_peak(dev)
+
+    xfer = [0, 0]
+
+    def timed(fn, steps):
+        ms, conv, launches, kern_ms, flops = [], 0, 0, 0.0, 0.0
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize(dev)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            torch.cuda.synchronize(dev)
+            ms.append(s.elapsed_time(e))
+            st = np.array([r.status for r in results])
+            conv += int((st == 0).sum())
+            launches += lib.pm3gpu_last_kernel_launches(ctx.ptr)
+            t = (ctypes.c_double * 8)()
+            lib.pm3gpu_last_timings(ctx.ptr, t, 8)
+            kern_ms += t[5]
+            hb, db = ctypes.c_longlong(), ctypes.c_longlong()
+            lib.pm3gpu_last_transfer_bytes(ctx.ptr, ctypes.byref(hb), ctypes.byref(db))
+            xfer[0], xfer[1] = hb.value, db.value
+            nao = np.array([r.nao for r in results])
+            nocc = np.array([r.n_occ for r in results])
+            its = np.array([r.iterations for r in results])
+            flops += scf_flops(nao[st == 0], nocc[st == 0], its[st == 0])
+        return ms, conv, launches, kern_ms, flops
+
+    for _ in range(args.warmup):
+        run_device()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(gpu_uuid(local)) as clk:
+        ms, conv, launches, kern_ms, flops = timed(run_device, args.steps)
+    clocks = clk.summary()
+    for _ in range(max(1, args.warmup // 2)):
+        run_host()
+    if dist:
+        dist.barrier()
+    e_ms, e_conv, _, _, _ = timed(run_host, args.steps)
+    h2d, d2h = xfer
+    tot = sum(ms)
+    e_tot = sum(e_ms)
+    stats = torch.tensor([tot, e_tot, float(conv), float(e_conv)], dtype=torch.float64, device=dev)
+    if dist:
+        t_max = stats[:2].clone()
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        c_sum = stats[2:].clone()
+        dist.all_reduce(c_sum, op=dist.ReduceOp.SUM)
+        tot, e_tot = float(t_max[0]), float(t_max[1])
+        conv, e_conv = int(c_sum[0]), int(c_sum[1])
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    value = conv / (tot * 1e-3)
+    e2e = e_conv / (e_tot * 1e-3)
+    achieved = flops / (kern_ms * 1e-3) / 1e12 if kern_ms > 0 else None
+    line = {
+        "metric": METRIC, "value": value, "unit": "SCF/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tot / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "molecules_per_step_per_gpu": n_mol, "parallelism": f"dp{world}",
+                   "l2": "flushed between steps (512 MiB write)", "converged_fraction": conv / (n_mol * args.steps * world)},
+        "e2e": {"value": e2e, "unit": "SCF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "kernel": "scf_batch_kernel", "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run",
+                     "flops_per_step": flops / args.steps, "kernel_ms_per_step": kern_ms / args.steps},
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        sample = mols[: args.cpu_sample]
+        r = cpu_throughput(sample, os.cpu_count() or 1, steps=1)
+        line["cpu_baseline"] = {"value": r[0][0] / r[0][1], "unit": "SCF/s", "cores": os.cpu_count(),
+                                "kind": "port",
+                                "sample": f"first {len(sample)} of the {n_mol} molecules, one oracle process per core"}
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

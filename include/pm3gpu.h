@@ -1,0 +1,169 @@
+/*
+ * pm3gpu -- B200 (sm_100a) implementation of the molecular PM3 SCF single point of pm3-rs,
+ * behind a plain C ABI (no CUDA or torch types in any signature).
+ *
+ * Reference interfaces each entry point replaces (paths inside the pm3-rs project):
+ *   pm3gpu_single_point      run_pm3(&Molecule, &Pm3Parameters, &Pm3Options) -> Result<Pm3Result>
+ *                            (src/scf.rs:450), and _native.single_point (src/python.rs:253-296)
+ *   pm3gpu_gradient          closed_form_gradient(..) -> GradientResult (src/gradient.rs:201-276),
+ *                            and _native.gradient (src/python.rs:299-357)
+ *   pm3gpu_batch             the same run_pm3 over many independent molecules in one call
+ *                            (no single reference counterpart: the reference loops run_pm3)
+ *   pm3gpu_options           Pm3Options molecular fields (src/scf.rs:160-287)
+ *   pm3gpu_result            Pm3Result scalar fields (src/scf.rs:353-396)
+ *   status codes             Pm3Error variants (src/error.rs:12-47)
+ *
+ * Units: positions in Bohr; energies in eV; dipole in Debye; gradients in eV/Bohr (the
+ * reference's internal units). Matrices are row-major nao x nao doubles.
+ *
+ * Threading: a context owns one CUDA device, one stream and its workspaces; calls on one
+ * context are serialised by an internal lock. Use one context per host thread for concurrency.
+ */
+#ifndef PM3GPU_H
+#define PM3GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (Pm3Error, src/error.rs:12-47). */
+#define PM3GPU_OK 0
+#define PM3GPU_INVALID_INPUT 1      /* Pm3Error::InvalidInput */
+#define PM3GPU_MISSING_ELEMENT 2    /* Pm3Error::MissingElement */
+#define PM3GPU_RESOURCE_LIMIT 3     /* Pm3Error::ResourceLimit */
+#define PM3GPU_SCF_NOT_CONVERGED 4  /* Pm3Error::ScfNotConverged */
+#define PM3GPU_LINALG 5             /* Pm3Error::LinearAlgebra */
+#define PM3GPU_CUDA_ERROR 6         /* device or driver failure */
+#define PM3GPU_UNSUPPORTED 8        /* outside the s/p analytic path (see pm3gpu_supported_element) */
+
+/* Accelerator / reference / guess / stability enums (src/scf.rs:26-158). */
+#define PM3GPU_ACCEL_NONE 0
+#define PM3GPU_ACCEL_CDIIS 1
+#define PM3GPU_ACCEL_ADIIS_CDIIS 2
+#define PM3GPU_REF_AUTO 0
+#define PM3GPU_REF_RHF 1
+#define PM3GPU_REF_UHF 2
+#define PM3GPU_GUESS_AUTO 0
+#define PM3GPU_GUESS_SAD 1
+#define PM3GPU_GUESS_CORE 2
+#define PM3GPU_GUESS_SYMMETRY_BROKEN 3
+#define PM3GPU_STABILITY_OFF 0
+#define PM3GPU_STABILITY_AUTO 1
+#define PM3GPU_STABILITY_ALWAYS 2
+
+typedef struct pm3gpu_ctx pm3gpu_ctx;
+
+/* Pm3Options, molecular-path fields (src/scf.rs:160-287). Defaults: pm3gpu_default_options. */
+typedef struct {
+  double charge;          /* total charge */
+  int multiplicity;       /* 2S+1 */
+  int max_scf;            /* 200 */
+  double e_tol;           /* eV, 1e-8 */
+  double p_tol;           /* RMS density change, 1e-7 */
+  int use_diis;           /* 1 */
+  int accelerator;        /* PM3GPU_ACCEL_* (A-DIIS -> CDIIS) */
+  double adiis_switch;    /* 0.1 */
+  int reference;          /* PM3GPU_REF_* */
+  int guess;              /* PM3GPU_GUESS_* */
+  int stability;          /* PM3GPU_STABILITY_* (auto) */
+  double level_shift_ev;  /* 0 */
+  double damping;         /* 0 */
+  int scf_memory_mb;      /* 512: accelerator-history budget (sets the DIIS depth) */
+} pm3gpu_options;
+
+/* Pm3Result scalar fields (src/scf.rs:353-396). Arrays are returned through caller buffers. */
+typedef struct {
+  int status;                    /* PM3GPU_* for this molecule */
+  int nao;
+  int n_occ, n_beta;
+  double electronic_ev, core_ev, total_ev, heat_of_formation_kcal;
+  double dipole_debye[3];
+  double dipole_magnitude;
+  double homo_ev, lumo_ev;
+  int has_homo, has_lumo;
+  int iterations;
+  int converged;
+  int unrestricted;
+  int scf_paths_tried;
+  double scf_improvement_ev;
+  double last_change;            /* RMS density change of the last iteration */
+} pm3gpu_result;
+
+void pm3gpu_default_options(pm3gpu_options* opts);
+
+/* 1 when element z is inside the s/p analytic path this library implements. */
+int pm3gpu_supported_element(int z);
+
+/* Basis size of a molecule (number of AOs), or -1 on an unsupported element
+ * (sizes the caller's density / MO-energy buffers). Replaces Basis::build (src/basis.rs:39). */
+int pm3gpu_result_sizes(int n_atoms, const int32_t* z, int* nao);
+
+int pm3gpu_context_create(int device, pm3gpu_ctx** out);
+void pm3gpu_context_destroy(pm3gpu_ctx* ctx);
+/* Message of the last failing call on this context (owned by the context). */
+const char* pm3gpu_last_error_message(pm3gpu_ctx* ctx);
+/* Run subsequent work on an existing CUDA stream (cudaStream_t passed as void*); NULL
+ * restores the context's own stream. */
+int pm3gpu_set_stream(pm3gpu_ctx* ctx, void* stream);
+
+/* One molecule: run_pm3. charges[n_atoms] required; density[nao*nao] (total density) and
+ * mo_energies[nao] (alpha MO energies of the last iteration) may be NULL.
+ * Returns the molecule's status (also in result->status). */
+int pm3gpu_single_point(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const double* xyz_bohr,
+                        const pm3gpu_options* opts, pm3gpu_result* result, double* charges,
+                        double* density, double* mo_energies);
+
+/* One molecule: run_pm3 followed by the closed-form Hellmann-Feynman gradient
+ * (gradient[3*n_atoms], eV/Bohr) at the converged density. */
+int pm3gpu_gradient(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const double* xyz_bohr,
+                    const pm3gpu_options* opts, pm3gpu_result* result, double* charges,
+                    double* gradient);
+
+/* Many independent molecules in one persistent launch. Molecule m owns atoms
+ * [atom_offsets[m], atom_offsets[m+1]) of z / xyz_bohr (host arrays). results[n_mol],
+ * charges[total atoms] required; gradients[3 * total atoms] optional (NULL = no gradient).
+ * opts may be one struct (per_molecule_options = 0) or an array of n_mol structs.
+ * Returns PM3GPU_OK when the batch ran (per-molecule outcomes are in results[m].status),
+ * or an error that stopped the whole batch. */
+int pm3gpu_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
+                 const double* xyz_bohr, const pm3gpu_options* opts, int per_molecule_options,
+                 pm3gpu_result* results, double* charges, double* gradients);
+
+/* pm3gpu_batch with z / xyz_bohr / atom_offsets already resident in device memory
+ * (device pointers); results, charges and gradients are host buffers as above. */
+int pm3gpu_batch_device_inputs(pm3gpu_ctx* ctx, int n_mol, const int32_t* d_atom_offsets,
+                               const int32_t* d_z, const double* d_xyz_bohr,
+                               const int32_t* h_atom_offsets, const int32_t* h_z,
+                               const pm3gpu_options* opts, pm3gpu_result* results,
+                               double* charges, double* gradients);
+
+/* H_core of one molecule (hamiltonian.rs:174 build_core): h[nao*nao]; core_ev (optional)
+ * receives the core-core repulsion energy (repulsion.rs:13). */
+int pm3gpu_core_hamiltonian(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const double* xyz_bohr,
+                            double* h, double* core_ev);
+
+/* Fock matrix for given densities (fock.rs:285 build_fock_spin / fock.rs:488 build_fock).
+ * RHF: p_alpha = p_beta = f_beta = NULL, f_alpha = H + J(P) - K(P/2). UHF: f_alpha from
+ * (p_tot, p_alpha), f_beta from (p_tot, p_beta). All nao*nao. */
+int pm3gpu_fock(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const double* xyz_bohr,
+                const double* p_tot, const double* p_alpha, const double* p_beta, double* f_alpha,
+                double* f_beta);
+
+/* Phase timings of the last call (milliseconds, CUDA events): [0] upload, [1] first SCF
+ * pass, [2] stability-search pass, [3] unused, [4] total, [5] time inside the SCF kernels.
+ * Returns the count written. */
+int pm3gpu_last_timings(pm3gpu_ctx* ctx, double* ms, int max_entries);
+
+/* Host-to-device and device-to-host bytes moved by the last call. */
+int pm3gpu_last_transfer_bytes(pm3gpu_ctx* ctx, long long* h2d, long long* d2h);
+
+/* Number of this library's kernels launched by the last call. */
+int pm3gpu_last_kernel_launches(pm3gpu_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PM3GPU_H */

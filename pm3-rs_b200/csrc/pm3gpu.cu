@@ -1,0 +1,830 @@
+// Host side of the pm3gpu C ABI: context, job planning, launches and the stability-search
+// driver of run_pm3 (pm3-rs src/scf.rs:450-848).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pm3gpu.h"
+#include "scf_job.cuh"
+
+using namespace pm3gpu;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, b < 256 ? 256 : b);
+    if (e == cudaSuccess) bytes = b < 256 ? 256 : b;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+constexpr int kMaxDiisDepthHost = 8;
+// scf.rs:309-331
+int diis_depth(int nao, int mats, int budget_mb) {
+  if (budget_mb == 0) return kMaxDiisDepthHost;
+  const size_t per = (size_t)mats * nao * nao * 8;
+  if (per == 0) return kMaxDiisDepthHost;
+  const size_t budget = (size_t)budget_mb * 1024 * 1024;
+  return (int)std::min<size_t>(std::max<size_t>(budget / per, 2), kMaxDiisDepthHost);
+}
+bool diis_depth_fits(int nao, int mats, int budget_mb) {
+  return budget_mb == 0 || 2 * (size_t)mats * nao * nao * 8 <= (size_t)budget_mb * 1024 * 1024;
+}
+
+struct Rung {
+  int guess, accel;
+  double shift, damp;
+  bool unrestricted;
+};
+
+struct MolPlan {
+  int status = 0;
+  std::string msg;
+  int natom = 0, nao = 0, atom0 = 0;
+  int n_alpha = 0, n_beta = 0;
+  bool use_uhf = false, steered = false;
+  const pm3gpu_options* o = nullptr;
+  int first_job = -1;
+  std::vector<int> rung_jobs;
+  std::vector<Rung> rungs;
+};
+
+}  // namespace
+
+struct pm3gpu_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  std::mutex mu;
+  std::string err;
+  ElemDev h_elem[kMaxZ];
+  PairDev h_pairs;
+  DevBuf elem, pairs, z, xyz, jobs, out, charges, dens, grads, eps, work, queue;
+  int sms = 0, smem_optin = 0;
+  double timings[6] = {0, 0, 0, 0, 0, 0};
+  int launches = 0;
+  long long h2d = 0, d2h = 0;  // bytes moved by the last call
+  cudaEvent_t ev[6] = {};
+  cudaEvent_t kev[2] = {};
+};
+
+namespace {
+
+int fail(pm3gpu_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+#define CUDA_TRY(ctx, call)                                                                        \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return fail((ctx), PM3GPU_CUDA_ERROR, std::string(#call ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+bool supported(int z) { return z > 0 && z < kMaxZ && [&] {
+  for (int k = 0; k < PM3_N_RAW_ELEMENTS; ++k)
+    if (PM3_RAW_ELEMENTS[k].z == z) return true;
+  return false;
+}(); }
+
+// Validate one molecule and resolve its electron counts (scf.rs:456-520).
+void plan_molecule(const pm3gpu_ctx* c, const int32_t* z, const double* xyz, int natom, const pm3gpu_options* o,
+                   MolPlan& m) {
+  m.natom = natom;
+  m.o = o;
+  if (natom < 1) {
+    m.status = PM3GPU_INVALID_INPUT;
+    m.msg = "molecule has no atoms";
+    return;
+  }
+  if (o->multiplicity < 1) {
+    m.status = PM3GPU_INVALID_INPUT;
+    m.msg = "multiplicity must be >= 1";
+    return;
+  }
+  int nao = 0;
+  double core = 0.0;
+  for (int a = 0; a < natom; ++a) {
+    const int zz = z[a];
+    if (!supported(zz)) {
+      const bool pm3_has = zz >= 1 && zz <= 107 && zz != 87;
+      m.status = pm3_has ? PM3GPU_UNSUPPORTED : PM3GPU_MISSING_ELEMENT;
+      m.msg = pm3_has ? "Z=" + std::to_string(zz) + " is outside the s/p analytic path of this library"
+                      : "missing PM3 parameter block for Z=" + std::to_string(zz);
+      return;
+    }
+    for (int k = 0; k < 3 && xyz; ++k)
+      if (!std::isfinite(xyz[3 * a + k])) {
+        m.status = PM3GPU_INVALID_INPUT;
+        m.msg = "non-finite coordinate";
+        return;
+      }
+    nao += c->h_elem[zz].norb;
+    core += c->h_elem[zz].core;
+  }
+  m.nao = nao;
+  const double ne = core - o->charge;
+  const long nei = std::lround(ne);
+  if (std::fabs(ne - (double)nei) > 1.0e-6 || nei < 0) {
+    m.status = PM3GPU_INVALID_INPUT;
+    m.msg = "invalid electron count";
+    return;
+  }
+  const long nu = o->multiplicity - 1;
+  if (nei - nu < 0 || (nei - nu) % 2 != 0) {
+    m.status = PM3GPU_INVALID_INPUT;
+    m.msg = "electron count " + std::to_string(nei) + " is incompatible with multiplicity " +
+            std::to_string(o->multiplicity) + " (need same parity)";
+    return;
+  }
+  m.n_alpha = (int)((nei + nu) / 2);
+  m.n_beta = (int)((nei - nu) / 2);
+  if (m.n_alpha > nao) {
+    m.status = PM3GPU_INVALID_INPUT;
+    m.msg = "more electrons than valence orbitals";
+    return;
+  }
+  if (o->reference == PM3GPU_REF_RHF && m.n_alpha != m.n_beta) {
+    m.status = PM3GPU_INVALID_INPUT;
+    m.msg = "RHF requested for an open-shell system; use UHF or Auto";
+    return;
+  }
+  m.use_uhf = o->reference == PM3GPU_REF_UHF || (o->reference == PM3GPU_REF_AUTO && m.n_alpha != m.n_beta);
+  if (nao > kMaxN || natom > kMaxN) {
+    m.status = PM3GPU_UNSUPPORTED;
+    m.msg = "molecule exceeds the per-CTA path (nao <= " + std::to_string(kMaxN) + ")";
+    return;
+  }
+  m.steered = o->level_shift_ev != 0.0 || o->damping != 0.0;
+}
+
+// run_scf of run_pm3 (scf.rs:531-555) as a job: resolve the accelerator the loop will use.
+JobDesc make_job(const MolPlan& m, int guess, int accel, double shift, double damp, bool force_uhf, int extra_flags) {
+  const pm3gpu_options& o = *m.o;
+  JobDesc j{};
+  j.atom0 = m.atom0;
+  j.natom = m.natom;
+  j.nao = m.nao;
+  j.n_alpha = m.n_alpha;
+  j.n_beta = m.n_beta;
+  const bool uhf = m.use_uhf || force_uhf;
+  j.flags = (uhf ? kJobUhf : 0) | extra_flags;
+  j.guess = (guess == PM3GPU_GUESS_CORE) ? 2 : (guess == PM3GPU_GUESS_SYMMETRY_BROKEN ? 3 : 1);
+  const bool use_diis = o.use_diis && accel != PM3GPU_ACCEL_NONE;
+  if (!uhf) {  // scf.rs:1201-1228
+    int a = use_diis ? accel : PM3GPU_ACCEL_NONE;
+    bool keep = a == PM3GPU_ACCEL_ADIIS_CDIIS && diis_depth_fits(m.nao, 3, o.scf_memory_mb);
+    if (a == PM3GPU_ACCEL_ADIIS_CDIIS && !keep) a = PM3GPU_ACCEL_CDIIS;
+    j.accel = a;
+    if (keep) j.flags |= kJobKeepDens;
+    j.depth = diis_depth(m.nao, keep ? 3 : 2, o.scf_memory_mb);
+  } else {  // scf.rs:1369-1374: the unrestricted loop extrapolates only with plain CDIIS
+    j.accel = (use_diis && accel == PM3GPU_ACCEL_CDIIS) ? PM3GPU_ACCEL_CDIIS : PM3GPU_ACCEL_NONE;
+    j.depth = diis_depth(m.nao, 4, o.scf_memory_mb);
+  }
+  j.max_scf = o.max_scf;
+  j.e_tol = o.e_tol;
+  j.p_tol = o.p_tol;
+  j.adiis_switch = o.adiis_switch;
+  j.shift = shift;
+  j.damping = damp;
+  return j;
+}
+
+long long pair_table_doubles(const pm3gpu_ctx* c, const int32_t* z, int natom) {
+  long long s = 0, s2 = 0;
+  for (int a = 0; a < natom; ++a) {
+    const long long p = c->h_elem[z[a]].norb == 4 ? 10 : 1;
+    s += p;
+    s2 += p * p;
+  }
+  return (s * s - s2) / 2;
+}
+
+SmemLayout make_layout(int amax, int nmax, int optin) {
+  SmemLayout L{};
+  L.amax = amax;
+  auto align = [](int b) { return (b + 15) & ~15; };
+  int off = 0;
+  L.off_int = off;
+  off += align((3 * amax + 1 + 16) * 4);
+  L.off_dbl = off;
+  off += align(amax * 8 + (3 * amax + 4 * kMaxDepth * kWarps + 4 * kMaxDepth + 2 * kMaxDepth * kMaxDepth + kMaxDepth + 8) * 8);
+  L.off_eig = off;
+  off += align(7 * kMaxN * 8 + (2 * kMaxN + 2) * 4);
+  L.off_union = off;
+  const int fixed_union = std::max(20 * amax, 2 * 16 * 65);
+  int nsm = nmax;
+  for (; nsm > 0; --nsm) {
+    const int need = std::max(fixed_union, nsm * (nsm + 1) / 2) * 8;
+    if (off + need <= optin) break;
+  }
+  L.nsm = nsm;
+  L.bytes = off + std::max(fixed_union, nsm * (nsm + 1) / 2) * 8;
+  return L;
+}
+
+// One persistent launch over `jobs` (already sorted largest first).
+int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vector<int32_t>& zs, const int32_t* d_z,
+                const double* d_xyz, std::vector<JobOut>& outs, size_t charge_total, size_t dens_total, size_t grad_total,
+                size_t eps_total, std::vector<double>& h_charges, std::vector<double>* h_dens, std::vector<double>* h_grads,
+                std::vector<double>* h_eps, const std::vector<double>* dens_in = nullptr) {
+  const int nj = (int)jobs.size();
+  outs.assign(nj, JobOut{});
+  if (nj == 0) return PM3GPU_OK;
+  int nmax = 1, amax = 1;
+  long long wcap = 1;
+  for (const JobDesc& j : jobs) {
+    nmax = std::max(nmax, j.nao);
+    amax = std::max(amax, j.natom);
+    wcap = std::max(wcap, pair_table_doubles(c, zs.data() + j.atom0, j.natom));
+  }
+  const SmemLayout L = make_layout(amax, nmax, c->smem_optin);
+  CUDA_TRY(c, cudaFuncSetAttribute(scf_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes));
+  int per_sm = 0;
+  CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scf_batch_kernel, kThreads, L.bytes));
+  if (per_sm < 1) return fail(c, PM3GPU_RESOURCE_LIMIT, "SCF kernel does not fit on an SM");
+  const long long slot = slot_doubles(nmax, wcap);
+  size_t free_b = 0, total_b = 0;
+  CUDA_TRY(c, cudaMemGetInfo(&free_b, &total_b));
+  long long grid = std::min<long long>(nj, (long long)c->sms * per_sm);
+  const size_t budget = (size_t)(0.6 * (double)(free_b + c->work.bytes));
+  while (grid > 1 && (size_t)grid * slot * 8 > budget) --grid;
+  if ((size_t)grid * slot * 8 > budget)
+    return fail(c, PM3GPU_RESOURCE_LIMIT, "SCF workspace exceeds device memory");
+  CUDA_TRY(c, c->work.ensure((size_t)grid * slot * 8));
+  CUDA_TRY(c, c->jobs.ensure(sizeof(JobDesc) * nj));
+  CUDA_TRY(c, c->out.ensure(sizeof(JobOut) * nj));
+  CUDA_TRY(c, c->charges.ensure(8 * std::max<size_t>(charge_total, 1)));
+  CUDA_TRY(c, c->dens.ensure(8 * std::max<size_t>(dens_total, 1)));
+  CUDA_TRY(c, c->grads.ensure(8 * std::max<size_t>(grad_total, 1)));
+  CUDA_TRY(c, c->eps.ensure(8 * std::max<size_t>(eps_total, 1)));
+  CUDA_TRY(c, c->queue.ensure(64));
+  CUDA_TRY(c, cudaMemcpyAsync(c->jobs.p, jobs.data(), sizeof(JobDesc) * nj, cudaMemcpyHostToDevice, c->stream));
+  if (dens_in && !dens_in->empty())
+    CUDA_TRY(c, cudaMemcpyAsync(c->dens.p, dens_in->data(), 8 * dens_in->size(), cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->queue.p, 0, 64, c->stream));
+  KernelArgs a{};
+  a.elem = c->elem.as<ElemDev>();
+  a.pairs = c->pairs.as<PairDev>();
+  a.z = d_z;
+  a.xyz = d_xyz;
+  a.jobs = c->jobs.as<JobDesc>();
+  a.njobs = nj;
+  a.out = c->out.as<JobOut>();
+  a.charges = c->charges.as<double>();
+  a.densities = c->dens.as<double>();
+  a.grads = c->grads.as<double>();
+  a.eps = c->eps.as<double>();
+  a.work = c->work.as<double>();
+  a.slot = slot;
+  a.nmax = nmax;
+  a.wcap = wcap;
+  a.queue = c->queue.as<int>();
+  a.sm = L;
+  CUDA_TRY(c, cudaEventRecord(c->kev[0], c->stream));
+  scf_batch_kernel<<<(unsigned)grid, kThreads, L.bytes, c->stream>>>(a);
+  c->launches += 1;
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaEventRecord(c->kev[1], c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(outs.data(), c->out.p, sizeof(JobOut) * nj, cudaMemcpyDeviceToHost, c->stream));
+  h_charges.resize(charge_total);
+  if (charge_total)
+    CUDA_TRY(c, cudaMemcpyAsync(h_charges.data(), c->charges.p, 8 * charge_total, cudaMemcpyDeviceToHost, c->stream));
+  if (h_dens && dens_total) {
+    h_dens->resize(dens_total);
+    CUDA_TRY(c, cudaMemcpyAsync(h_dens->data(), c->dens.p, 8 * dens_total, cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (h_grads && grad_total) {
+    h_grads->resize(grad_total);
+    CUDA_TRY(c, cudaMemcpyAsync(h_grads->data(), c->grads.p, 8 * grad_total, cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (h_eps && eps_total) {
+    h_eps->resize(eps_total);
+    CUDA_TRY(c, cudaMemcpyAsync(h_eps->data(), c->eps.p, 8 * eps_total, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  float kms = 0.f;
+  CUDA_TRY(c, cudaEventElapsedTime(&kms, c->kev[0], c->kev[1]));
+  c->timings[5] += kms;
+  c->h2d += (long long)(sizeof(JobDesc) * nj + (dens_in ? 8 * dens_in->size() : 0));
+  c->d2h += (long long)(sizeof(JobOut) * nj + 8 * charge_total + (h_dens ? 8 * dens_total : 0) +
+                        (h_grads ? 8 * grad_total : 0) + (h_eps ? 8 * eps_total : 0));
+  return PM3GPU_OK;
+}
+
+// Output requests of a whole batch call.
+struct Want {
+  bool density = false, eps = false, grad = false;
+};
+
+// Per-job output bookkeeping: offsets of each job's arrays.
+struct Offsets {
+  size_t charges = 0, dens = 0, grads = 0, eps = 0;
+};
+
+void assign_offsets(JobDesc& j, const Want& w, Offsets& t) {
+  j.charge_off = (long long)t.charges;
+  t.charges += j.natom;
+  if (w.density) {
+    j.flags |= kJobDensity;
+    j.dens_off = (long long)t.dens;
+    t.dens += (size_t)j.nao * j.nao;
+  }
+  if (w.eps) {
+    j.flags |= kJobEps;
+    j.eps_off = (long long)t.eps;
+    t.eps += 2 * (size_t)j.nao;
+  }
+  if (w.grad) {
+    j.flags |= kJobGrad;
+    j.grad_off = (long long)t.grads;
+    t.grads += 3 * (size_t)j.natom;
+  }
+}
+
+struct HostJobResult {
+  JobOut o;
+  const double* charges = nullptr;
+  const double* dens = nullptr;
+  const double* grads = nullptr;
+  const double* eps = nullptr;
+  bool unrestricted = false;
+};
+
+// The whole run_pm3 flow for a batch: first solve, stability search (scf.rs:599-715) as a
+// second persistent launch, selection, and the result epilogue (scf.rs:716-847).
+int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_z, const double* h_xyz,
+              const int32_t* d_z, const double* d_xyz, const pm3gpu_options* opts, int per_mol, const Want& want,
+              pm3gpu_result* results, double* charges, double* gradients, double* density, double* mo_energies) {
+  c->launches = 0;
+  c->timings[5] = 0.0;
+  c->h2d = c->d2h = 0;
+  for (int k = 0; k < 6; ++k) cudaEventRecord(c->ev[k], c->stream);  // placeholders
+  cudaEventRecord(c->ev[0], c->stream);
+  const int total_atoms = h_offs[n_mol];
+  std::vector<int32_t> zs(h_z, h_z + total_atoms);
+  const int32_t* dz = d_z;
+  const double* dxyz = d_xyz;
+  if (!dz) {
+    CUDA_TRY(c, c->z.ensure(4 * (size_t)std::max(total_atoms, 1)));
+    CUDA_TRY(c, c->xyz.ensure(24 * (size_t)std::max(total_atoms, 1)));
+    CUDA_TRY(c, cudaMemcpyAsync(c->z.p, h_z, 4 * (size_t)total_atoms, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->xyz.p, h_xyz, 24 * (size_t)total_atoms, cudaMemcpyHostToDevice, c->stream));
+    dz = c->z.as<int32_t>();
+    dxyz = c->xyz.as<double>();
+    c->h2d += 28LL * total_atoms;
+  }
+  cudaEventRecord(c->ev[1], c->stream);
+  std::vector<MolPlan> plans(n_mol);
+  std::vector<JobDesc> jobs;
+  std::vector<int> job_mol;
+  Offsets t1;
+  for (int m = 0; m < n_mol; ++m) {
+    MolPlan& p = plans[m];
+    p.atom0 = h_offs[m];
+    const int na = h_offs[m + 1] - h_offs[m];
+    if (na < 0) return fail(c, PM3GPU_INVALID_INPUT, "atom_offsets must be non-decreasing");
+    const pm3gpu_options* o = per_mol ? opts + m : opts;
+    plan_molecule(c, h_z + p.atom0, h_xyz ? h_xyz + 3 * (size_t)p.atom0 : nullptr, na, o, p);
+    if (p.status != PM3GPU_OK) continue;
+    JobDesc j = p.steered ? make_job(p, o->guess, o->accelerator, o->level_shift_ev, o->damping, false, 0)
+                          : make_job(p, o->guess, o->accelerator, 0.0, 0.0, false, 0);
+    assign_offsets(j, want, t1);
+    p.first_job = (int)jobs.size();
+    jobs.push_back(j);
+    job_mol.push_back(m);
+  }
+  // largest first (longest-processing-time order) for the work queue
+  std::vector<int> order(jobs.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return jobs[a].nao > jobs[b].nao; });
+  std::vector<JobDesc> sorted(jobs.size());
+  std::vector<int> pos(jobs.size());
+  for (size_t i = 0; i < order.size(); ++i) {
+    sorted[i] = jobs[order[i]];
+    pos[order[i]] = (int)i;
+  }
+  std::vector<JobOut> o1;
+  std::vector<double> q1, d1, g1, e1;
+  int rc = launch_jobs(c, sorted, zs, dz, dxyz, o1, t1.charges, t1.dens, t1.grads, t1.eps, q1, &d1, &g1, &e1);
+  if (rc != PM3GPU_OK) return rc;
+  cudaEventRecord(c->ev[2], c->stream);
+
+  // ---------------------------------------------------------------- stability search
+  std::vector<JobDesc> rjobs;
+  std::vector<int> rmol;
+  Offsets t2;
+  for (int m = 0; m < n_mol; ++m) {
+    MolPlan& p = plans[m];
+    if (p.status != PM3GPU_OK) continue;
+    const pm3gpu_options& o = *p.o;
+    const JobOut& f = o1[pos[p.first_job]];
+    bool search = false;
+    if (o.stability == PM3GPU_STABILITY_ALWAYS) search = !p.steered;
+    else if (o.stability == PM3GPU_STABILITY_AUTO) search = !p.steered && f.gap < 6.0;
+    if (!search) continue;
+    const int primary = o.guess == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_CORE : PM3GPU_GUESS_SAD;
+    const int other = primary == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_SAD : PM3GPU_GUESS_CORE;
+    const bool closed = !p.use_uhf;
+    const Rung all[7] = {{primary, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                         {other, o.accelerator, 0.0, 0.0, false},
+                         {other, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                         {PM3GPU_GUESS_SYMMETRY_BROKEN, o.accelerator, 0.0, 0.0, false},
+                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, -2.0, 0.0, closed},
+                         {primary, PM3GPU_ACCEL_CDIIS, 0.0, 0.85, closed}};
+    for (const Rung& r : all) {
+      if (r.unrestricted != closed) continue;  // scf.rs:676-678
+      JobDesc j = make_job(p, r.guess, r.accel, r.shift, r.damp, r.unrestricted, 0);
+      assign_offsets(j, want, t2);
+      p.rung_jobs.push_back((int)rjobs.size());
+      p.rungs.push_back(r);
+      rjobs.push_back(j);
+      rmol.push_back(m);
+    }
+  }
+  std::vector<int> rorder(rjobs.size()), rpos(rjobs.size());
+  for (size_t i = 0; i < rorder.size(); ++i) rorder[i] = (int)i;
+  std::stable_sort(rorder.begin(), rorder.end(), [&](int a, int b) { return rjobs[a].nao > rjobs[b].nao; });
+  std::vector<JobDesc> rsorted(rjobs.size());
+  for (size_t i = 0; i < rorder.size(); ++i) {
+    rsorted[i] = rjobs[rorder[i]];
+    rpos[rorder[i]] = (int)i;
+  }
+  std::vector<JobOut> o2;
+  std::vector<double> q2, d2, g2, e2;
+  if (!rjobs.empty()) {
+    rc = launch_jobs(c, rsorted, zs, dz, dxyz, o2, t2.charges, t2.dens, t2.grads, t2.eps, q2, &d2, &g2, &e2);
+    if (rc != PM3GPU_OK) return rc;
+  }
+  cudaEventRecord(c->ev[3], c->stream);
+
+  // ---------------------------------------------------------------- selection + epilogue
+  for (int m = 0; m < n_mol; ++m) {
+    MolPlan& p = plans[m];
+    pm3gpu_result& R = results[m];
+    std::memset(&R, 0, sizeof(R));
+    R.status = p.status;
+    R.nao = p.nao;
+    const int atom0 = h_offs[m];
+    if (p.status != PM3GPU_OK) {
+      if (!c->err.size()) c->err = p.msg;
+      if (n_mol == 1) c->err = p.msg;
+      continue;
+    }
+    const JobDesc& fj = jobs[p.first_job];
+    HostJobResult st;
+    st.o = o1[pos[p.first_job]];
+    st.unrestricted = (fj.flags & kJobUhf) != 0;
+    st.charges = q1.data() + fj.charge_off;
+    if (want.density) st.dens = d1.data() + fj.dens_off;
+    if (want.grad) st.grads = g1.data() + fj.grad_off;
+    if (want.eps) st.eps = e1.data() + fj.eps_off;
+    const double first_ev = st.o.electronic;
+    int paths = 1;
+    for (size_t r = 0; r < p.rung_jobs.size(); ++r) {
+      ++paths;
+      const JobDesc& rj = rjobs[p.rung_jobs[r]];
+      HostJobResult cand;
+      cand.o = o2[rpos[p.rung_jobs[r]]];
+      cand.unrestricted = (rj.flags & kJobUhf) != 0;
+      if (!cand.o.converged) continue;
+      if (p.rungs[r].unrestricted) {  // a spin-pure unrestricted closed shell is a restricted state
+        if (!(cand.o.spin_max < 1.0e-8)) continue;
+        cand.unrestricted = false;
+        cand.o.homo = cand.o.homo_a;
+        cand.o.lumo = cand.o.lumo_a;
+        cand.o.has_homo = cand.o.has_homo_a;
+        cand.o.has_lumo = cand.o.has_lumo_a;
+      }
+      cand.charges = q2.data() + rj.charge_off;
+      if (want.density) cand.dens = d2.data() + rj.dens_off;
+      if (want.grad) cand.grads = g2.data() + rj.grad_off;
+      if (want.eps) cand.eps = e2.data() + rj.eps_off;
+      if (!st.o.converged || cand.o.electronic < st.o.electronic - 1.0e-6) st = cand;
+    }
+    double e_isol = 0.0, eheat = 0.0;
+    for (int a = 0; a < p.natom; ++a) {
+      e_isol += c->h_elem[h_z[atom0 + a]].e_isol;
+      eheat += c->h_elem[h_z[atom0 + a]].eheat_ev;
+    }
+    R.n_occ = p.n_alpha;
+    R.n_beta = st.unrestricted ? p.n_beta : p.n_alpha;
+    R.electronic_ev = st.o.electronic;
+    R.core_ev = st.o.core;
+    R.total_ev = st.o.electronic + st.o.core;
+    R.heat_of_formation_kcal = (R.total_ev - e_isol + eheat) * kEvToKcal;
+    R.iterations = st.o.iterations;
+    R.converged = st.o.converged;
+    R.unrestricted = st.unrestricted ? 1 : 0;
+    R.scf_paths_tried = paths;
+    R.scf_improvement_ev = std::max(first_ev - st.o.electronic, 0.0);
+    R.last_change = st.o.last_change;
+    R.homo_ev = st.o.homo;
+    R.lumo_ev = st.o.lumo;
+    R.has_homo = st.o.has_homo;
+    R.has_lumo = st.o.has_lumo;
+    for (int k = 0; k < 3; ++k) R.dipole_debye[k] = st.o.dipole[k];
+    R.dipole_magnitude = std::sqrt(R.dipole_debye[0] * R.dipole_debye[0] + R.dipole_debye[1] * R.dipole_debye[1] +
+                                   R.dipole_debye[2] * R.dipole_debye[2]);
+    if (!st.o.converged) {
+      R.status = PM3GPU_SCF_NOT_CONVERGED;
+      char msg[160];
+      std::snprintf(msg, sizeof msg, "PM3 SCF did not converge after %d iterations (error=%.3e)", st.o.iterations,
+                    st.o.last_change);
+      c->err = msg;
+    }
+    if (charges) std::memcpy(charges + atom0, st.charges, 8 * (size_t)p.natom);
+    if (gradients && st.grads) std::memcpy(gradients + 3 * (size_t)atom0, st.grads, 24 * (size_t)p.natom);
+    if (density && st.dens) std::memcpy(density, st.dens, 8 * (size_t)p.nao * p.nao);
+    if (mo_energies && st.eps) std::memcpy(mo_energies, st.eps, 8 * (size_t)p.nao);
+  }
+  cudaEventRecord(c->ev[4], c->stream);
+  cudaEventSynchronize(c->ev[4]);
+  float ms[4];
+  cudaEventElapsedTime(&ms[0], c->ev[0], c->ev[1]);
+  cudaEventElapsedTime(&ms[1], c->ev[1], c->ev[2]);
+  cudaEventElapsedTime(&ms[2], c->ev[2], c->ev[3]);
+  cudaEventElapsedTime(&ms[3], c->ev[0], c->ev[4]);
+  c->timings[0] = ms[0];
+  c->timings[1] = ms[1];
+  c->timings[2] = ms[2];
+  c->timings[3] = 0.0;
+  c->timings[4] = ms[3];
+  return PM3GPU_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+void pm3gpu_default_options(pm3gpu_options* o) {  // scf.rs:259-287
+  o->charge = 0.0;
+  o->multiplicity = 1;
+  o->max_scf = 200;
+  o->e_tol = 1.0e-8;
+  o->p_tol = 1.0e-7;
+  o->use_diis = 1;
+  o->accelerator = PM3GPU_ACCEL_ADIIS_CDIIS;
+  o->adiis_switch = 0.1;
+  o->reference = PM3GPU_REF_AUTO;
+  o->guess = PM3GPU_GUESS_AUTO;
+  o->stability = PM3GPU_STABILITY_AUTO;
+  o->level_shift_ev = 0.0;
+  o->damping = 0.0;
+  o->scf_memory_mb = 512;
+}
+
+int pm3gpu_supported_element(int z) { return supported(z) ? 1 : 0; }
+
+int pm3gpu_result_sizes(int n_atoms, const int32_t* z, int* nao) {
+  ElemDev el[kMaxZ];
+  derive_elements(el, nullptr);
+  int s = 0;
+  for (int a = 0; a < n_atoms; ++a) {
+    if (!supported(z[a])) {
+      if (nao) *nao = -1;
+      return -1;
+    }
+    s += el[z[a]].norb;
+  }
+  if (nao) *nao = s;
+  return s;
+}
+
+int pm3gpu_context_create(int device, pm3gpu_ctx** out) {
+  if (!out) return PM3GPU_INVALID_INPUT;
+  *out = nullptr;
+  pm3gpu_ctx* c = new pm3gpu_ctx();
+  c->device = device;
+  auto bail = [&](cudaError_t e) {
+    delete c;
+    (void)e;
+    return PM3GPU_CUDA_ERROR;
+  };
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return bail(e);
+  if ((e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
+  c->stream = c->own;
+  for (int k = 0; k < 6; ++k)
+    if ((e = cudaEventCreate(&c->ev[k])) != cudaSuccess) return bail(e);
+  for (int k = 0; k < 2; ++k)
+    if ((e = cudaEventCreate(&c->kev[k])) != cudaSuccess) return bail(e);
+  cudaDeviceProp prop;
+  if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) return bail(e);
+  c->sms = prop.multiProcessorCount;
+  c->smem_optin = (int)prop.sharedMemPerBlockOptin;
+  derive_elements(c->h_elem, &c->h_pairs);
+  if ((e = c->elem.ensure(sizeof(c->h_elem))) != cudaSuccess) return bail(e);
+  if ((e = c->pairs.ensure(sizeof(PairDev))) != cudaSuccess) return bail(e);
+  if ((e = cudaMemcpy(c->elem.p, c->h_elem, sizeof(c->h_elem), cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e);
+  if ((e = cudaMemcpy(c->pairs.p, &c->h_pairs, sizeof(PairDev), cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e);
+  *out = c;
+  return PM3GPU_OK;
+}
+
+void pm3gpu_context_destroy(pm3gpu_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (DevBuf* b : {&c->elem, &c->pairs, &c->z, &c->xyz, &c->jobs, &c->out, &c->charges, &c->dens, &c->grads, &c->eps,
+                    &c->work, &c->queue})
+    b->release();
+  for (int k = 0; k < 6; ++k)
+    if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+  for (int k = 0; k < 2; ++k)
+    if (c->kev[k]) cudaEventDestroy(c->kev[k]);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+}
+
+const char* pm3gpu_last_error_message(pm3gpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int pm3gpu_set_stream(pm3gpu_ctx* c, void* stream) {
+  if (!c) return PM3GPU_INVALID_INPUT;
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : c->own;
+  return PM3GPU_OK;
+}
+
+int pm3gpu_single_point(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz, const pm3gpu_options* opts,
+                        pm3gpu_result* result, double* charges, double* density, double* mo_energies) {
+  if (!c || !z || !xyz || !result || !charges) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->err.clear();
+  pm3gpu_options d;
+  pm3gpu_default_options(&d);
+  const int32_t offs[2] = {0, n_atoms};
+  Want w;
+  w.density = density != nullptr;
+  w.eps = mo_energies != nullptr;
+  int rc = run_batch(c, 1, offs, z, xyz, nullptr, nullptr, opts ? opts : &d, 0, w, result, charges, nullptr, density,
+                     mo_energies);
+  if (rc != PM3GPU_OK) {
+    result->status = rc;
+    return rc;
+  }
+  return result->status;
+}
+
+int pm3gpu_gradient(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz, const pm3gpu_options* opts,
+                    pm3gpu_result* result, double* charges, double* gradient) {
+  if (!c || !z || !xyz || !result || !charges || !gradient) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->err.clear();
+  pm3gpu_options d;
+  pm3gpu_default_options(&d);
+  const int32_t offs[2] = {0, n_atoms};
+  Want w;
+  w.grad = true;
+  int rc = run_batch(c, 1, offs, z, xyz, nullptr, nullptr, opts ? opts : &d, 0, w, result, charges, gradient, nullptr,
+                     nullptr);
+  if (rc != PM3GPU_OK) {
+    result->status = rc;
+    return rc;
+  }
+  return result->status;
+}
+
+int pm3gpu_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t* z, const double* xyz,
+                 const pm3gpu_options* opts, int per_mol, pm3gpu_result* results, double* charges, double* gradients) {
+  if (!c || n_mol < 0 || !offs || !z || !xyz || !results || !charges) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->err.clear();
+  pm3gpu_options d;
+  pm3gpu_default_options(&d);
+  Want w;
+  w.grad = gradients != nullptr;
+  return run_batch(c, n_mol, offs, z, xyz, nullptr, nullptr, opts ? opts : &d, opts ? per_mol : 0, w, results, charges,
+                   gradients, nullptr, nullptr);
+}
+
+int pm3gpu_batch_device_inputs(pm3gpu_ctx* c, int n_mol, const int32_t* d_offs, const int32_t* d_z, const double* d_xyz,
+                               const int32_t* h_offs, const int32_t* h_z, const pm3gpu_options* opts,
+                               pm3gpu_result* results, double* charges, double* gradients) {
+  if (!c || n_mol < 0 || !d_z || !d_xyz || !h_offs || !h_z || !results || !charges)
+    return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  (void)d_offs;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->err.clear();
+  pm3gpu_options d;
+  pm3gpu_default_options(&d);
+  Want w;
+  w.grad = gradients != nullptr;
+  return run_batch(c, n_mol, h_offs, h_z, nullptr, d_z, d_xyz, opts ? opts : &d, 0, w, results, charges, gradients,
+                   nullptr, nullptr);
+}
+
+// build_core (hamiltonian.rs:174-344) and build_fock_spin (fock.rs:285-332) on the GPU, for
+// element-by-element checks of the pair-integral and Fock kernels.
+static int single_stage(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz, int flag, int uhf,
+                        std::vector<double>& io, double* core_ev) {
+  if (n_atoms < 1 || n_atoms > kMaxN) return fail(c, PM3GPU_INVALID_INPUT, "atom count outside 1..256");
+  int nao = 0;
+  for (int a = 0; a < n_atoms; ++a) {
+    if (!supported(z[a])) return fail(c, PM3GPU_UNSUPPORTED, "unsupported element Z=" + std::to_string(z[a]));
+    for (int k = 0; k < 3; ++k)
+      if (!std::isfinite(xyz[3 * a + k])) return fail(c, PM3GPU_INVALID_INPUT, "non-finite coordinate");
+    nao += c->h_elem[z[a]].norb;
+  }
+  if (nao > kMaxN) return fail(c, PM3GPU_UNSUPPORTED, "basis exceeds the per-CTA path");
+  JobDesc j{};
+  j.natom = n_atoms;
+  j.nao = nao;
+  j.flags = flag | (uhf ? kJobUhf : 0);
+  j.guess = 1;
+  j.depth = 2;
+  j.dens_off = 0;
+  std::vector<int32_t> zs(z, z + n_atoms);
+  CUDA_TRY(c, c->z.ensure(4 * (size_t)n_atoms));
+  CUDA_TRY(c, c->xyz.ensure(24 * (size_t)n_atoms));
+  CUDA_TRY(c, cudaMemcpyAsync(c->z.p, z, 4 * (size_t)n_atoms, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->xyz.p, xyz, 24 * (size_t)n_atoms, cudaMemcpyHostToDevice, c->stream));
+  std::vector<JobOut> outs;
+  std::vector<double> q, dens;
+  c->launches = 0;
+  int rc = launch_jobs(c, {j}, zs, c->z.as<int32_t>(), c->xyz.as<double>(), outs, (size_t)n_atoms, io.size(), 0, 0, q,
+                       &dens, nullptr, nullptr, &io);
+  if (rc != PM3GPU_OK) return rc;
+  io.swap(dens);
+  if (core_ev) *core_ev = outs[0].core;
+  return PM3GPU_OK;
+}
+
+int pm3gpu_core_hamiltonian(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz, double* h, double* core_ev) {
+  if (!c || !z || !xyz || !h) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->err.clear();
+  int nao = 0;
+  if (pm3gpu_result_sizes(n_atoms, z, &nao) < 0) return fail(c, PM3GPU_UNSUPPORTED, "unsupported element");
+  std::vector<double> io((size_t)nao * nao, 0.0);
+  int rc = single_stage(c, n_atoms, z, xyz, kJobCoreOnly, 0, io, core_ev);
+  if (rc != PM3GPU_OK) return rc;
+  std::memcpy(h, io.data(), 8 * (size_t)nao * nao);
+  return PM3GPU_OK;
+}
+
+int pm3gpu_fock(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz, const double* p_tot,
+                const double* p_alpha, const double* p_beta, double* f_alpha, double* f_beta) {
+  if (!c || !z || !xyz || !p_tot || !f_alpha) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  const int uhf = (p_alpha && p_beta && f_beta) ? 1 : 0;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->err.clear();
+  int nao = 0;
+  if (pm3gpu_result_sizes(n_atoms, z, &nao) < 0) return fail(c, PM3GPU_UNSUPPORTED, "unsupported element");
+  const size_t nn = (size_t)nao * nao;
+  std::vector<double> io(5 * nn, 0.0);
+  std::memcpy(io.data(), p_tot, 8 * nn);
+  if (uhf) {
+    std::memcpy(io.data() + nn, p_alpha, 8 * nn);
+    std::memcpy(io.data() + 2 * nn, p_beta, 8 * nn);
+  }
+  int rc = single_stage(c, n_atoms, z, xyz, kJobFockOnly, uhf, io, nullptr);
+  if (rc != PM3GPU_OK) return rc;
+  std::memcpy(f_alpha, io.data() + 3 * nn, 8 * nn);
+  if (uhf) std::memcpy(f_beta, io.data() + 4 * nn, 8 * nn);
+  return PM3GPU_OK;
+}
+
+int pm3gpu_last_timings(pm3gpu_ctx* c, double* ms, int max_entries) {
+  if (!c || !ms) return 0;
+  const int k = std::min(max_entries, 6);
+  for (int i = 0; i < k; ++i) ms[i] = c->timings[i];
+  return k;
+}
+
+int pm3gpu_last_kernel_launches(pm3gpu_ctx* c) { return c ? c->launches : 0; }
+
+int pm3gpu_last_transfer_bytes(pm3gpu_ctx* c, long long* h2d, long long* d2h) {
+  if (!c) return PM3GPU_INVALID_INPUT;
+  if (h2d) *h2d = c->h2d;
+  if (d2h) *d2h = c->d2h;
+  return PM3GPU_OK;
+}
+
+}  // extern "C"

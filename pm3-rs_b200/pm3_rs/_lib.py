@@ -1,0 +1,149 @@
+"""ctypes binding of libpm3gpu.so (the C ABI declared in include/pm3gpu.h)."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpm3gpu.so")
+
+OK = 0
+INVALID_INPUT = 1
+MISSING_ELEMENT = 2
+RESOURCE_LIMIT = 3
+SCF_NOT_CONVERGED = 4
+LINALG = 5
+CUDA_ERROR = 6
+UNSUPPORTED = 8
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("charge", ctypes.c_double),
+        ("multiplicity", ctypes.c_int),
+        ("max_scf", ctypes.c_int),
+        ("e_tol", ctypes.c_double),
+        ("p_tol", ctypes.c_double),
+        ("use_diis", ctypes.c_int),
+        ("accelerator", ctypes.c_int),
+        ("adiis_switch", ctypes.c_double),
+        ("reference", ctypes.c_int),
+        ("guess", ctypes.c_int),
+        ("stability", ctypes.c_int),
+        ("level_shift_ev", ctypes.c_double),
+        ("damping", ctypes.c_double),
+        ("scf_memory_mb", ctypes.c_int),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int),
+        ("nao", ctypes.c_int),
+        ("n_occ", ctypes.c_int),
+        ("n_beta", ctypes.c_int),
+        ("electronic_ev", ctypes.c_double),
+        ("core_ev", ctypes.c_double),
+        ("total_ev", ctypes.c_double),
+        ("heat_of_formation_kcal", ctypes.c_double),
+        ("dipole_debye", ctypes.c_double * 3),
+        ("dipole_magnitude", ctypes.c_double),
+        ("homo_ev", ctypes.c_double),
+        ("lumo_ev", ctypes.c_double),
+        ("has_homo", ctypes.c_int),
+        ("has_lumo", ctypes.c_int),
+        ("iterations", ctypes.c_int),
+        ("converged", ctypes.c_int),
+        ("unrestricted", ctypes.c_int),
+        ("scf_paths_tried", ctypes.c_int),
+        ("scf_improvement_ev", ctypes.c_double),
+        ("last_change", ctypes.c_double),
+    ]
+
+
+# Every symbol include/pm3gpu.h declares.
+EXPORTS = [
+    "pm3gpu_default_options", "pm3gpu_supported_element", "pm3gpu_result_sizes",
+    "pm3gpu_context_create", "pm3gpu_context_destroy", "pm3gpu_last_error_message",
+    "pm3gpu_set_stream", "pm3gpu_single_point", "pm3gpu_gradient", "pm3gpu_batch",
+    "pm3gpu_batch_device_inputs", "pm3gpu_core_hamiltonian", "pm3gpu_fock", "pm3gpu_last_timings",
+    "pm3gpu_last_kernel_launches", "pm3gpu_last_transfer_bytes",
+]
+
+_lib = None
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int32)
+
+
+def load() -> ctypes.CDLL:
+    """Load the CUDA library; raises when it has not been built (there is no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python pm3-rs_b200/build.py` "
+            "(pm3_rs runs only on the GPU library; there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.pm3gpu_default_options.argtypes = [ctypes.POINTER(Options)]
+    L.pm3gpu_default_options.restype = None
+    L.pm3gpu_supported_element.argtypes = [ctypes.c_int]
+    L.pm3gpu_result_sizes.argtypes = [ctypes.c_int, _I, ctypes.POINTER(ctypes.c_int)]
+    L.pm3gpu_context_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.pm3gpu_context_destroy.argtypes = [ctypes.c_void_p]
+    L.pm3gpu_context_destroy.restype = None
+    L.pm3gpu_last_error_message.argtypes = [ctypes.c_void_p]
+    L.pm3gpu_last_error_message.restype = ctypes.c_char_p
+    L.pm3gpu_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.pm3gpu_single_point.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, ctypes.POINTER(Options),
+                                      ctypes.POINTER(Result), _D, _D, _D]
+    L.pm3gpu_gradient.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, ctypes.POINTER(Options),
+                                  ctypes.POINTER(Result), _D, _D]
+    L.pm3gpu_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, ctypes.POINTER(Options), ctypes.c_int,
+                               ctypes.POINTER(Result), _D, _D]
+    L.pm3gpu_batch_device_inputs.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, _I, _I, ctypes.POINTER(Options),
+                                             ctypes.POINTER(Result), _D, _D]
+    L.pm3gpu_core_hamiltonian.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, _D, _D]
+    L.pm3gpu_fock.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, _D, _D, _D, _D, _D]
+    L.pm3gpu_last_timings.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
+    L.pm3gpu_last_kernel_launches.argtypes = [ctypes.c_void_p]
+    L.pm3gpu_last_transfer_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                                             ctypes.POINTER(ctypes.c_longlong)]
+    _lib = L
+    return L
+
+
+class Context:
+    """One CUDA device + stream + workspaces (pm3gpu_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        self.ptr = ctypes.c_void_p()
+        rc = self.lib.pm3gpu_context_create(device, ctypes.byref(self.ptr))
+        if rc != OK:
+            raise RuntimeError(f"pm3gpu_context_create failed with status {rc} (is a CUDA device visible?)")
+
+    def last_error(self) -> str:
+        return self.lib.pm3gpu_last_error_message(self.ptr).decode()
+
+    def close(self):
+        if self.ptr:
+            self.lib.pm3gpu_context_destroy(self.ptr)
+            self.ptr = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default = {}
+
+
+def default_context(device: int = 0) -> Context:
+    ctx = _default.get(device)
+    if ctx is None:
+        ctx = _default[device] = Context(device)
+    return ctx

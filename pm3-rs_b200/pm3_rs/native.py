@@ -1,0 +1,214 @@
+"""PM3 API of pm3-rs (atomic units out, Angstrom in), running on the pm3gpu CUDA library.
+
+Drop-in for ``pm3_rs.native`` of pm3-rs (python/pm3_rs/native.py:41-140 and
+src/python.rs:253-357): same functions, signatures, dictionary keys and units, and the same
+``ValueError`` on any failure (src/python.rs:22-24). ``method`` is limited to plain ``"pm3"``
+and ``field`` to ``None``: the post-SCF corrections and external fields are outside this
+library's path, and asking for them raises rather than being silently ignored.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+
+PM3_EV = 27.211386245988
+PM3_A0 = 0.529177210903
+EV_TO_HARTREE = 1.0 / PM3_EV
+ANGSTROM_TO_BOHR = 1.0 / PM3_A0
+
+_REFERENCES = {"auto": 0, "": 0, "rhf": 1, "r": 1, "restricted": 1, "uhf": 2, "u": 2, "unrestricted": 2}
+
+
+def _parse_reference(reference: str) -> int:
+    key = str(reference).lower()
+    if key not in _REFERENCES:
+        raise ValueError(f"reference must be 'auto', 'rhf' or 'uhf' (got {reference!r})")
+    return _REFERENCES[key]
+
+
+def _check_method(method: str, field) -> None:
+    m = str(method).strip().lower().replace(" ", "-").replace("_", "-")
+    if m not in ("", "pm3"):
+        raise ValueError(f"method {method!r} is not available here: only plain 'pm3' runs on pm3gpu")
+    if field is not None:
+        raise ValueError("an external field is not available on pm3gpu")
+
+
+def _as_arrays(numbers, positions):
+    z = np.ascontiguousarray(np.asarray(numbers).reshape(-1), dtype=np.int32)
+    xyz = np.asarray(positions, dtype=np.float64)
+    if xyz.size != 3 * len(z):
+        raise ValueError("numbers and positions length mismatch")
+    return z, np.ascontiguousarray(xyz.reshape(len(z), 3) * ANGSTROM_TO_BOHR)
+
+
+def options(charge: float = 0.0, multiplicity: int = 1, reference: str = "auto", **overrides) -> _lib.Options:
+    """Pm3Options with the reference's defaults (src/scf.rs:259-287) and the given overrides."""
+    lib = _lib.load()
+    o = _lib.Options()
+    lib.pm3gpu_default_options(ctypes.byref(o))
+    o.charge = float(charge)
+    o.multiplicity = int(multiplicity)
+    o.reference = _parse_reference(reference)
+    for k, v in overrides.items():
+        setattr(o, k, v)
+    return o
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def run(z, xyz_bohr, opts: _lib.Options, want_density=False, want_mo_energies=False, want_gradient=False,
+        device: int = 0) -> dict:
+    """run_pm3 on one molecule (Bohr in, eV out). Raises ValueError on any non-OK status."""
+    ctx = _lib.default_context(device)
+    lib = ctx.lib
+    z = np.ascontiguousarray(z, dtype=np.int32)
+    xyz = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(len(z), 3)
+    nao = ctypes.c_int()
+    lib.pm3gpu_result_sizes(len(z), _ip(z), ctypes.byref(nao))
+    n = max(nao.value, 0)
+    res = _lib.Result()
+    charges = np.zeros(len(z))
+    dens = np.zeros((n, n)) if want_density else None
+    eps = np.zeros(n) if want_mo_energies else None
+    if want_gradient:
+        grad = np.zeros((len(z), 3))
+        rc = lib.pm3gpu_gradient(ctx.ptr, len(z), _ip(z), _dp(xyz), ctypes.byref(opts), ctypes.byref(res),
+                                 _dp(charges), _dp(grad))
+    else:
+        grad = None
+        rc = lib.pm3gpu_single_point(ctx.ptr, len(z), _ip(z), _dp(xyz), ctypes.byref(opts), ctypes.byref(res),
+                                     _dp(charges), _dp(dens), _dp(eps))
+    if rc != _lib.OK:
+        raise ValueError(ctx.last_error() or f"pm3gpu status {rc}")
+    out = {name: getattr(res, name) for name, _ in _lib.Result._fields_}
+    out["dipole_debye"] = list(res.dipole_debye)
+    out["homo_ev"] = res.homo_ev if res.has_homo else None
+    out["lumo_ev"] = res.lumo_ev if res.has_lumo else None
+    out["converged"] = bool(res.converged)
+    out["unrestricted"] = bool(res.unrestricted)
+    out["charges"] = charges
+    if dens is not None:
+        out["density"] = dens
+    if eps is not None:
+        out["mo_energies"] = eps
+    if grad is not None:
+        out["gradient"] = grad
+    return out
+
+
+def single_point(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+                 reference: str = "auto", method: str = "pm3", field=None) -> dict:
+    """PM3 single-point energy and properties (python/pm3_rs/native.py:41-83).
+
+    Positions in Angstrom. Returns ``energy_hartree``, ``energy_ev``, ``heat_of_formation_kcal``,
+    ``electronic_ev``, ``core_ev``, ``charges`` (Mulliken, e), ``dipole_debye`` ([x, y, z]),
+    ``homo_ev``, ``lumo_ev``, ``converged`` and ``unrestricted``.
+    """
+    _check_method(method, field)
+    z, xyz = _as_arrays(numbers, positions)
+    r = run(z, xyz, options(charge, multiplicity, reference))
+    return {
+        "energy_hartree": r["total_ev"] * EV_TO_HARTREE,
+        "energy_ev": r["total_ev"],
+        "heat_of_formation_kcal": r["heat_of_formation_kcal"],
+        "electronic_ev": r["electronic_ev"],
+        "core_ev": r["core_ev"],
+        "charges": [float(q) for q in r["charges"]],
+        "dipole_debye": [float(v) for v in r["dipole_debye"]],
+        "homo_ev": r["homo_ev"],
+        "lumo_ev": r["lumo_ev"],
+        "converged": r["converged"],
+        "unrestricted": r["unrestricted"],
+    }
+
+
+def gradient(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+             reference: str = "auto", method: str = "pm3", field=None) -> dict:
+    """Energy and analytic gradient dE/dR (src/python.rs:299-357): Hartree/Bohr and eV/Angstrom."""
+    _check_method(method, field)
+    z, xyz = _as_arrays(numbers, positions)
+    r = run(z, xyz, options(charge, multiplicity, reference), want_gradient=True)
+    g = r["gradient"]
+    return {
+        "energy_hartree": r["total_ev"] * EV_TO_HARTREE,
+        "energy_ev": r["total_ev"],
+        "heat_of_formation_kcal": r["heat_of_formation_kcal"],
+        "gradient_hartree_per_bohr": (g * EV_TO_HARTREE).tolist(),
+        "gradient_ev_per_angstrom": (g * ANGSTROM_TO_BOHR).tolist(),
+    }
+
+
+def forces(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+           reference: str = "auto", method: str = "pm3", field=None) -> dict:
+    """Energy and forces (= -gradient), Hartree/Bohr and eV/Angstrom."""
+    g = gradient(numbers, positions, charge, multiplicity, reference, method, field)
+    return {
+        "energy_hartree": g["energy_hartree"],
+        "energy_ev": g["energy_ev"],
+        "heat_of_formation_kcal": g["heat_of_formation_kcal"],
+        "forces_hartree_per_bohr": (-np.asarray(g["gradient_hartree_per_bohr"])).tolist(),
+        "forces_ev_per_angstrom": (-np.asarray(g["gradient_ev_per_angstrom"])).tolist(),
+    }
+
+
+class BatchResult:
+    """Column arrays of a batched solve (one row per molecule)."""
+
+    def __init__(self, results, charges, gradients, offsets):
+        self.status = np.array([r.status for r in results], dtype=np.int32)
+        self.heat_of_formation_kcal = np.array([r.heat_of_formation_kcal for r in results])
+        self.total_ev = np.array([r.total_ev for r in results])
+        self.electronic_ev = np.array([r.electronic_ev for r in results])
+        self.core_ev = np.array([r.core_ev for r in results])
+        self.dipole_debye = np.array([list(r.dipole_debye) for r in results]).reshape(-1, 3)
+        self.homo_ev = np.array([r.homo_ev if r.has_homo else np.nan for r in results])
+        self.lumo_ev = np.array([r.lumo_ev if r.has_lumo else np.nan for r in results])
+        self.iterations = np.array([r.iterations for r in results], dtype=np.int32)
+        self.converged = np.array([bool(r.converged) for r in results])
+        self.unrestricted = np.array([bool(r.unrestricted) for r in results])
+        self.scf_paths_tried = np.array([r.scf_paths_tried for r in results], dtype=np.int32)
+        self.charges = charges
+        self.gradients = gradients
+        self.offsets = offsets
+
+    def charges_of(self, m: int) -> np.ndarray:
+        return self.charges[self.offsets[m]:self.offsets[m + 1]]
+
+
+def batch(offsets, z, xyz_bohr, opts=None, want_gradient=False, device: int = 0) -> BatchResult:
+    """run_pm3 over many molecules in one persistent launch. Molecule m owns atoms
+    [offsets[m], offsets[m+1]) of z / xyz_bohr (Bohr). ``opts``: one Options or a list."""
+    ctx = _lib.default_context(device)
+    lib = ctx.lib
+    offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+    z = np.ascontiguousarray(z, dtype=np.int32)
+    xyz = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1, 3)
+    n_mol = len(offsets) - 1
+    if opts is None:
+        opts = options()
+    per_mol = isinstance(opts, (list, tuple))
+    if per_mol:
+        arr = (_lib.Options * n_mol)(*opts)
+        optp = ctypes.cast(arr, ctypes.POINTER(_lib.Options))
+    else:
+        arr = opts
+        optp = ctypes.pointer(opts)
+    results = (_lib.Result * max(n_mol, 1))()
+    charges = np.zeros(len(z))
+    grads = np.zeros((len(z), 3)) if want_gradient else None
+    rc = lib.pm3gpu_batch(ctx.ptr, n_mol, _ip(offsets), _ip(z), _dp(xyz), optp, int(per_mol), results,
+                          _dp(charges), _dp(grads))
+    if rc != _lib.OK:
+        raise ValueError(ctx.last_error() or f"pm3gpu status {rc}")
+    return BatchResult(list(results)[:n_mol], charges, grads, offsets)
