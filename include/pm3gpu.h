@@ -157,6 +157,14 @@ int pm3gpu_fock(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const double* xy
  * Returns the count written. */
 int pm3gpu_last_timings(pm3gpu_ctx* ctx, double* ms, int max_entries);
 
+/* SM cycles spent per SCF phase by the last call, summed over CTAs, when the context was
+ * created with PM3GPU_PROFILE=1 in the environment (the counterpart of pm3-rs's PM3_TIMING,
+ * src/scf.rs:469-485). Phases: 0 integrals + H_core, 1 Fock build + energy, 2 commutator,
+ * 3 accelerator solve, 4 extrapolation / packing, 5 tridiagonalisation, 6 eigenvalues,
+ * 7 eigenvectors, 8 back-transformation, 9 density, 10 closing energy + properties,
+ * 11 gradient. Returns the number of phases written (0 when profiling is off). */
+int pm3gpu_last_phase_cycles(pm3gpu_ctx* ctx, double* cycles, int max_entries);
+
 /* Host-to-device and device-to-host bytes moved by the last call. */
 int pm3gpu_last_transfer_bytes(pm3gpu_ctx* ctx, long long* h2d, long long* d2h);
 

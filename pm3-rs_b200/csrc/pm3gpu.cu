@@ -5,12 +5,14 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/pm3gpu.h"
+#include "gradient_kernel.cuh"
 #include "scf_job.cuh"
 
 using namespace pm3gpu;
@@ -77,13 +79,16 @@ struct pm3gpu_ctx {
   std::string err;
   ElemDev h_elem[kMaxZ];
   PairDev h_pairs;
-  DevBuf elem, pairs, z, xyz, jobs, out, charges, dens, grads, eps, work, queue;
+  DevBuf elem, pairs, z, xyz, jobs, out, charges, dens, grads, eps, work, queue, rq, gmols, aooff;
   int sms = 0, smem_optin = 0;
   double timings[6] = {0, 0, 0, 0, 0, 0};
   int launches = 0;
   long long h2d = 0, d2h = 0;  // bytes moved by the last call
   cudaEvent_t ev[6] = {};
   cudaEvent_t kev[2] = {};
+  bool profile = false;
+  DevBuf prof;
+  double phase_cycles[kPhases] = {};
 };
 
 namespace {
@@ -241,21 +246,54 @@ SmemLayout make_layout(int amax, int nmax, int optin) {
   return L;
 }
 
-// One persistent launch over `jobs` (already sorted largest first).
-int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vector<int32_t>& zs, const int32_t* d_z,
-                const double* d_xyz, std::vector<JobOut>& outs, size_t charge_total, size_t dens_total, size_t grad_total,
-                size_t eps_total, std::vector<double>& h_charges, std::vector<double>* h_dens, std::vector<double>* h_grads,
-                std::vector<double>* h_eps, const std::vector<double>* dens_in = nullptr) {
-  const int nj = (int)jobs.size();
-  outs.assign(nj, JobOut{});
+// Output requests of a whole batch call.
+struct Want {
+  bool density = false, eps = false, grad = false;
+};
+
+// Per-job output bookkeeping: offsets of each job's arrays.
+struct Offsets {
+  size_t charges = 0, dens = 0, eps = 0;
+};
+
+void assign_offsets(JobDesc& j, const Want& w, Offsets& t) {
+  j.charge_off = (long long)t.charges;
+  t.charges += j.natom;
+  const bool uhf = (j.flags & kJobUhf) != 0;
+  if (w.density || w.grad) {
+    j.flags |= (w.density ? kJobDensity : 0) | (w.grad ? kJobGrad : 0);
+    j.dens_off = (long long)t.dens;
+    t.dens += (size_t)j.nao * j.nao * ((w.grad && uhf) ? 3 : 1);
+  }
+  if (w.eps) {
+    j.flags |= kJobEps;
+    j.eps_off = (long long)t.eps;
+    t.eps += 2 * (size_t)j.nao;
+  }
+}
+
+// One persistent launch: the first-pass jobs (sorted largest first) plus the rung table the
+// kernel may enqueue from (scf.rs:599-715). Outputs are read back to the host.
+struct LaunchOut {
+  std::vector<JobOut> out, rout;
+  std::vector<double> charges, dens, eps;
+};
+
+int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vector<JobDesc>& rjobs,
+                const std::vector<int32_t>& zs, const int32_t* d_z, const double* d_xyz, const Offsets& tot,
+                bool read_dens, bool read_eps, LaunchOut& R, const std::vector<double>* dens_in = nullptr) {
+  const int nj = (int)jobs.size(), nr = (int)rjobs.size();
+  R.out.assign(nj, JobOut{});
+  R.rout.assign(nr, JobOut{});
   if (nj == 0) return PM3GPU_OK;
   int nmax = 1, amax = 1;
   long long wcap = 1;
-  for (const JobDesc& j : jobs) {
-    nmax = std::max(nmax, j.nao);
-    amax = std::max(amax, j.natom);
-    wcap = std::max(wcap, pair_table_doubles(c, zs.data() + j.atom0, j.natom));
-  }
+  for (const std::vector<JobDesc>* L : {&jobs, &rjobs})
+    for (const JobDesc& j : *L) {
+      nmax = std::max(nmax, j.nao);
+      amax = std::max(amax, j.natom);
+      wcap = std::max(wcap, pair_table_doubles(c, zs.data() + j.atom0, j.natom));
+    }
   const SmemLayout L = make_layout(amax, nmax, c->smem_optin);
   CUDA_TRY(c, cudaFuncSetAttribute(scf_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes));
   int per_sm = 0;
@@ -264,23 +302,27 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   const long long slot = slot_doubles(nmax, wcap);
   size_t free_b = 0, total_b = 0;
   CUDA_TRY(c, cudaMemGetInfo(&free_b, &total_b));
-  long long grid = std::min<long long>(nj, (long long)c->sms * per_sm);
+  long long grid = std::min<long long>(nj + nr, (long long)c->sms * per_sm);
   const size_t budget = (size_t)(0.6 * (double)(free_b + c->work.bytes));
   while (grid > 1 && (size_t)grid * slot * 8 > budget) --grid;
-  if ((size_t)grid * slot * 8 > budget)
-    return fail(c, PM3GPU_RESOURCE_LIMIT, "SCF workspace exceeds device memory");
+  if ((size_t)grid * slot * 8 > budget) return fail(c, PM3GPU_RESOURCE_LIMIT, "SCF workspace exceeds device memory");
   CUDA_TRY(c, c->work.ensure((size_t)grid * slot * 8));
-  CUDA_TRY(c, c->jobs.ensure(sizeof(JobDesc) * nj));
-  CUDA_TRY(c, c->out.ensure(sizeof(JobOut) * nj));
-  CUDA_TRY(c, c->charges.ensure(8 * std::max<size_t>(charge_total, 1)));
-  CUDA_TRY(c, c->dens.ensure(8 * std::max<size_t>(dens_total, 1)));
-  CUDA_TRY(c, c->grads.ensure(8 * std::max<size_t>(grad_total, 1)));
-  CUDA_TRY(c, c->eps.ensure(8 * std::max<size_t>(eps_total, 1)));
+  CUDA_TRY(c, c->jobs.ensure(sizeof(JobDesc) * (nj + nr)));
+  CUDA_TRY(c, c->out.ensure(sizeof(JobOut) * (nj + nr)));
+  CUDA_TRY(c, c->rq.ensure(2 * sizeof(int) * std::max(nr, 1)));
+  CUDA_TRY(c, c->charges.ensure(8 * std::max<size_t>(tot.charges, 1)));
+  CUDA_TRY(c, c->dens.ensure(8 * std::max<size_t>(tot.dens, 1)));
+  CUDA_TRY(c, c->eps.ensure(8 * std::max<size_t>(tot.eps, 1)));
   CUDA_TRY(c, c->queue.ensure(64));
   CUDA_TRY(c, cudaMemcpyAsync(c->jobs.p, jobs.data(), sizeof(JobDesc) * nj, cudaMemcpyHostToDevice, c->stream));
+  if (nr)
+    CUDA_TRY(c, cudaMemcpyAsync(c->jobs.as<JobDesc>() + nj, rjobs.data(), sizeof(JobDesc) * nr, cudaMemcpyHostToDevice,
+                                c->stream));
   if (dens_in && !dens_in->empty())
     CUDA_TRY(c, cudaMemcpyAsync(c->dens.p, dens_in->data(), 8 * dens_in->size(), cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaMemsetAsync(c->queue.p, 0, 64, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->rq.p, 0, 2 * sizeof(int) * std::max(nr, 1), c->stream));
+  if (nr) CUDA_TRY(c, cudaMemsetAsync(c->out.as<JobOut>() + nj, 0xff, sizeof(JobOut) * nr, c->stream));
   KernelArgs a{};
   a.elem = c->elem.as<ElemDev>();
   a.pairs = c->pairs.as<PairDev>();
@@ -289,95 +331,117 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   a.jobs = c->jobs.as<JobDesc>();
   a.njobs = nj;
   a.out = c->out.as<JobOut>();
+  a.rjobs = c->jobs.as<JobDesc>() + nj;
+  a.nrjobs = nr;
+  a.rout = c->out.as<JobOut>() + nj;
+  a.rlist = c->rq.as<int>();
+  a.rready = c->rq.as<int>() + std::max(nr, 1);
   a.charges = c->charges.as<double>();
   a.densities = c->dens.as<double>();
-  a.grads = c->grads.as<double>();
+  a.grads = nullptr;
   a.eps = c->eps.as<double>();
   a.work = c->work.as<double>();
   a.slot = slot;
   a.nmax = nmax;
   a.wcap = wcap;
   a.queue = c->queue.as<int>();
+  a.prof = nullptr;
+  if (c->profile) {
+    CUDA_TRY(c, c->prof.ensure(sizeof(unsigned long long) * kPhases));
+    CUDA_TRY(c, cudaMemsetAsync(c->prof.p, 0, sizeof(unsigned long long) * kPhases, c->stream));
+    a.prof = c->prof.as<unsigned long long>();
+  }
   a.sm = L;
   CUDA_TRY(c, cudaEventRecord(c->kev[0], c->stream));
   scf_batch_kernel<<<(unsigned)grid, kThreads, L.bytes, c->stream>>>(a);
   c->launches += 1;
   CUDA_TRY(c, cudaGetLastError());
   CUDA_TRY(c, cudaEventRecord(c->kev[1], c->stream));
-  CUDA_TRY(c, cudaMemcpyAsync(outs.data(), c->out.p, sizeof(JobOut) * nj, cudaMemcpyDeviceToHost, c->stream));
-  h_charges.resize(charge_total);
-  if (charge_total)
-    CUDA_TRY(c, cudaMemcpyAsync(h_charges.data(), c->charges.p, 8 * charge_total, cudaMemcpyDeviceToHost, c->stream));
-  if (h_dens && dens_total) {
-    h_dens->resize(dens_total);
-    CUDA_TRY(c, cudaMemcpyAsync(h_dens->data(), c->dens.p, 8 * dens_total, cudaMemcpyDeviceToHost, c->stream));
+  int qh[4] = {0, 0, 0, 0};
+  CUDA_TRY(c, cudaMemcpyAsync(qh, c->queue.p, sizeof(qh), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(R.out.data(), c->out.p, sizeof(JobOut) * nj, cudaMemcpyDeviceToHost, c->stream));
+  if (nr)
+    CUDA_TRY(c, cudaMemcpyAsync(R.rout.data(), c->out.as<JobOut>() + nj, sizeof(JobOut) * nr, cudaMemcpyDeviceToHost,
+                                c->stream));
+  R.charges.resize(tot.charges);
+  if (tot.charges)
+    CUDA_TRY(c, cudaMemcpyAsync(R.charges.data(), c->charges.p, 8 * tot.charges, cudaMemcpyDeviceToHost, c->stream));
+  if (read_dens && tot.dens) {
+    R.dens.resize(tot.dens);
+    CUDA_TRY(c, cudaMemcpyAsync(R.dens.data(), c->dens.p, 8 * tot.dens, cudaMemcpyDeviceToHost, c->stream));
   }
-  if (h_grads && grad_total) {
-    h_grads->resize(grad_total);
-    CUDA_TRY(c, cudaMemcpyAsync(h_grads->data(), c->grads.p, 8 * grad_total, cudaMemcpyDeviceToHost, c->stream));
-  }
-  if (h_eps && eps_total) {
-    h_eps->resize(eps_total);
-    CUDA_TRY(c, cudaMemcpyAsync(h_eps->data(), c->eps.p, 8 * eps_total, cudaMemcpyDeviceToHost, c->stream));
+  if (read_eps && tot.eps) {
+    R.eps.resize(tot.eps);
+    CUDA_TRY(c, cudaMemcpyAsync(R.eps.data(), c->eps.p, 8 * tot.eps, cudaMemcpyDeviceToHost, c->stream));
   }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (qh[3]) return fail(c, PM3GPU_CUDA_ERROR, "stability-search queue handshake timed out on the device");
+  if (c->profile) {
+    unsigned long long ph[kPhases];
+    CUDA_TRY(c, cudaMemcpy(ph, c->prof.p, sizeof(ph), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < kPhases; ++k) c->phase_cycles[k] += (double)ph[k];
+  }
   float kms = 0.f;
   CUDA_TRY(c, cudaEventElapsedTime(&kms, c->kev[0], c->kev[1]));
   c->timings[5] += kms;
-  c->h2d += (long long)(sizeof(JobDesc) * nj + (dens_in ? 8 * dens_in->size() : 0));
-  c->d2h += (long long)(sizeof(JobOut) * nj + 8 * charge_total + (h_dens ? 8 * dens_total : 0) +
-                        (h_grads ? 8 * grad_total : 0) + (h_eps ? 8 * eps_total : 0));
+  c->h2d += (long long)(sizeof(JobDesc) * (nj + nr) + (dens_in ? 8 * dens_in->size() : 0));
+  c->d2h += (long long)(sizeof(JobOut) * (nj + nr) + 8 * tot.charges + (read_dens ? 8 * tot.dens : 0) +
+                        (read_eps ? 8 * tot.eps : 0) + sizeof(qh));
   return PM3GPU_OK;
 }
 
-// Output requests of a whole batch call.
-struct Want {
-  bool density = false, eps = false, grad = false;
-};
-
-// Per-job output bookkeeping: offsets of each job's arrays.
-struct Offsets {
-  size_t charges = 0, dens = 0, grads = 0, eps = 0;
-};
-
-void assign_offsets(JobDesc& j, const Want& w, Offsets& t) {
-  j.charge_off = (long long)t.charges;
-  t.charges += j.natom;
-  if (w.density) {
-    j.flags |= kJobDensity;
-    j.dens_off = (long long)t.dens;
-    t.dens += (size_t)j.nao * j.nao;
+// Gradients of the selected states of `mols` (one thread per atom pair of the whole batch).
+int launch_gradients(pm3gpu_ctx* c, const std::vector<GradMol>& mols, const std::vector<int32_t>& ao_off,
+                     const int32_t* d_z, const double* d_xyz, size_t total_atoms, std::vector<double>& grads) {
+  grads.assign(3 * total_atoms, 0.0);
+  if (mols.empty()) return PM3GPU_OK;
+  long long npairs = mols.back().pair0 + (long long)mols.back().natom * (mols.back().natom - 1) / 2;
+  CUDA_TRY(c, c->gmols.ensure(sizeof(GradMol) * mols.size()));
+  CUDA_TRY(c, c->aooff.ensure(4 * std::max<size_t>(ao_off.size(), 1)));
+  CUDA_TRY(c, c->grads.ensure(24 * std::max<size_t>(total_atoms, 1)));
+  CUDA_TRY(c, cudaMemcpyAsync(c->gmols.p, mols.data(), sizeof(GradMol) * mols.size(), cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->aooff.p, ao_off.data(), 4 * ao_off.size(), cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->grads.p, 0, 24 * total_atoms, c->stream));
+  if (npairs > 0) {
+    GradArgs g{};
+    g.elem = c->elem.as<ElemDev>();
+    g.pairs = c->pairs.as<PairDev>();
+    g.z = d_z;
+    g.xyz = d_xyz;
+    g.ao_off = c->aooff.as<int>();
+    g.mols = c->gmols.as<GradMol>();
+    g.nmol = (int)mols.size();
+    g.npairs = npairs;
+    g.dens = c->dens.as<double>();
+    g.grad = c->grads.as<double>();
+    const long long blocks = std::min<long long>((npairs + 127) / 128, (long long)c->sms * 16);
+    gradient_kernel<<<(unsigned)blocks, 128, 0, c->stream>>>(g);
+    c->launches += 1;
+    CUDA_TRY(c, cudaGetLastError());
   }
-  if (w.eps) {
-    j.flags |= kJobEps;
-    j.eps_off = (long long)t.eps;
-    t.eps += 2 * (size_t)j.nao;
-  }
-  if (w.grad) {
-    j.flags |= kJobGrad;
-    j.grad_off = (long long)t.grads;
-    t.grads += 3 * (size_t)j.natom;
-  }
+  CUDA_TRY(c, cudaMemcpyAsync(grads.data(), c->grads.p, 24 * total_atoms, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->h2d += (long long)(sizeof(GradMol) * mols.size() + 4 * ao_off.size());
+  c->d2h += (long long)(24 * total_atoms);
+  return PM3GPU_OK;
 }
 
 struct HostJobResult {
   JobOut o;
-  const double* charges = nullptr;
-  const double* dens = nullptr;
-  const double* grads = nullptr;
-  const double* eps = nullptr;
+  const JobDesc* job = nullptr;
   bool unrestricted = false;
 };
 
-// The whole run_pm3 flow for a batch: first solve, stability search (scf.rs:599-715) as a
-// second persistent launch, selection, and the result epilogue (scf.rs:716-847).
+// The run_pm3 flow over a batch (scf.rs:450-848): one persistent launch solves every
+// molecule and the stability-search rungs its first pass asks for; the host then selects
+// each molecule's state exactly as run_pm3 does and forms the epilogue.
 int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_z, const double* h_xyz,
               const int32_t* d_z, const double* d_xyz, const pm3gpu_options* opts, int per_mol, const Want& want,
               pm3gpu_result* results, double* charges, double* gradients, double* density, double* mo_energies) {
   c->launches = 0;
   c->timings[5] = 0.0;
   c->h2d = c->d2h = 0;
-  for (int k = 0; k < 6; ++k) cudaEventRecord(c->ev[k], c->stream);  // placeholders
+  for (int k = 0; k < kPhases; ++k) c->phase_cycles[k] = 0.0;
   cudaEventRecord(c->ev[0], c->stream);
   const int total_atoms = h_offs[n_mol];
   std::vector<int32_t> zs(h_z, h_z + total_atoms);
@@ -394,9 +458,8 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
   }
   cudaEventRecord(c->ev[1], c->stream);
   std::vector<MolPlan> plans(n_mol);
-  std::vector<JobDesc> jobs;
-  std::vector<int> job_mol;
-  Offsets t1;
+  std::vector<JobDesc> jobs, rjobs;
+  Offsets tot;
   for (int m = 0; m < n_mol; ++m) {
     MolPlan& p = plans[m];
     p.atom0 = h_offs[m];
@@ -407,104 +470,80 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
     if (p.status != PM3GPU_OK) continue;
     JobDesc j = p.steered ? make_job(p, o->guess, o->accelerator, o->level_shift_ev, o->damping, false, 0)
                           : make_job(p, o->guess, o->accelerator, 0.0, 0.0, false, 0);
-    assign_offsets(j, want, t1);
+    j.mol = m;
+    assign_offsets(j, want, tot);
+    // the rungs run_pm3 would try, in its order, skipping those it skips (scf.rs:610-678)
+    j.stab = 0;
+    if (o->stability == PM3GPU_STABILITY_ALWAYS && !p.steered) j.stab = 2;
+    if (o->stability == PM3GPU_STABILITY_AUTO && !p.steered) j.stab = 1;
+    j.rung0 = (int)rjobs.size();
+    j.nrung = 0;
+    if (j.stab) {
+      const int primary = o->guess == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_CORE : PM3GPU_GUESS_SAD;
+      const int other = primary == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_SAD : PM3GPU_GUESS_CORE;
+      const bool closed = !p.use_uhf;
+      const Rung all[7] = {{primary, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                           {other, o->accelerator, 0.0, 0.0, false},
+                           {other, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                           {PM3GPU_GUESS_SYMMETRY_BROKEN, o->accelerator, 0.0, 0.0, false},
+                           {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                           {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, -2.0, 0.0, closed},
+                           {primary, PM3GPU_ACCEL_CDIIS, 0.0, 0.85, closed}};
+      for (const Rung& r : all) {
+        if (r.unrestricted != closed) continue;
+        JobDesc rj = make_job(p, r.guess, r.accel, r.shift, r.damp, r.unrestricted, 0);
+        rj.mol = m;
+        rj.stab = 0;
+        rj.nrung = 0;
+        assign_offsets(rj, want, tot);
+        p.rungs.push_back(r);
+        rjobs.push_back(rj);
+        ++j.nrung;
+      }
+    }
     p.first_job = (int)jobs.size();
     jobs.push_back(j);
-    job_mol.push_back(m);
   }
   // largest first (longest-processing-time order) for the work queue
-  std::vector<int> order(jobs.size());
+  std::vector<int> order(jobs.size()), pos(jobs.size());
   for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return jobs[a].nao > jobs[b].nao; });
   std::vector<JobDesc> sorted(jobs.size());
-  std::vector<int> pos(jobs.size());
   for (size_t i = 0; i < order.size(); ++i) {
     sorted[i] = jobs[order[i]];
     pos[order[i]] = (int)i;
   }
-  std::vector<JobOut> o1;
-  std::vector<double> q1, d1, g1, e1;
-  int rc = launch_jobs(c, sorted, zs, dz, dxyz, o1, t1.charges, t1.dens, t1.grads, t1.eps, q1, &d1, &g1, &e1);
+  LaunchOut R;
+  int rc = launch_jobs(c, sorted, rjobs, zs, dz, dxyz, tot, want.density, want.eps, R);
   if (rc != PM3GPU_OK) return rc;
   cudaEventRecord(c->ev[2], c->stream);
 
-  // ---------------------------------------------------------------- stability search
-  std::vector<JobDesc> rjobs;
-  std::vector<int> rmol;
-  Offsets t2;
-  for (int m = 0; m < n_mol; ++m) {
-    MolPlan& p = plans[m];
-    if (p.status != PM3GPU_OK) continue;
-    const pm3gpu_options& o = *p.o;
-    const JobOut& f = o1[pos[p.first_job]];
-    bool search = false;
-    if (o.stability == PM3GPU_STABILITY_ALWAYS) search = !p.steered;
-    else if (o.stability == PM3GPU_STABILITY_AUTO) search = !p.steered && f.gap < 6.0;
-    if (!search) continue;
-    const int primary = o.guess == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_CORE : PM3GPU_GUESS_SAD;
-    const int other = primary == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_SAD : PM3GPU_GUESS_CORE;
-    const bool closed = !p.use_uhf;
-    const Rung all[7] = {{primary, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                         {other, o.accelerator, 0.0, 0.0, false},
-                         {other, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                         {PM3GPU_GUESS_SYMMETRY_BROKEN, o.accelerator, 0.0, 0.0, false},
-                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, -2.0, 0.0, closed},
-                         {primary, PM3GPU_ACCEL_CDIIS, 0.0, 0.85, closed}};
-    for (const Rung& r : all) {
-      if (r.unrestricted != closed) continue;  // scf.rs:676-678
-      JobDesc j = make_job(p, r.guess, r.accel, r.shift, r.damp, r.unrestricted, 0);
-      assign_offsets(j, want, t2);
-      p.rung_jobs.push_back((int)rjobs.size());
-      p.rungs.push_back(r);
-      rjobs.push_back(j);
-      rmol.push_back(m);
-    }
-  }
-  std::vector<int> rorder(rjobs.size()), rpos(rjobs.size());
-  for (size_t i = 0; i < rorder.size(); ++i) rorder[i] = (int)i;
-  std::stable_sort(rorder.begin(), rorder.end(), [&](int a, int b) { return rjobs[a].nao > rjobs[b].nao; });
-  std::vector<JobDesc> rsorted(rjobs.size());
-  for (size_t i = 0; i < rorder.size(); ++i) {
-    rsorted[i] = rjobs[rorder[i]];
-    rpos[rorder[i]] = (int)i;
-  }
-  std::vector<JobOut> o2;
-  std::vector<double> q2, d2, g2, e2;
-  if (!rjobs.empty()) {
-    rc = launch_jobs(c, rsorted, zs, dz, dxyz, o2, t2.charges, t2.dens, t2.grads, t2.eps, q2, &d2, &g2, &e2);
-    if (rc != PM3GPU_OK) return rc;
-  }
-  cudaEventRecord(c->ev[3], c->stream);
-
   // ---------------------------------------------------------------- selection + epilogue
+  std::vector<HostJobResult> chosen(n_mol);
   for (int m = 0; m < n_mol; ++m) {
     MolPlan& p = plans[m];
-    pm3gpu_result& R = results[m];
-    std::memset(&R, 0, sizeof(R));
-    R.status = p.status;
-    R.nao = p.nao;
-    const int atom0 = h_offs[m];
+    pm3gpu_result& Rm = results[m];
+    std::memset(&Rm, 0, sizeof(Rm));
+    Rm.status = p.status;
+    Rm.nao = p.nao;
     if (p.status != PM3GPU_OK) {
-      if (!c->err.size()) c->err = p.msg;
-      if (n_mol == 1) c->err = p.msg;
+      if (c->err.empty() || n_mol == 1) c->err = p.msg;
       continue;
     }
     const JobDesc& fj = jobs[p.first_job];
     HostJobResult st;
-    st.o = o1[pos[p.first_job]];
+    st.o = R.out[pos[p.first_job]];
+    st.job = &fj;
     st.unrestricted = (fj.flags & kJobUhf) != 0;
-    st.charges = q1.data() + fj.charge_off;
-    if (want.density) st.dens = d1.data() + fj.dens_off;
-    if (want.grad) st.grads = g1.data() + fj.grad_off;
-    if (want.eps) st.eps = e1.data() + fj.eps_off;
     const double first_ev = st.o.electronic;
     int paths = 1;
-    for (size_t r = 0; r < p.rung_jobs.size(); ++r) {
+    const bool searched = fj.nrung > 0 && R.rout[fj.rung0].status != -1;
+    for (int r = 0; searched && r < fj.nrung; ++r) {
       ++paths;
-      const JobDesc& rj = rjobs[p.rung_jobs[r]];
+      const JobDesc& rj = rjobs[fj.rung0 + r];
       HostJobResult cand;
-      cand.o = o2[rpos[p.rung_jobs[r]]];
+      cand.o = R.rout[fj.rung0 + r];
+      cand.job = &rj;
       cand.unrestricted = (rj.flags & kJobUhf) != 0;
       if (!cand.o.converged) continue;
       if (p.rungs[r].unrestricted) {  // a spin-pure unrestricted closed shell is a restricted state
@@ -515,48 +554,79 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
         cand.o.has_homo = cand.o.has_homo_a;
         cand.o.has_lumo = cand.o.has_lumo_a;
       }
-      cand.charges = q2.data() + rj.charge_off;
-      if (want.density) cand.dens = d2.data() + rj.dens_off;
-      if (want.grad) cand.grads = g2.data() + rj.grad_off;
-      if (want.eps) cand.eps = e2.data() + rj.eps_off;
       if (!st.o.converged || cand.o.electronic < st.o.electronic - 1.0e-6) st = cand;
     }
+    chosen[m] = st;
     double e_isol = 0.0, eheat = 0.0;
     for (int a = 0; a < p.natom; ++a) {
-      e_isol += c->h_elem[h_z[atom0 + a]].e_isol;
-      eheat += c->h_elem[h_z[atom0 + a]].eheat_ev;
+      e_isol += c->h_elem[h_z[p.atom0 + a]].e_isol;
+      eheat += c->h_elem[h_z[p.atom0 + a]].eheat_ev;
     }
-    R.n_occ = p.n_alpha;
-    R.n_beta = st.unrestricted ? p.n_beta : p.n_alpha;
-    R.electronic_ev = st.o.electronic;
-    R.core_ev = st.o.core;
-    R.total_ev = st.o.electronic + st.o.core;
-    R.heat_of_formation_kcal = (R.total_ev - e_isol + eheat) * kEvToKcal;
-    R.iterations = st.o.iterations;
-    R.converged = st.o.converged;
-    R.unrestricted = st.unrestricted ? 1 : 0;
-    R.scf_paths_tried = paths;
-    R.scf_improvement_ev = std::max(first_ev - st.o.electronic, 0.0);
-    R.last_change = st.o.last_change;
-    R.homo_ev = st.o.homo;
-    R.lumo_ev = st.o.lumo;
-    R.has_homo = st.o.has_homo;
-    R.has_lumo = st.o.has_lumo;
-    for (int k = 0; k < 3; ++k) R.dipole_debye[k] = st.o.dipole[k];
-    R.dipole_magnitude = std::sqrt(R.dipole_debye[0] * R.dipole_debye[0] + R.dipole_debye[1] * R.dipole_debye[1] +
-                                   R.dipole_debye[2] * R.dipole_debye[2]);
+    Rm.n_occ = p.n_alpha;
+    Rm.n_beta = st.unrestricted ? p.n_beta : p.n_alpha;
+    Rm.electronic_ev = st.o.electronic;
+    Rm.core_ev = st.o.core;
+    Rm.total_ev = st.o.electronic + st.o.core;
+    Rm.heat_of_formation_kcal = (Rm.total_ev - e_isol + eheat) * kEvToKcal;
+    Rm.iterations = st.o.iterations;
+    Rm.converged = st.o.converged;
+    Rm.unrestricted = st.unrestricted ? 1 : 0;
+    Rm.scf_paths_tried = paths;
+    Rm.scf_improvement_ev = std::max(first_ev - st.o.electronic, 0.0);
+    Rm.last_change = st.o.last_change;
+    Rm.homo_ev = st.o.homo;
+    Rm.lumo_ev = st.o.lumo;
+    Rm.has_homo = st.o.has_homo;
+    Rm.has_lumo = st.o.has_lumo;
+    for (int k = 0; k < 3; ++k) Rm.dipole_debye[k] = st.o.dipole[k];
+    Rm.dipole_magnitude = std::sqrt(Rm.dipole_debye[0] * Rm.dipole_debye[0] + Rm.dipole_debye[1] * Rm.dipole_debye[1] +
+                                    Rm.dipole_debye[2] * Rm.dipole_debye[2]);
     if (!st.o.converged) {
-      R.status = PM3GPU_SCF_NOT_CONVERGED;
+      Rm.status = PM3GPU_SCF_NOT_CONVERGED;
       char msg[160];
       std::snprintf(msg, sizeof msg, "PM3 SCF did not converge after %d iterations (error=%.3e)", st.o.iterations,
                     st.o.last_change);
       c->err = msg;
     }
-    if (charges) std::memcpy(charges + atom0, st.charges, 8 * (size_t)p.natom);
-    if (gradients && st.grads) std::memcpy(gradients + 3 * (size_t)atom0, st.grads, 24 * (size_t)p.natom);
-    if (density && st.dens) std::memcpy(density, st.dens, 8 * (size_t)p.nao * p.nao);
-    if (mo_energies && st.eps) std::memcpy(mo_energies, st.eps, 8 * (size_t)p.nao);
+    if (charges) std::memcpy(charges + p.atom0, R.charges.data() + st.job->charge_off, 8 * (size_t)p.natom);
+    if (density && want.density) std::memcpy(density, R.dens.data() + st.job->dens_off, 8 * (size_t)p.nao * p.nao);
+    if (mo_energies && want.eps) std::memcpy(mo_energies, R.eps.data() + st.job->eps_off, 8 * (size_t)p.nao);
   }
+  // ---------------------------------------------------------------- analytic gradients
+  if (want.grad && gradients) {
+    std::vector<GradMol> gm;
+    std::vector<int32_t> ao_off(total_atoms, 0);
+    long long pair0 = 0;
+    for (int m = 0; m < n_mol; ++m) {
+      const MolPlan& p = plans[m];
+      if (p.status != PM3GPU_OK || !chosen[m].o.converged) continue;
+      int off = 0;
+      for (int a = 0; a < p.natom; ++a) {
+        ao_off[p.atom0 + a] = off;
+        off += c->h_elem[h_z[p.atom0 + a]].norb;
+      }
+      GradMol g{};
+      g.atom0 = p.atom0;
+      g.natom = p.natom;
+      g.nao = p.nao;
+      // a collapsed (spin-pure) unrestricted state takes the restricted gradient
+      g.uhf = chosen[m].unrestricted ? 1 : 0;
+      if ((chosen[m].job->flags & kJobUhf) == 0) g.uhf = 0;
+      g.pair0 = pair0;
+      g.dens_off = chosen[m].job->dens_off;
+      pair0 += (long long)p.natom * (p.natom - 1) / 2;
+      gm.push_back(g);
+    }
+    std::vector<double> gr;
+    rc = launch_gradients(c, gm, ao_off, dz, dxyz, (size_t)total_atoms, gr);
+    if (rc != PM3GPU_OK) return rc;
+    for (int m = 0; m < n_mol; ++m) {
+      const MolPlan& p = plans[m];
+      if (p.status != PM3GPU_OK || !chosen[m].o.converged) continue;
+      std::memcpy(gradients + 3 * (size_t)p.atom0, gr.data() + 3 * (size_t)p.atom0, 24 * (size_t)p.natom);
+    }
+  }
+  cudaEventRecord(c->ev[3], c->stream);
   cudaEventRecord(c->ev[4], c->stream);
   cudaEventSynchronize(c->ev[4]);
   float ms[4];
@@ -634,6 +704,10 @@ int pm3gpu_context_create(int device, pm3gpu_ctx** out) {
   c->sms = prop.multiProcessorCount;
   c->smem_optin = (int)prop.sharedMemPerBlockOptin;
   derive_elements(c->h_elem, &c->h_pairs);
+  {
+    const char* pe = std::getenv("PM3GPU_PROFILE");
+    c->profile = pe && pe[0] && pe[0] != '0';
+  }
   if ((e = c->elem.ensure(sizeof(c->h_elem))) != cudaSuccess) return bail(e);
   if ((e = c->pairs.ensure(sizeof(PairDev))) != cudaSuccess) return bail(e);
   if ((e = cudaMemcpy(c->elem.p, c->h_elem, sizeof(c->h_elem), cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e);
@@ -647,7 +721,7 @@ void pm3gpu_context_destroy(pm3gpu_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (DevBuf* b : {&c->elem, &c->pairs, &c->z, &c->xyz, &c->jobs, &c->out, &c->charges, &c->dens, &c->grads, &c->eps,
-                    &c->work, &c->queue})
+                    &c->work, &c->queue, &c->prof, &c->rq, &c->gmols, &c->aooff})
     b->release();
   for (int k = 0; k < 6; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
@@ -763,14 +837,15 @@ static int single_stage(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const doub
   CUDA_TRY(c, c->xyz.ensure(24 * (size_t)n_atoms));
   CUDA_TRY(c, cudaMemcpyAsync(c->z.p, z, 4 * (size_t)n_atoms, cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaMemcpyAsync(c->xyz.p, xyz, 24 * (size_t)n_atoms, cudaMemcpyHostToDevice, c->stream));
-  std::vector<JobOut> outs;
-  std::vector<double> q, dens;
   c->launches = 0;
-  int rc = launch_jobs(c, {j}, zs, c->z.as<int32_t>(), c->xyz.as<double>(), outs, (size_t)n_atoms, io.size(), 0, 0, q,
-                       &dens, nullptr, nullptr, &io);
+  Offsets tot;
+  tot.charges = (size_t)n_atoms;
+  tot.dens = io.size();
+  LaunchOut R;
+  int rc = launch_jobs(c, {j}, {}, zs, c->z.as<int32_t>(), c->xyz.as<double>(), tot, true, false, R, &io);
   if (rc != PM3GPU_OK) return rc;
-  io.swap(dens);
-  if (core_ev) *core_ev = outs[0].core;
+  io.swap(R.dens);
+  if (core_ev) *core_ev = R.out[0].core;
   return PM3GPU_OK;
 }
 
@@ -819,6 +894,13 @@ int pm3gpu_last_timings(pm3gpu_ctx* c, double* ms, int max_entries) {
 }
 
 int pm3gpu_last_kernel_launches(pm3gpu_ctx* c) { return c ? c->launches : 0; }
+
+int pm3gpu_last_phase_cycles(pm3gpu_ctx* c, double* cycles, int max_entries) {
+  if (!c || !cycles) return 0;
+  const int k = std::min(max_entries, (int)kPhases);
+  for (int i = 0; i < k; ++i) cycles[i] = c->phase_cycles[i];
+  return c->profile ? k : 0;
+}
 
 int pm3gpu_last_transfer_bytes(pm3gpu_ctx* c, long long* h2d, long long* d2h) {
   if (!c) return PM3GPU_INVALID_INPUT;

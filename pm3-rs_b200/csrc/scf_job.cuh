@@ -6,109 +6,11 @@
 
 namespace pm3gpu {
 
-// Closed-form Hellmann-Feynman gradient at fixed densities (eV/Bohr), one thread per pair,
-// forward-mode dual numbers through every integral.
-__device__ void gradient_phase(Ctx& c, const double* Pt, const double* Pa, const double* Pb, double* gout) {
-  const KernelArgs& A = *c.A;
-  const int n = c.n, N = c.N, tid = threadIdx.x;
-  const bool uhf = Pb != nullptr;
-  double* g = c.jacc;  // [3N]
-  for (int k = tid; k < 3 * N; k += kThreads) g[k] = 0.0;
-  __syncthreads();
-  const int npairs = N * (N - 1) / 2;
-  for (int t = tid; t < npairs; t += kThreads) {
-    int u, v;
-    pair_uv(N, t, u, v);
-    const bool hu = heavy(c, u), hv = heavy(c, v);
-    const int a = (hu || !hv) ? u : v, b = a == u ? v : u;
-    const ElemDev& ea = A.elem[c.sz[a]];
-    const ElemDev& eb = A.elem[c.sz[b]];
-    const int na = ea.norb, nb = eb.norb, oa = c.soff[a], ob = c.soff[b];
-    const D3 dv[3] = {{c.sxyz[3 * b] - c.sxyz[3 * a], {1.0, 0.0, 0.0}},
-                      {c.sxyz[3 * b + 1] - c.sxyz[3 * a + 1], {0.0, 1.0, 0.0}},
-                      {c.sxyz[3 * b + 2] - c.sxyz[3 * a + 2], {0.0, 0.0, 1.0}}};
-    double f[3] = {0.0, 0.0, 0.0};
-    auto add = [&](double coef, const D3& x) {
-      f[0] = fma(coef, x.g[0], f[0]);
-      f[1] = fma(coef, x.g[1], f[1]);
-      f[2] = fma(coef, x.g[2], f[2]);
-    };
-    {  // resonance: sum P_ab (beta_i + beta_j) dS
-      D3 s[16];
-      overlap_block(ea, eb, dv, s);
-      for (int i = 0; i < na; ++i)
-        for (int j = 0; j < nb; ++j)
-          add(Pt[(size_t)(oa + i) * n + ob + j] * ((i ? ea.bp : ea.bs) + (j ? eb.bp : eb.bs)), s[i * 4 + j]);
-    }
-    {  // electron-core attraction
-      D3 blk[10];
-      core_attraction(ea, eb, dv, blk);
-      for (int i = 0; i < na; ++i)
-        for (int j = 0; j < na; ++j) add(Pt[(size_t)(oa + i) * n + oa + j], blk[pk(i, j)]);
-      const D3 mdv[3] = {-dv[0], -dv[1], -dv[2]};
-      core_attraction(eb, ea, mdv, blk);
-      for (int i = 0; i < nb; ++i)
-        for (int j = 0; j < nb; ++j) add(Pt[(size_t)(ob + i) * n + ob + j], blk[pk(i, j)]);
-    }
-    const D3 r = sq_rt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
-    {  // two-electron: (Coulomb - exchange) x dW
-      const D3 ir = inv(r);
-      D3 R[9];
-      frame(-(dv[0] * ir), -(dv[1] * ir), -(dv[2] * ir), R);
-      auto coef = [&](int p, int q) {  // sum over the unpacked index pairs of p and q
-        int ph, pl, qh, ql;
-        unpk(p, ph, pl);
-        unpk(q, qh, ql);
-        double s = 0.0;
-        for (int o1 = 0; o1 < (ph == pl ? 1 : 2); ++o1) {
-          const int mu = o1 ? pl : ph, nu = o1 ? ph : pl;
-          for (int o2 = 0; o2 < (qh == ql ? 1 : 2); ++o2) {
-            const int la = o2 ? ql : qh, si = o2 ? qh : ql;
-            const double coul = Pt[(size_t)(oa + mu) * n + oa + nu] * Pt[(size_t)(ob + la) * n + ob + si];
-            double exch;
-            if (uhf)
-              exch = -(Pa[(size_t)(oa + mu) * n + ob + la] * Pa[(size_t)(oa + nu) * n + ob + si] +
-                       Pb[(size_t)(oa + mu) * n + ob + la] * Pb[(size_t)(oa + nu) * n + ob + si]);
-            else
-              exch = -0.5 * Pt[(size_t)(oa + mu) * n + ob + la] * Pt[(size_t)(oa + nu) * n + ob + si];
-            s += coul + exch;
-          }
-        }
-        return s;
-      };
-      if (na == 1) {
-        const double sr = ea.rho0 + eb.rho0;
-        add(coef(0, 0), rsq(r * r + sr * sr) * kEv);
-      } else if (nb == 1) {
-        D3 ri[4];
-        local4(ee_pole(ea), eb.rho0, r, ri);
-        for (int kk = 0; kk < 4; ++kk)
-          for (int ll = 0; ll <= kk; ++ll) add(coef(pk(kk, ll), 0), w4(ri, R, kk, ll));
-      } else {
-        D3 ri[22];
-        local22(ee_pole(ea), ee_pole(eb), r, ri);
-        for (int kk = 0; kk < 4; ++kk)
-          for (int ll = 0; ll <= kk; ++ll)
-            for (int mm = 0; mm < 4; ++mm)
-              for (int nn = 0; nn <= mm; ++nn) add(coef(pk(kk, ll), pk(mm, nn)), w22(ri, R, kk, ll, mm, nn));
-      }
-    }
-    // core-core term (repulsion.rs:30-49): dE/dd along the same displacement
-    add(1.0, core_core(ea, eb, *A.pairs, r));
-    for (int ax = 0; ax < 3; ++ax) {
-      atomicAdd(&g[3 * b + ax], f[ax]);
-      atomicAdd(&g[3 * a + ax], -f[ax]);
-    }
-  }
-  __syncthreads();
-  for (int k = tid; k < 3 * N; k += kThreads) gout[k] = g[k];
-  __syncthreads();
-}
-
 // ------------------------------------------------------------------------------- one job
-__device__ void run_job(Ctx& c, int jid) {
+__device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
   const KernelArgs& A = *c.A;
-  c.job = A.jobs[jid];
+  c.job = job;
+  c.out = out;
   const JobDesc& J = c.job;
   c.n = J.nao;
   c.N = J.natom;
@@ -122,8 +24,10 @@ __device__ void run_job(Ctx& c, int jid) {
   o.iterations = 0;
   o.pad = 0;
 
+  c.tmark = clock64();
   setup_job(c);
   o.core = build_core(c);
+  mark(c, kPhCore);
   if (J.flags & (kJobCoreOnly | kJobFockOnly)) {
     double* io = A.densities + J.dens_off;
     if (J.flags & kJobCoreOnly) {
@@ -133,7 +37,7 @@ __device__ void run_job(Ctx& c, int jid) {
       else build_fock(c, io, nullptr, nullptr, io + 3 * nn, nullptr);
     }
     __syncthreads();
-    if (tid == 0) A.out[jid] = o;
+    if (tid == 0) *out = o;
     __syncthreads();
     return;
   }
@@ -212,6 +116,7 @@ __device__ void run_job(Ctx& c, int jid) {
       double part = 0.0;
       for (size_t k = tid; k < nn; k += kThreads) part = fma(Pc[k], c.H[k] + Fa[k], part);
       e_elec = 0.5 * block_sum(part, c.red);
+      mark(c, kPhFock);
     } else {
       double* Pt = c.Vb + nn;  // scratch right after Vb (slot reserves it)
       for (size_t k = tid; k < nn; k += kThreads) Pt[k] = Pc[k] + Qc[k];
@@ -220,6 +125,7 @@ __device__ void run_job(Ctx& c, int jid) {
       double part = 0.0;
       for (size_t k = tid; k < nn; k += kThreads) part += Pt[k] * c.H[k] + Pc[k] * Fa[k] + Qc[k] * Fb[k];
       e_elec = 0.5 * block_sum(part, c.red);
+      mark(c, kPhFock);
     }
 
     // ---- accelerator (scf.rs:1240-1259 RHF; 1398-1413 UHF)
@@ -230,6 +136,7 @@ __device__ void run_job(Ctx& c, int jid) {
       if (keep)
         for (size_t k = tid; k < nn; k += kThreads) Dh[k] = Pc[k];
       __syncthreads();
+      mark(c, kPhCommutator);
       // new Gram row against the surviving entries l < len, then the new diagonal
       double acc[3 * kMaxDepth + 2];
 #pragma unroll
@@ -279,6 +186,7 @@ __device__ void run_job(Ctx& c, int jid) {
       ++len;
       __syncthreads();
       use_hist = c.iv[0] != 0;
+      mark(c, kPhDiisSolve);
     }
 
     // ---- diagonalise (level shift for UHF only, scf.rs:1416-1418) and rebuild densities
@@ -312,9 +220,11 @@ __device__ void run_job(Ctx& c, int jid) {
         if (spin == 0) {
           eigensolve(c, Ap, kva, na, c.Vt, eps_a, c.tri_a);
           sq_a = density(c, c.Vt, na, uhf ? 1.0 : 2.0, Pc, Pn, uhf ? J.damping : 0.0);
+          mark(c, kPhDensity);
         } else {
           eigensolve(c, Ap, kvb, nb, c.Vb, eps_b, c.tri_b);
           sq_b = density(c, c.Vb, nb, 1.0, Qc, Qn, J.damping);
+          mark(c, kPhDensity);
         }
       }
     }
@@ -379,22 +289,36 @@ __device__ void run_job(Ctx& c, int jid) {
   o.gap = (o.has_homo && o.has_lumo) ? o.lumo - o.homo : INFINITY;
 
   properties(c, Pt, o);
-  if (J.flags & kJobDensity) {
+  if (J.flags & (kJobDensity | kJobGrad)) {
     double* dst = A.densities + J.dens_off;
     for (size_t k = tid; k < nn; k += kThreads) dst[k] = Pt[k];
+    if ((J.flags & kJobGrad) && uhf)
+      for (size_t k = tid; k < nn; k += kThreads) {
+        dst[nn + k] = Pf[k];
+        dst[2 * nn + k] = Qf[k];
+      }
   }
   if (J.flags & kJobEps) {
     all_eigenvalues(n, c.tri_a, c.tri_a + n, A.eps + J.eps_off, c.es);
     if (uhf) all_eigenvalues(n, c.tri_b, c.tri_b + n, A.eps + J.eps_off + n, c.es);
   }
-  if (J.flags & kJobGrad) gradient_phase(c, Pt, uhf ? Pf : nullptr, uhf ? Qf : nullptr, A.grads + J.grad_off);
   __syncthreads();
-  if (tid == 0) A.out[jid] = o;
+  mark(c, kPhFinal);
+  if (tid == 0) {
+    *out = o;
+    // stability search (scf.rs:599-715): queue this molecule's rungs for any free CTA
+    if (J.nrung > 0 && (J.stab == 2 || (J.stab == 1 && o.gap < 6.0))) {
+      const int base = atomicAdd(&A.queue[1], J.nrung);
+      for (int k = 0; k < J.nrung; ++k) A.rlist[base + k] = J.rung0 + k;
+      __threadfence();
+      for (int k = 0; k < J.nrung; ++k) atomicExch(&A.rready[base + k], 1);
+    }
+  }
   __syncthreads();
 }
 
 // ----------------------------------------------------------------------- the kernel
-__global__ void __launch_bounds__(kThreads, 1) scf_batch_kernel(KernelArgs args) {
+__global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_job;
   Ctx c;
@@ -458,14 +382,62 @@ __global__ void __launch_bounds__(kThreads, 1) scf_batch_kernel(KernelArgs args)
   c.tri_b = c.tri_a + 3 * args.nmax;
   c.W = c.tri_b + 3 * args.nmax;
 
+  __shared__ unsigned long long s_ph[kPhases];
+  c.ph = s_ph;
+  if (threadIdx.x < kPhases) s_ph[threadIdx.x] = 0ULL;
+  __syncthreads();
+  __shared__ int s_kind;
+  int* q = args.queue;
   for (;;) {
-    if (threadIdx.x == 0) s_job = atomicAdd(args.queue, 1);
+    if (threadIdx.x == 0) {
+      // Rung jobs first (they are the long ones and only exist once a first pass asked for
+      // them), else the next first-pass job. Every wait here is bounded; a handshake that
+      // times out raises the error flag instead of hanging.
+      int kind = -1, idx = -1;
+      bool first_done = false;
+      for (int guard = 0; guard < (1 << 20); ++guard) {
+        const int h = atomicAdd(&q[2], 0), t = atomicAdd(&q[1], 0);
+        if (h < t) {
+          if (atomicCAS(&q[2], h, h + 1) != h) continue;
+          bool ok = false;
+          for (int spin = 0; spin < (1 << 22); ++spin) {
+            if (atomicAdd(&args.rready[h], 0)) {
+              ok = true;
+              break;
+            }
+            __nanosleep(64);
+          }
+          if (ok) {
+            kind = 1;
+            idx = ((volatile int*)args.rlist)[h];
+          } else {
+            atomicExch(&q[3], 1);
+          }
+          break;
+        }
+        if (!first_done) {
+          const int j = atomicAdd(&q[0], 1);
+          if (j < args.njobs) {
+            kind = 0;
+            idx = j;
+            break;
+          }
+          first_done = true;
+          continue;
+        }
+        break;
+      }
+      s_kind = kind;
+      s_job = idx;
+    }
     __syncthreads();
-    const int jid = s_job;
+    const int kind = s_kind, jid = s_job;
     __syncthreads();
-    if (jid >= args.njobs) break;
-    run_job(c, jid);
+    if (kind < 0) break;
+    if (kind == 0) run_job(c, args.jobs[jid], args.out + jid);
+    else run_job(c, args.rjobs[jid], args.rout + jid);
   }
+  if (args.prof && threadIdx.x < kPhases) atomicAdd(&args.prof[threadIdx.x], s_ph[threadIdx.x]);
 }
 
 inline long long slot_doubles(int nmax, long long wcap) {

@@ -17,11 +17,16 @@
 namespace pm3gpu {
 
 constexpr int kMaxDepth = 8;  // deepest accelerator history (scf.rs:300)
+// Phases of one job, timed with clock64 by thread 0 when profiling is on.
+enum Phase : int {
+  kPhCore = 0, kPhFock, kPhCommutator, kPhDiisSolve, kPhPack, kPhTridiag, kPhEigval, kPhEigvec, kPhBack,
+  kPhDensity, kPhFinal, kPhGradient, kPhases
+};
 
 enum JobFlags : int {
   kJobUhf = 1,        // unrestricted iteration
   kJobKeepDens = 2,   // A-DIIS density history
-  kJobGrad = 4,       // compute the analytic gradient at the end
+  kJobGrad = 4,       // export the densities the gradient kernel needs (P, and Pa/Pb for UHF)
   kJobDensity = 8,    // export the total density
   kJobEps = 16,       // export all MO energies of the last iteration
   kJobCoreOnly = 32,  // stop after H_core: export H (build_core)
@@ -32,6 +37,9 @@ struct JobDesc {
   int atom0, natom, nao;
   int n_alpha, n_beta;
   int flags;
+  int mol;     // molecule index (host bookkeeping)
+  int rung0, nrung;  // stability-search jobs of this molecule in the rung table (first pass only)
+  int stab;    // 0 no search, 1 search when the frontier gap < 6 eV, 2 always (first pass only)
   int guess;   // 1 SAD, 2 core Hamiltonian, 3 symmetry-broken SAD
   int accel;   // 0 none, 1 CDIIS, 2 A-DIIS -> CDIIS (already combined with use_diis)
   int depth;   // accelerator history length
@@ -39,7 +47,7 @@ struct JobDesc {
   double e_tol, p_tol, adiis_switch, shift, damping;
   long long charge_off;   // into charges[] (natom values)
   long long dens_off;     // into densities[] (nao^2), when kJobDensity
-  long long grad_off;     // into grads[] (3 natom), when kJobGrad
+  long long grad_off;     // unused (the gradient kernel works from the exported densities)
   long long eps_off;      // into eps[] (2 nao: alpha then beta), when kJobEps
 };
 
@@ -69,9 +77,14 @@ struct KernelArgs {
   const PairDev* pairs;
   const int* z;          // [total atoms]
   const double* xyz;     // [3 * total atoms], Bohr
-  const JobDesc* jobs;
+  const JobDesc* jobs;   // first-pass jobs, largest first
   int njobs;
   JobOut* out;
+  const JobDesc* rjobs;  // stability-search rung table (all candidates)
+  int nrjobs;
+  JobOut* rout;          // status stays -1 for rungs that were never enqueued
+  int* rlist;            // [nrjobs] rung queue entries (rung table indices)
+  int* rready;           // [nrjobs] 1 once rlist[i] is published
   double* charges;
   double* densities;
   double* grads;
@@ -80,7 +93,8 @@ struct KernelArgs {
   long long slot;        // doubles per slot
   int nmax;              // largest nao of the launch (slot dimension)
   long long wcap;        // doubles reserved for the pair table
-  int* queue;            // [0] next job index
+  int* queue;            // [0] next first-pass job, [1] rung queue tail, [2] rung queue head, [3] error
+  unsigned long long* prof;  // [kPhases] SM cycles per phase, summed over CTAs (null = off)
   SmemLayout sm;
 };
 
@@ -102,6 +116,7 @@ __device__ __forceinline__ double oc_integral(const ElemDev& e, int a, int b, in
 struct Ctx {
   const KernelArgs* A;
   JobDesc job;
+  JobOut* out;
   int n, N;             // AOs, atoms
   // shared
   int* sz;              // [amax] Z of each atom
@@ -120,10 +135,20 @@ struct Ctx {
   double* tile;         // GEMM tiles
   double* Asm;          // packed matrix (eigen phase)
   EigenScratch es;
+  unsigned long long* ph;  // [kPhases] shared accumulators
+  long long tmark;
   // global (slot)
   double *H, *P[2], *Q[2], *F, *G, *Vt, *Vb, *Ag, *tf, *hist, *W, *tri_a, *tri_b;
   int cur;              // which P/Q buffer is current
 };
+
+__device__ __forceinline__ void mark(Ctx& c, int phase) {
+  if (c.A->prof && threadIdx.x == 0) {
+    const long long now = clock64();
+    c.ph[phase] += (unsigned long long)(now - c.tmark);
+    c.tmark = now;
+  }
+}
 
 __device__ __forceinline__ bool heavy(const Ctx& c, int a) { return c.A->elem[c.sz[a]].norb == 4; }
 __device__ __forceinline__ int psize(const Ctx& c, int a) { return heavy(c, a) ? 10 : 1; }
@@ -516,19 +541,24 @@ __device__ double* pack_input(Ctx& c, const double* X, const double* Pproj, doub
 // into Y (rows). The tridiagonal (d, e) is saved to `tri_save` (2n) for the final MO energies.
 __device__ void eigensolve(Ctx& c, double* Ap, int kval, int kvec, double* Y, double* lam_out, double* tri_save) {
   const int n = c.n;
+  mark(c, kPhPack);
   tridiagonalize(n, Ap, c.es);
   if (tri_save && threadIdx.x == 0)
     for (int i = 0; i < n; ++i) {
       tri_save[i] = c.es.d[i];
       tri_save[n + i] = c.es.e[i];
     }
+  mark(c, kPhTridiag);
   tridiag_eigenvalues(n, kval, c.es);
   for (int j = threadIdx.x; j < kval; j += kThreads) lam_out[j] = c.es.lam[j];
+  mark(c, kPhEigval);
   if (kvec > 0) {
     tridiag_vectors(n, kvec, Y, c.tf, c.es);
+    mark(c, kPhEigvec);
     back_transform(n, kvec, Ap, Y, c.es);
   }
   __syncthreads();
+  mark(c, kPhBack);
 }
 
 // Pnew = w Y^T Y (first k rows of Y); returns sum (Pnew - Pold)^2 to all threads. With

@@ -155,11 +155,16 @@ def test_generated_organics_batch_matches_oracle():
 
 
 def test_generated_radicals_batch_matches_oracle():
+    # unrestricted doublets iterate without an accelerator (scf.rs:1369-1374): give them room
     mols = workloads.radical_batch(16, 10, 40, seed=5)
     offs, z, xyz = workloads.pack(mols)
-    res = native.batch(offs, z, xyz * A2B, native.options(multiplicity=2))
+    res = native.batch(offs, z, xyz * A2B, native.options(multiplicity=2, max_scf=1000))
     for m, (zz, xx) in enumerate(mols):
-        ref = O.single_point(zz, xx * A2B, multiplicity=2)
+        try:
+            ref = O.single_point(zz, xx * A2B, multiplicity=2, max_scf=1000)
+        except O.OracleError as e:
+            assert e.code == 4 and res.status[m] == _lib.SCF_NOT_CONVERGED
+            continue
         assert res.status[m] == 0 and res.unrestricted[m]
         assert abs(res.heat_of_formation_kcal[m] - ref["heat_of_formation_kcal"]) < HOF_TOL
         assert np.abs(res.charges_of(m) - ref["charges"]).max() < Q_TOL
@@ -176,7 +181,7 @@ def test_water_cluster_34_matches_oracle():
 def test_gradient_matches_oracle_and_mopac():
     tight = dict(e_tol=1e-12, p_tol=1e-11)
     for geom, mult in ((WATER_GRAD_GEOM, 1), ("C 0.0 0.0 0.0; O 0.03 0.0 1.25; H 0.95 0.02 -0.55; H -0.94 -0.03 -0.52", 1),
-                       ("C 0.0 0.0 0.05; H 1.12 0.0 0.0; H -0.55 0.95 0.0; H -0.55 -0.95 0.0", 2), MIXED_GRAD):
+                       ("C 0.0 0.0 0.05; H 1.12 0.0 0.0; H -0.55 0.95 0.0; H -0.55 -0.95 0.0", 2), (MIXED_GRAD, 1)):
         z, xyz = parse(geom)
         ref = O.single_point(z, xyz * A2B, want_gradient=True, multiplicity=mult, **tight)
         got = native.run(z, xyz * A2B, native.options(multiplicity=mult, **tight), want_gradient=True)
@@ -205,7 +210,7 @@ def test_edge_cases_and_errors():
     r = native.run(np.array([1], np.int32), np.zeros((1, 3)), native.options(multiplicity=2))
     ref = O.single_point([1], np.zeros((1, 3)), multiplicity=2)
     assert abs(r["heat_of_formation_kcal"] - ref["heat_of_formation_kcal"]) < HOF_TOL
-    # H2+ (one electron), odd count with multiplicity 1 -> invalid
+    # OH with multiplicity 1: odd electron count -> invalid
     with pytest.raises(ValueError):
         native.run(np.array([8, 1], np.int32), np.array([[0, 0, 0], [1.8, 0, 0.0]]), native.options())
     with pytest.raises(ValueError):
