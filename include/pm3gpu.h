@@ -116,6 +116,34 @@ int pm3gpu_single_point(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const do
                         const pm3gpu_options* opts, pm3gpu_result* result, double* charges,
                         double* density, double* mo_energies);
 
+/* Size of the fixed device scratch array behind pm3gpu_single_point_noalloc. */
+#define PM3GPU_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+
+/* pm3gpu_single_point without any memory allocation in the call. It has no counterpart in the
+ * reference, which never runs on a device.
+ *
+ * Who needs it: a host program that already owns the device memory, such as a framework whose
+ * caching allocator has reserved most of HBM (there a library cudaMalloc can fail or force the
+ * cache to be released), or a per-step loop (molecular dynamics, geometry optimisation) that
+ * cannot pay for cudaMalloc/cudaFree in every step (cudaFree waits for the whole device). This
+ * call makes no cudaMalloc, cudaFree or other allocating call, neither does it grow the
+ * context's buffers: the SCF kernel's workspace, job table and outputs live in one
+ * PM3GPU_NOALLOC_SCRATCH_BYTES array of this library's own device image.
+ *
+ * Same inputs, options and results as pm3gpu_single_point (host arrays: z[n_atoms],
+ * xyz_bohr[3*n_atoms]; charges[n_atoms] out), without the density and MO-energy outputs.
+ * Limit: one SCF workspace slot must fit the scratch (about 190 basis functions, e.g. 40 heavy
+ * atoms with 30 hydrogens); larger molecules return PM3GPU_RESOURCE_LIMIT with the needed size.
+ * The stability-search rungs share the slots that fit and run one after another if only one does.
+ * The first call on each device looks up the array's address (and may load this library's device
+ * code), so make it before any stream capture begins. The caller clears nothing: each call resets
+ * the queue counters and flags it needs at zero itself. All contexts of a process on one device
+ * share the one array, so calls that overlap in time on that device (two contexts, or two
+ * threads on different contexts) race and give wrong results; calls through one context are
+ * serialised by the context. The call returns once its results are on the host. */
+int pm3gpu_single_point_noalloc(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const double* xyz_bohr,
+                                const pm3gpu_options* opts, pm3gpu_result* result, double* charges);
+
 /* One molecule: run_pm3 followed by the closed-form Hellmann-Feynman gradient
  * (gradient[3*n_atoms], eV/Bohr) at the converged density. */
 int pm3gpu_gradient(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const double* xyz_bohr,

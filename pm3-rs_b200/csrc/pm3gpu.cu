@@ -910,3 +910,259 @@ int pm3gpu_last_transfer_bytes(pm3gpu_ctx* c, long long* h2d, long long* d2h) {
 }
 
 }  // extern "C"
+
+// ===================================================================== allocation-free single point
+// pm3gpu_single_point_noalloc: the run_pm3 single point of pm3gpu_single_point (charges only),
+// with every device buffer the SCF kernel needs carved out of one fixed array of this library's
+// own device image instead of allocated. Layout of the array for one call (each region starts on a
+// 256-byte boundary):
+//   [queue: 16 ints][rung list + rung ready flags: 2 x 8 ints][job descriptors: 8]
+//   [job outcomes: 8][z: n_atoms int32][xyz: 3 n_atoms][charges: 8 x n_atoms][SCF workspace slots]
+// The queue counters and the rung ready flags must be zero when the kernel starts and the rung
+// outcomes must read status -1 ("not run"); each call writes both itself before its launch. Nothing
+// else in the array needs an initial value: the kernel writes every workspace element before it
+// reads it.
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[PM3GPU_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+constexpr int kNoAllocMaxJobs = 8;  // the first pass plus the at most seven stability rungs
+void* g_noalloc_base[kNoAllocMaxDevices] = {};
+std::mutex g_noalloc_setup_mu;
+
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Device address of the scratch array on the context's device (which must be current). Resolved
+// once per device and cached; the first resolution may also load this library's device code.
+int noalloc_scratch(pm3gpu_ctx* c, unsigned char** base) {
+  if (c->device < 0 || c->device >= kNoAllocMaxDevices)
+    return fail(c, PM3GPU_INVALID_INPUT, "device ordinal outside the allocation-free path's table");
+  std::lock_guard<std::mutex> lk(g_noalloc_setup_mu);
+  if (!g_noalloc_base[c->device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(c, PM3GPU_CUDA_ERROR,
+                  std::string("cudaGetSymbolAddress of the allocation-free scratch: ") + cudaGetErrorString(e));
+    g_noalloc_base[c->device] = p;
+  }
+  *base = static_cast<unsigned char*>(g_noalloc_base[c->device]);
+  return PM3GPU_OK;
+}
+
+int noalloc_run(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz, const pm3gpu_options* o,
+                pm3gpu_result* result, double* charges) {
+  std::memset(result, 0, sizeof(*result));
+  if (n_atoms < 1 || n_atoms > kMaxN)
+    return fail(c, PM3GPU_INVALID_INPUT, "atom count outside 1..256 for the allocation-free path");
+  MolPlan p;
+  plan_molecule(c, z, xyz, n_atoms, o, p);
+  result->nao = p.nao;
+  if (p.status != PM3GPU_OK) {
+    c->err = p.msg;
+    return p.status;
+  }
+  // the first pass and the stability rungs run_pm3 would try, in its order (scf.rs:599-715)
+  JobDesc jobs[kNoAllocMaxJobs];
+  Rung rungs[kNoAllocMaxJobs - 1];
+  int nr = 0;
+  jobs[0] = p.steered ? make_job(p, o->guess, o->accelerator, o->level_shift_ev, o->damping, false, 0)
+                      : make_job(p, o->guess, o->accelerator, 0.0, 0.0, false, 0);
+  JobDesc& fj = jobs[0];
+  fj.mol = 0;
+  fj.charge_off = 0;
+  fj.stab = 0;
+  if (o->stability == PM3GPU_STABILITY_ALWAYS && !p.steered) fj.stab = 2;
+  if (o->stability == PM3GPU_STABILITY_AUTO && !p.steered) fj.stab = 1;
+  if (fj.stab) {
+    const int primary = o->guess == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_CORE : PM3GPU_GUESS_SAD;
+    const int other = primary == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_SAD : PM3GPU_GUESS_CORE;
+    const bool closed = !p.use_uhf;
+    const Rung all[7] = {{primary, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                         {other, o->accelerator, 0.0, 0.0, false},
+                         {other, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                         {PM3GPU_GUESS_SYMMETRY_BROKEN, o->accelerator, 0.0, 0.0, false},
+                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, -2.0, 0.0, closed},
+                         {primary, PM3GPU_ACCEL_CDIIS, 0.0, 0.85, closed}};
+    for (const Rung& r : all) {
+      if (r.unrestricted != closed) continue;
+      JobDesc rj = make_job(p, r.guess, r.accel, r.shift, r.damp, r.unrestricted, 0);
+      rj.mol = 0;
+      rj.stab = 0;
+      rj.nrung = 0;
+      rj.charge_off = (long long)(1 + nr) * n_atoms;
+      rungs[nr] = r;
+      jobs[1 + nr] = rj;
+      ++nr;
+    }
+  }
+  fj.rung0 = 0;
+  fj.nrung = nr;
+  const int njobs = 1 + nr;
+
+  // carve the scratch array
+  const size_t off_queue = 0;
+  const size_t off_rq = off_queue + 256;
+  const size_t off_jobs = off_rq + 256;
+  const size_t off_out = off_jobs + round256(sizeof(JobDesc) * kNoAllocMaxJobs);
+  const size_t off_z = off_out + round256(sizeof(JobOut) * kNoAllocMaxJobs);
+  const size_t off_xyz = off_z + round256(4 * (size_t)n_atoms);
+  const size_t off_q = off_xyz + round256(24 * (size_t)n_atoms);
+  const size_t off_work = off_q + round256(8 * (size_t)kNoAllocMaxJobs * n_atoms);
+  const long long wcap = std::max(1LL, pair_table_doubles(c, z, n_atoms));
+  const long long slot = (slot_doubles(p.nao, wcap) + 31) & ~31LL;  // 256-byte aligned slots
+  const size_t slot_bytes = 8 * (size_t)slot;
+  const size_t room = PM3GPU_NOALLOC_SCRATCH_BYTES > off_work ? PM3GPU_NOALLOC_SCRATCH_BYTES - off_work : 0;
+  if (slot_bytes > room) {
+    char msg[200];
+    std::snprintf(msg, sizeof msg,
+                  "molecule (nao=%d) needs %zu bytes of SCF workspace; the allocation-free path's fixed scratch "
+                  "has %zu bytes for it (%d MiB in total)",
+                  p.nao, slot_bytes, room, (int)(PM3GPU_NOALLOC_SCRATCH_BYTES >> 20));
+    return fail(c, PM3GPU_RESOURCE_LIMIT, msg);
+  }
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(c, &base);
+  if (rc != PM3GPU_OK) return rc;
+
+  const SmemLayout L = make_layout(n_atoms, p.nao, c->smem_optin);
+  CUDA_TRY(c, cudaFuncSetAttribute(scf_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes));
+  int per_sm = 0;
+  CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scf_batch_kernel, kThreads, L.bytes));
+  if (per_sm < 1) return fail(c, PM3GPU_RESOURCE_LIMIT, "SCF kernel does not fit on an SM");
+  long long grid = std::min<long long>(njobs, (long long)(room / slot_bytes));
+  grid = std::min<long long>(grid, (long long)c->sms * per_sm);
+
+  int* d_queue = reinterpret_cast<int*>(base + off_queue);
+  int* d_rq = reinterpret_cast<int*>(base + off_rq);
+  JobDesc* d_jobs = reinterpret_cast<JobDesc*>(base + off_jobs);
+  JobOut* d_out = reinterpret_cast<JobOut*>(base + off_out);
+  int32_t* d_z = reinterpret_cast<int32_t*>(base + off_z);
+  double* d_xyz = reinterpret_cast<double*>(base + off_xyz);
+  double* d_q = reinterpret_cast<double*>(base + off_q);
+  CUDA_TRY(c, cudaMemcpyAsync(d_z, z, 4 * (size_t)n_atoms, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(d_xyz, xyz, 24 * (size_t)n_atoms, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(d_jobs, jobs, sizeof(JobDesc) * njobs, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(d_queue, 0, 512, c->stream));  // queue counters, rung list and flags
+  if (nr) CUDA_TRY(c, cudaMemsetAsync(d_out + 1, 0xff, sizeof(JobOut) * nr, c->stream));
+
+  KernelArgs a{};
+  a.elem = c->elem.as<ElemDev>();
+  a.pairs = c->pairs.as<PairDev>();
+  a.z = d_z;
+  a.xyz = d_xyz;
+  a.jobs = d_jobs;
+  a.njobs = 1;
+  a.out = d_out;
+  a.rjobs = d_jobs + 1;
+  a.nrjobs = nr;
+  a.rout = d_out + 1;
+  a.rlist = d_rq;
+  a.rready = d_rq + kNoAllocMaxJobs;
+  a.charges = d_q;
+  a.densities = nullptr;
+  a.grads = nullptr;
+  a.eps = nullptr;
+  a.work = reinterpret_cast<double*>(base + off_work);
+  a.slot = slot;
+  a.nmax = p.nao;
+  a.wcap = wcap;
+  a.queue = d_queue;
+  a.prof = nullptr;
+  a.sm = L;
+  c->launches = 0;
+  scf_batch_kernel<<<(unsigned)grid, kThreads, L.bytes, c->stream>>>(a);
+  c->launches = 1;
+  CUDA_TRY(c, cudaGetLastError());
+  int qh[4] = {0, 0, 0, 0};
+  JobOut outs[kNoAllocMaxJobs];
+  CUDA_TRY(c, cudaMemcpyAsync(qh, d_queue, sizeof(qh), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(outs, d_out, sizeof(JobOut) * njobs, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (qh[3]) return fail(c, PM3GPU_CUDA_ERROR, "stability-search queue handshake timed out on the device");
+
+  // run_pm3's selection among the first pass and the rungs (scf.rs:680-715)
+  JobOut st = outs[0];
+  int st_job = 0;
+  bool st_unres = (fj.flags & kJobUhf) != 0;
+  const double first_ev = st.electronic;
+  int paths = 1;
+  const bool searched = nr > 0 && outs[1].status != -1;
+  for (int r = 0; searched && r < nr; ++r) {
+    ++paths;
+    JobOut cand = outs[1 + r];
+    bool cand_unres = (jobs[1 + r].flags & kJobUhf) != 0;
+    if (!cand.converged) continue;
+    if (rungs[r].unrestricted) {  // a spin-pure unrestricted closed shell is a restricted state
+      if (!(cand.spin_max < 1.0e-8)) continue;
+      cand_unres = false;
+      cand.homo = cand.homo_a;
+      cand.lumo = cand.lumo_a;
+      cand.has_homo = cand.has_homo_a;
+      cand.has_lumo = cand.has_lumo_a;
+    }
+    if (!st.converged || cand.electronic < st.electronic - 1.0e-6) {
+      st = cand;
+      st_job = 1 + r;
+      st_unres = cand_unres;
+    }
+  }
+  CUDA_TRY(c, cudaMemcpyAsync(charges, d_q + (size_t)st_job * n_atoms, 8 * (size_t)n_atoms, cudaMemcpyDeviceToHost,
+                              c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->h2d = (long long)(28 * (size_t)n_atoms + sizeof(JobDesc) * njobs);
+  c->d2h = (long long)(sizeof(qh) + sizeof(JobOut) * njobs + 8 * (size_t)n_atoms);
+
+  double e_isol = 0.0, eheat = 0.0;
+  for (int k = 0; k < n_atoms; ++k) {
+    e_isol += c->h_elem[z[k]].e_isol;
+    eheat += c->h_elem[z[k]].eheat_ev;
+  }
+  pm3gpu_result& Rm = *result;
+  Rm.status = PM3GPU_OK;
+  Rm.n_occ = p.n_alpha;
+  Rm.n_beta = st_unres ? p.n_beta : p.n_alpha;
+  Rm.electronic_ev = st.electronic;
+  Rm.core_ev = st.core;
+  Rm.total_ev = st.electronic + st.core;
+  Rm.heat_of_formation_kcal = (Rm.total_ev - e_isol + eheat) * kEvToKcal;
+  Rm.iterations = st.iterations;
+  Rm.converged = st.converged;
+  Rm.unrestricted = st_unres ? 1 : 0;
+  Rm.scf_paths_tried = paths;
+  Rm.scf_improvement_ev = std::max(first_ev - st.electronic, 0.0);
+  Rm.last_change = st.last_change;
+  Rm.homo_ev = st.homo;
+  Rm.lumo_ev = st.lumo;
+  Rm.has_homo = st.has_homo;
+  Rm.has_lumo = st.has_lumo;
+  for (int k = 0; k < 3; ++k) Rm.dipole_debye[k] = st.dipole[k];
+  Rm.dipole_magnitude = std::sqrt(Rm.dipole_debye[0] * Rm.dipole_debye[0] + Rm.dipole_debye[1] * Rm.dipole_debye[1] +
+                                  Rm.dipole_debye[2] * Rm.dipole_debye[2]);
+  if (!st.converged) {
+    Rm.status = PM3GPU_SCF_NOT_CONVERGED;
+    char msg[160];
+    std::snprintf(msg, sizeof msg, "PM3 SCF did not converge after %d iterations (error=%.3e)", st.iterations,
+                  st.last_change);
+    c->err = msg;
+  }
+  return Rm.status;
+}
+
+}  // namespace
+
+extern "C" int pm3gpu_single_point_noalloc(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz,
+                                           const pm3gpu_options* opts, pm3gpu_result* result, double* charges) {
+  if (!c || !z || !xyz || !result || !charges) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  c->err.clear();
+  pm3gpu_options d;
+  pm3gpu_default_options(&d);
+  const int rc = noalloc_run(c, n_atoms, z, xyz, opts ? opts : &d, result, charges);
+  if (rc != PM3GPU_OK && result->status == PM3GPU_OK) result->status = rc;
+  return rc;
+}

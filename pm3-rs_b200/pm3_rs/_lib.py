@@ -68,6 +68,7 @@ EXPORTS = [
     "pm3gpu_set_stream", "pm3gpu_single_point", "pm3gpu_gradient", "pm3gpu_batch",
     "pm3gpu_batch_device_inputs", "pm3gpu_core_hamiltonian", "pm3gpu_fock", "pm3gpu_last_timings",
     "pm3gpu_last_kernel_launches", "pm3gpu_last_transfer_bytes", "pm3gpu_last_phase_cycles",
+    "pm3gpu_single_point_noalloc",
 ]
 
 _lib = None
@@ -97,6 +98,8 @@ def load() -> ctypes.CDLL:
     L.pm3gpu_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     L.pm3gpu_single_point.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, ctypes.POINTER(Options),
                                       ctypes.POINTER(Result), _D, _D, _D]
+    L.pm3gpu_single_point_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, ctypes.POINTER(Options),
+                                              ctypes.POINTER(Result), _D]
     L.pm3gpu_gradient.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, ctypes.POINTER(Options),
                                   ctypes.POINTER(Result), _D, _D]
     L.pm3gpu_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, ctypes.POINTER(Options), ctypes.c_int,
