@@ -2,8 +2,10 @@
 // `self_adjoint_eigen` (pm3-rs src/linalg.rs:221-263) on the SCF path:
 //   1. Householder reduction to tridiagonal form, the matrix held as a packed lower triangle
 //      (row-major: element (r, c), r >= c, at r(r+1)/2 + c) in shared memory (or global memory
-//      when it does not fit). Reflectors stay in the strictly-lower part of column i.
-//   2. Eigenvalues of the tridiagonal T by Sturm-count bisection, one thread per eigenvalue.
+//      when it does not fit), one thread per row. Reflectors stay in the strictly-lower part
+//      of column i.
+//   2. Eigenvalues of the tridiagonal T by Sturm-count multisection, a group of lanes per
+//      eigenvalue, started from the previous SCF iteration's eigenvalues when given.
 //   3. Eigenvectors of T by twisted (N_r D_r N_r^T) factorisation, one thread per vector,
 //      on the unreduced block holding the eigenvalue (T is split where |e_i| <= 1000 eps ||T||,
 //      which separates exact degeneracies); members of a within-block cluster (gap below
@@ -38,64 +40,93 @@ struct EigenScratch {
 };
 
 // ---------------------------------------------------------------- 1. tridiagonalisation
-__device__ void tridiagonalize(int n, double* A, const EigenScratch& s) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+// Sum over the CTA with one barrier: `red` holds two alternating kWarps buffers, so a call may
+// overwrite the buffer two calls back without waiting (the previous call's barrier separates them).
+__device__ __forceinline__ double block_sum_alt(double v, double* red, int& parity) {
+  v = warp_sum(v);
+  double* buf = red + parity * kWarps;
+  parity ^= 1;
+  if ((threadIdx.x & 31) == 0) buf[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+#pragma unroll
+  for (int i = 0; i < kWarps; ++i) t += buf[i];
+  return t;
+}
+
+// Householder reduction, one thread per row (n <= kThreads): thread r owns row r of the packed
+// lower triangle for the matrix-vector product (its row segment plus the column below it) and
+// for the rank-2 update of its row segment, and contributes its element of the next column to
+// the next reflector's norm. Three barriers per column.
+__device__ void tridiagonalize(int n, double* __restrict__ A, const EigenScratch& s_) {
+  // scratch pointers in registers: the stores below go through generic pointers, which
+  // would otherwise force the struct to be re-read after every store
+  struct {
+    double *v, *p, *red, *tau, *e, *d;
+  } s = {s_.v, s_.p, s_.red, s_.tau, s_.e, s_.d};
+  const int r = threadIdx.x;
+  int parity = 0;
+  const int tr = r < n ? tri(r) : 0;
+  double xn2 = block_sum_alt(r >= 2 && r < n ? A[tr] * A[tr] : 0.0, s.red, parity);
   for (int i = 0; i + 2 < n; ++i) {
-    // x = A[i+1.., i]; annihilate A[i+2.., i]
-    double part = 0.0;
-    for (int r = i + 2 + tid; r < n; r += kThreads) {
-      const double x = A[tri(r) + i];
-      part += x * x;
-    }
-    const double xn2 = block_sum(part, s.red);
     const double alpha = A[tri(i + 1) + i];
-    double beta = 0.0, tau = 0.0, scal = 0.0;
+    double beta = alpha, tau = 0.0, scal = 0.0;
     if (xn2 > 0.0) {
       beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
       tau = (beta - alpha) / beta;
       scal = 1.0 / (alpha - beta);
     }
-    if (tid == 0) {
+    if (r == 0) {
       s.tau[i] = tau;
-      s.e[i] = xn2 > 0.0 ? beta : alpha;
+      s.e[i] = beta;
       s.d[i] = A[tri(i) + i];
     }
-    if (xn2 == 0.0) {  // already reduced: nothing to apply (uniform branch)
-      __syncthreads();
+    if (xn2 == 0.0) {  // column already reduced (uniform): only the next norm is needed
+      xn2 = block_sum_alt(r >= i + 3 && r < n ? A[tr + i + 1] * A[tr + i + 1] : 0.0, s.red, parity);
       continue;
     }
-    for (int r = i + 1 + tid; r < n; r += kThreads) {
-      double vr = 1.0;
+    const bool mine = r > i && r < n;
+    double vr = 0.0;
+    if (mine) {
+      vr = 1.0;
       if (r > i + 1) {
-        vr = A[tri(r) + i] * scal;
-        A[tri(r) + i] = vr;
+        vr = A[tr + i] * scal;
+        A[tr + i] = vr;
       }
       s.v[r] = vr;
     }
     __syncthreads();
-    // p = tau * A22 v (A22 = A[i+1.., i+1..]); warp per row, lanes across the row
-    double dpart = 0.0;
-    for (int r = i + 1 + warp; r < n; r += kWarps) {
-      double acc = 0.0;
-      for (int c = i + 1 + lane; c < n; c += 32) acc = fma(ap_get(A, r, c), s.v[c], acc);
-      acc = warp_sum(acc) * tau;
-      if (lane == 0) s.p[r] = acc;
-      dpart = fma(acc, s.v[r], dpart);
+    // y_r = sum_c A(r, c) v_c over c > i: row segment (c <= r), then the column below r
+    double y = 0.0;
+    if (mine) {
+      double y2 = 0.0;
+      int c = i + 1;
+      for (; c + 1 <= r; c += 2) {
+        y = fma(A[tr + c], s.v[c], y);
+        y2 = fma(A[tr + c + 1], s.v[c + 1], y2);
+      }
+      if (c <= r) y = fma(A[tr + c], s.v[c], y);
+      for (int q = r + 1, idx = tri(r + 1) + r; q < n; idx += q + 1, ++q) y2 = fma(A[idx], s.v[q], y2);
+      y = tau * (y + y2);
+      s.p[r] = y;
     }
-    const double dot = block_sum(lane == 0 ? dpart : 0.0, s.red);
-    const double a2 = -0.5 * tau * dot;
-    // A22 -= v w^T + w v^T with w = p + a2 v
-    for (int r = i + 1 + warp; r < n; r += kWarps) {
-      const double vr = s.v[r], wr = s.p[r] + a2 * vr;
-      double* row = A + tri(r);
-      for (int c = i + 1 + lane; c <= r; c += 32) {
+    const double a2 = -0.5 * tau * block_sum_alt(mine ? y * vr : 0.0, s.red, parity);
+    // A22 -= v w^T + w v^T on row r (w = p + a2 v), keeping the next column's norm part
+    double part = 0.0;
+    if (mine) {
+      const double wr = y + a2 * vr;
+      for (int c = i + 1; c <= r; ++c) {
         const double vc = s.v[c], wc = s.p[c] + a2 * vc;
-        row[c] -= vr * wc + wr * vc;
+        A[tr + c] -= vr * wc + wr * vc;
+      }
+      if (r >= i + 3) {
+        const double x = A[tr + i + 1];
+        part = x * x;
       }
     }
-    __syncthreads();
+    xn2 = block_sum_alt(part, s.red, parity);
   }
-  if (tid == 0) {
+  if (r == 0) {
     if (n >= 2) {
       s.d[n - 2] = A[tri(n - 2) + n - 2];
       s.e[n - 2] = A[tri(n - 1) + n - 2];
@@ -123,8 +154,15 @@ __device__ __forceinline__ int sturm(const double* d, const double* e2, int lo, 
 }
 
 // Splits T where the coupling is negligible and computes the lowest `kval` eigenvalues.
-// Leaves pivmin / tnorm in misc[0] / misc[1].
-__device__ void tridiag_eigenvalues(int n, int kval, const EigenScratch& s) {
+// Leaves pivmin / tnorm in misc[0] / misc[1]. With `prev` (the same eigenvalues of the
+// previous SCF iteration) and `dprev` (their last change) the search starts from a bracket
+// around prev[j] once Sturm counts confirm it.
+__device__ void tridiag_eigenvalues(int n, int kval, const EigenScratch& s_, const double* prev = nullptr,
+                                    const double* dprev = nullptr) {
+  struct {
+    double *d, *e, *e2, *misc, *lam;
+    int *blk, *nblk;
+  } s = {s_.d, s_.e, s_.e2, s_.misc, s_.lam, s_.blk, s_.nblk};
   const int tid = threadIdx.x;
   constexpr double eps = 2.220446049250313e-16;
   if (tid == 0) {
@@ -160,17 +198,73 @@ __device__ void tridiag_eigenvalues(int n, int kval, const EigenScratch& s) {
     s.misc[3] = gu + 4.0 * eps * tnorm * n + 1.0e-300;
   }
   __syncthreads();
-  const double pivmin = s.misc[0], glo = s.misc[2], ghi = s.misc[3];
-  for (int j = tid; j < kval; j += kThreads) {
+  const double pivmin = s.misc[0], tnorm = s.misc[1], glo = s.misc[2], ghi = s.misc[3];
+  // Multisection: a group of g lanes (a power of two, g <= 32, kval * g <= kThreads) brackets
+  // one eigenvalue; each step the g lanes take Sturm counts at g interior points, which cuts
+  // the bracket by g + 1 instead of 2. Invariant: count(lo) <= j < count(hi).
+  int g = 1;
+  while (g < 32 && kval * (2 * g) <= kThreads) g *= 2;
+  const int lane = tid & 31;
+  const int gbase = lane & ~(g - 1), gl = lane & (g - 1);
+  const unsigned gbits = g == 32 ? 0xffffffffu : ((1u << g) - 1u);
+  for (int j0 = 0; j0 < kval; j0 += kThreads / g) {
+    const int j = j0 + tid / g;
+    const bool active = j < kval;
     double lo = glo, hi = ghi;
-    for (int it = 0; it < 128; ++it) {
-      const double mid = 0.5 * (lo + hi);
-      if (mid <= lo || mid >= hi) break;
-      if (hi - lo <= 2.0 * eps * fmax(fabs(lo), fabs(hi)) + 4.0 * pivmin) break;
-      if (sturm(s.d, s.e2, 0, n - 1, mid, pivmin) > j) hi = mid;
-      else lo = mid;
+    if (prev) {
+      // warm bracket around the previous SCF iteration's value, widened until two Sturm
+      // counts confirm that it holds eigenvalue j (else the Gershgorin interval stays)
+      const double c0 = active ? prev[j] : 0.0;
+      double w = active ? fmax(4.0 * fabs(dprev[j]), 1.0e-9 * fmax(tnorm, 1.0)) : 0.0;
+      bool found = !active;
+      for (int tr = 0; tr < 3; ++tr) {
+        const double a = fmax(c0 - w, glo), b = fmin(c0 + w, ghi);
+        int ca, cb;
+        if (g == 1) {
+          ca = found ? 0 : sturm(s.d, s.e2, 0, n - 1, a, pivmin);
+          cb = found ? 0 : sturm(s.d, s.e2, 0, n - 1, b, pivmin);
+        } else {
+          const int cnt = found ? 0 : sturm(s.d, s.e2, 0, n - 1, gl == 0 ? a : b, pivmin);
+          ca = __shfl_sync(0xffffffffu, cnt, gbase);
+          cb = __shfl_sync(0xffffffffu, cnt, gbase + 1);
+        }
+        if (!found && a < b && ca <= j && cb >= j + 1) {
+          lo = a;
+          hi = b;
+          found = true;
+        }
+        w *= 64.0;
+      }
     }
-    s.lam[j] = 0.5 * (lo + hi);
+    bool act = active;
+    for (int it = 0; it < 128; ++it) {
+      if (act) {
+        const double mid = 0.5 * (lo + hi);
+        if (hi - lo <= 2.0 * eps * fmax(fabs(lo), fabs(hi)) + 4.0 * pivmin || !(mid > lo && mid < hi)) act = false;
+      }
+      if (!__any_sync(0xffffffffu, act)) break;
+      const double x = lo + (hi - lo) * (double)(gl + 1) / (double)(g + 1);
+      const int cnt = act ? sturm(s.d, s.e2, 0, n - 1, x, pivmin) : 0;
+      const unsigned bal = __ballot_sync(0xffffffffu, act && cnt > j);
+      const unsigned mine = (bal >> gbase) & gbits;
+      if (act) {
+        double nlo, nhi;
+        if (mine == 0u) {  // every point is at or below eigenvalue j
+          nlo = lo + (hi - lo) * (double)g / (double)(g + 1);
+          nhi = hi;
+        } else {
+          const int f = __ffs(mine) - 1;  // first point above it
+          nlo = f > 0 ? lo + (hi - lo) * (double)f / (double)(g + 1) : lo;
+          nhi = lo + (hi - lo) * (double)(f + 1) / (double)(g + 1);
+        }
+        if (!(nhi - nlo < hi - lo)) act = false;
+        else {
+          lo = nlo;
+          hi = nhi;
+        }
+      }
+    }
+    if (active && gl == 0) s.lam[j] = 0.5 * (lo + hi);
   }
   __syncthreads();
 }
@@ -178,7 +272,12 @@ __device__ void tridiag_eigenvalues(int n, int kval, const EigenScratch& s) {
 // ------------------------------------------------------------- 3. tridiagonal eigenvectors
 // Eigenvector j (< kvec) of T into Y[j*n .. j*n+n) (zero outside its block). `tf` is per-CTA
 // global scratch of kvec * 6n doubles.
-__device__ void tridiag_vectors(int n, int kvec, double* Y, double* tf, const EigenScratch& s) {
+__device__ void tridiag_vectors(int n, int kvec, double* Y, double* tf, const EigenScratch& s_) {
+  struct {
+    const double *d, *e, *e2, *lam, *misc;
+    const int *blk, *nblk;
+    int* vinfo;
+  } s = {s_.d, s_.e, s_.e2, s_.lam, s_.misc, s_.blk, s_.nblk, s_.vinfo};
   const int tid = threadIdx.x;
   const double pivmin = s.misc[0], tnorm = s.misc[1];
   const int nb = *s.nblk;
@@ -341,7 +440,8 @@ __device__ void tridiag_vectors(int n, int kvec, double* Y, double* tf, const Ei
 
 // ------------------------------------------------------------------- 4. back-transform
 // Y[j] <- H(0) H(1) ... H(n-3) Y[j] for j < kvec, two vectors per warp held in registers.
-__device__ void back_transform(int n, int kvec, const double* A, double* Y, const EigenScratch& s) {
+__device__ void back_transform(int n, int kvec, const double* __restrict__ A, double* Y, const EigenScratch& s_) {
+  const double* __restrict__ tau_ = s_.tau;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int j0 = 2 * warp; j0 < kvec; j0 += 2 * kWarps) {
     const bool two = j0 + 1 < kvec;
@@ -355,7 +455,7 @@ __device__ void back_transform(int n, int kvec, const double* A, double* Y, cons
       z1[t] = r < n ? y1[r] : 0.0;
     }
     for (int i = n - 3; i >= 0; --i) {
-      const double tau = s.tau[i];
+      const double tau = tau_[i];
       if (tau == 0.0) continue;
       double a0 = 0.0, a1 = 0.0;
 #pragma unroll

@@ -80,7 +80,7 @@ struct pm3gpu_ctx {
   ElemDev h_elem[kMaxZ];
   PairDev h_pairs;
   DevBuf elem, pairs, z, xyz, jobs, out, charges, dens, grads, eps, work, queue, rq, gmols, aooff;
-  int sms = 0, smem_optin = 0;
+  int sms = 0, smem_optin = 0, smem_per_sm = 0;
   double timings[6] = {0, 0, 0, 0, 0, 0};
   int launches = 0;
   long long h2d = 0, d2h = 0;  // bytes moved by the last call
@@ -223,7 +223,10 @@ long long pair_table_doubles(const pm3gpu_ctx* c, const int32_t* z, int natom) {
   return (s * s - s2) / 2;
 }
 
-SmemLayout make_layout(int amax, int nmax, int optin) {
+// Shared-memory carve-up of one launch. The packed eigen input lives in shared memory for
+// bases up to `nsm` (global memory above). When `naos` is given, the layout is shrunk to let
+// two CTAs share an SM as long as at least 90% of the launch's jobs still fit in shared memory.
+SmemLayout make_layout(int amax, int nmax, int optin, int smem_per_sm = 0, const std::vector<int>* naos = nullptr) {
   SmemLayout L{};
   L.amax = amax;
   auto align = [](int b) { return (b + 15) & ~15; };
@@ -233,13 +236,24 @@ SmemLayout make_layout(int amax, int nmax, int optin) {
   L.off_dbl = off;
   off += align(amax * 8 + (3 * amax + 4 * kMaxDepth * kWarps + 4 * kMaxDepth + 2 * kMaxDepth * kMaxDepth + kMaxDepth + 8) * 8);
   L.off_eig = off;
-  off += align(7 * kMaxN * 8 + (2 * kMaxN + 2) * 4);
+  off += align(7 * nmax * 8 + (2 * nmax + 2) * 4);
   L.off_union = off;
   const int fixed_union = std::max(20 * amax, 2 * 16 * 65);
-  int nsm = nmax;
-  for (; nsm > 0; --nsm) {
-    const int need = std::max(fixed_union, nsm * (nsm + 1) / 2) * 8;
-    if (off + need <= optin) break;
+  auto fit = [&](int budget) {
+    int nsm = nmax;
+    for (; nsm > 0; --nsm)
+      if (off + std::max(fixed_union, nsm * (nsm + 1) / 2) * 8 <= budget) break;
+    return nsm;
+  };
+  int nsm = fit(optin);
+  if (smem_per_sm > 0 && naos && !naos->empty()) {
+    const int budget2 = smem_per_sm / 2 - 1024 - 512;  // per-CTA reservation and static shared memory
+    const int nsm2 = fit(budget2);
+    if (nsm2 < nsm && off + fixed_union * 8 <= budget2) {
+      size_t inside = 0;
+      for (int v : *naos) inside += v <= nsm2;
+      if (inside * 10 >= naos->size() * 9) nsm = nsm2;
+    }
   }
   L.nsm = nsm;
   L.bytes = off + std::max(fixed_union, nsm * (nsm + 1) / 2) * 8;
@@ -288,13 +302,16 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   if (nj == 0) return PM3GPU_OK;
   int nmax = 1, amax = 1;
   long long wcap = 1;
+  std::vector<int> naos;
+  naos.reserve(jobs.size());
   for (const std::vector<JobDesc>* L : {&jobs, &rjobs})
     for (const JobDesc& j : *L) {
       nmax = std::max(nmax, j.nao);
       amax = std::max(amax, j.natom);
       wcap = std::max(wcap, pair_table_doubles(c, zs.data() + j.atom0, j.natom));
     }
-  const SmemLayout L = make_layout(amax, nmax, c->smem_optin);
+  for (const JobDesc& j : jobs) naos.push_back(j.nao);
+  const SmemLayout L = make_layout(amax, nmax, c->smem_optin, c->smem_per_sm, &naos);
   CUDA_TRY(c, cudaFuncSetAttribute(scf_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes));
   int per_sm = 0;
   CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scf_batch_kernel, kThreads, L.bytes));
@@ -703,6 +720,7 @@ int pm3gpu_context_create(int device, pm3gpu_ctx** out) {
   if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) return bail(e);
   c->sms = prop.multiProcessorCount;
   c->smem_optin = (int)prop.sharedMemPerBlockOptin;
+  c->smem_per_sm = (int)prop.sharedMemPerMultiprocessor;
   derive_elements(c->h_elem, &c->h_pairs);
   {
     const char* pe = std::getenv("PM3GPU_PROFILE");

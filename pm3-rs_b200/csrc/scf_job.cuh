@@ -175,16 +175,22 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
         const int m = len + 1;
         const double err = sqrt(c.misc[3 * kMaxDepth]);
         bool ok;
+        int mode = 0;
         if (!uhf && J.accel == 2 && err > J.adiis_switch) {
           ok = keep && m >= 2;
-          if (ok) adiis_coeffs(m, c.mg, c.coef);
+          mode = ok ? 1 : 0;  // A-DIIS weights: solved by warp 0 below
         } else {
           ok = cdiis_coeffs(m, c.bg, c.coef);
         }
         c.iv[0] = ok ? 1 : 0;
+        c.iv[1] = mode;
       }
       ++len;
       __syncthreads();
+      if (c.iv[1] == 1) {  // uniform across the CTA
+        if (tid < 32) adiis_coeffs_warp(len, c.mg, c.coef, c.red);
+        __syncthreads();
+      }
       use_hist = c.iv[0] != 0;
       mark(c, kPhDiisSolve);
     }
@@ -194,6 +200,9 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
     {
       double* Ap = n <= A.sm.nsm ? c.Asm : c.Ag;
       const int nt = n * (n + 1) / 2;
+      const double* __restrict__ coef = c.coef;
+      const double* __restrict__ hist = c.hist;
+      const double shift = J.shift;
       for (int spin = 0; spin < (uhf ? 2 : 1); ++spin) {
         const double* Pproj = spin == 0 ? Pc : Qc;
         const double* Fnew = spin == 0 ? Fa : Fb;
@@ -207,22 +216,22 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
           if (use_hist) {
             v = 0.0;
             for (int l = 0; l < len; ++l) {
-              const double* bl = c.hist + (size_t)((head + l) % depth) * slot_mats * nn;
-              v = fma(c.coef[l], bl[(spin == 0 ? 0 : 2 * nn) + ix], v);
+              const double* bl = hist + (size_t)((head + l) % depth) * slot_mats * nn;
+              v = fma(coef[l], bl[(spin == 0 ? 0 : 2 * nn) + ix], v);
             }
           } else {
             v = Fnew[ix];
           }
-          if (uhf && J.shift != 0.0) v += J.shift * ((r == col ? 1.0 : 0.0) - Pproj[ix]);
+          if (uhf && shift != 0.0) v += shift * ((r == col ? 1.0 : 0.0) - Pproj[ix]);
           Ap[k] = v;
         }
         __syncthreads();
         if (spin == 0) {
-          eigensolve(c, Ap, kva, na, c.Vt, eps_a, c.tri_a);
+          eigensolve(c, Ap, kva, na, c.Vt, eps_a, c.tri_a, iter > 0, c.tri_a + 3 * n);
           sq_a = density(c, c.Vt, na, uhf ? 1.0 : 2.0, Pc, Pn, uhf ? J.damping : 0.0);
           mark(c, kPhDensity);
         } else {
-          eigensolve(c, Ap, kvb, nb, c.Vb, eps_b, c.tri_b);
+          eigensolve(c, Ap, kvb, nb, c.Vb, eps_b, c.tri_b, iter > 0, c.tri_b + 3 * n);
           sq_b = density(c, c.Vb, nb, 1.0, Qc, Qn, J.damping);
           mark(c, kPhDensity);
         }
@@ -345,19 +354,20 @@ __global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args)
   dp += kMaxDepth * kMaxDepth;
   c.coef = dp;
   double* ep = reinterpret_cast<double*>(smem + L.off_eig);
+  const int nm = args.nmax;  // eigen scratch sized for the largest basis of the launch
   c.es.d = ep;
-  c.es.e = ep + kMaxN;
-  c.es.e2 = ep + 2 * kMaxN;
-  c.es.tau = ep + 3 * kMaxN;
-  c.es.v = ep + 4 * kMaxN;
-  c.es.p = ep + 5 * kMaxN;
-  c.es.lam = ep + 6 * kMaxN;
+  c.es.e = ep + nm;
+  c.es.e2 = ep + 2 * nm;
+  c.es.tau = ep + 3 * nm;
+  c.es.v = ep + 4 * nm;
+  c.es.p = ep + 5 * nm;
+  c.es.lam = ep + 6 * nm;
   c.es.red = c.red;
   c.es.misc = c.misc;
-  int* eip = reinterpret_cast<int*>(ep + 7 * kMaxN);
+  int* eip = reinterpret_cast<int*>(ep + 7 * nm);
   c.es.blk = eip;
-  c.es.nblk = eip + kMaxN + 1;
-  c.es.vinfo = eip + kMaxN + 2;
+  c.es.nblk = eip + nm + 1;
+  c.es.vinfo = eip + nm + 2;
   double* up = reinterpret_cast<double*>(smem + L.off_union);
   c.dpk = up;
   c.jacc = up + 10 * amax;
@@ -379,8 +389,8 @@ __global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args)
   c.tf = slot + 11 * nn;     // 6 nn: eigenvector scratch
   c.hist = slot + 17 * nn;   // 32 nn: accelerator history
   c.tri_a = slot + 49 * nn;
-  c.tri_b = c.tri_a + 3 * args.nmax;
-  c.W = c.tri_b + 3 * args.nmax;
+  c.tri_b = c.tri_a + 4 * args.nmax;  // per spin: saved tridiagonal (2n), eigenvalues (n), their change (n)
+  c.W = c.tri_b + 4 * args.nmax;
 
   __shared__ unsigned long long s_ph[kPhases];
   c.ph = s_ph;
@@ -442,7 +452,7 @@ __global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args)
 
 inline long long slot_doubles(int nmax, long long wcap) {
   const long long nn = (long long)nmax * nmax;
-  return 49 * nn + 6LL * nmax + wcap + 64;
+  return 49 * nn + 8LL * nmax + wcap + 64;
 }
 
 }  // namespace pm3gpu

@@ -271,6 +271,64 @@ __device__ double build_core(Ctx& c) {
 }
 
 // ------------------------------------------------------------------------ Fock build
+// Two-centre part of one atom pair (fock.rs:106-193): Coulomb sums into the atoms' packed
+// accumulators and the exchange block F_ab = H_ab - K_ab, written to both triangles. NA / NB are
+// the orbital counts of atom a (the heavier one) and b, so every loop has a fixed trip count and
+// every array stays in registers. W is the pair's (PA x PB) row-major integral block.
+template <int NA, int NB, bool UHF>
+__device__ __forceinline__ void fock_pair(int n, int a, int b, int oa, int ob, const double* __restrict__ dpk,
+                                          double* jacc, const double* __restrict__ H, const double* __restrict__ w,
+                                          const double* Pt, const double* Pa, const double* Pb, double* F, double* G) {
+  constexpr int PA = NA == 4 ? 10 : 1, PB = NB == 4 ? 10 : 1;
+  {  // Coulomb: J_a[p] += sum_q W[p][q] Pb_q, J_b[q] += sum_p Pa_p W[p][q]
+    double db[PB], jb[PB];
+#pragma unroll
+    for (int q = 0; q < PB; ++q) {
+      db[q] = dpk[b * 10 + q];
+      jb[q] = 0.0;
+    }
+#pragma unroll
+    for (int p = 0; p < PA; ++p) {
+      const double da = dpk[a * 10 + p];
+      double acc = 0.0;
+#pragma unroll
+      for (int q = 0; q < PB; ++q) {
+        const double wv = w[p * PB + q];
+        acc = fma(db[q], wv, acc);
+        jb[q] = fma(da, wv, jb[q]);
+      }
+      atomicAdd(&jacc[a * 10 + p], acc);
+    }
+#pragma unroll
+    for (int q = 0; q < PB; ++q) atomicAdd(&jacc[b * 10 + q], jb[q]);
+  }
+  // exchange: K[mu][la] = sum_{nu, si} X[nu][si] (mu nu | la si), one spin at a time
+#pragma unroll
+  for (int spin = 0; spin < (UHF ? 2 : 1); ++spin) {
+    const double* X = UHF ? (spin == 0 ? Pa : Pb) : Pt;
+    const double xs = UHF ? 1.0 : 0.5;
+    double* out = spin == 0 ? F : G;
+    double x[NA * NB];
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+      for (int j = 0; j < NB; ++j) x[i * NB + j] = xs * X[(size_t)(oa + i) * n + ob + j];
+#pragma unroll
+    for (int mu = 0; mu < NA; ++mu)
+#pragma unroll
+      for (int la = 0; la < NB; ++la) {
+        double k = 0.0;
+#pragma unroll
+        for (int nu = 0; nu < NA; ++nu)
+#pragma unroll
+          for (int si = 0; si < NB; ++si) k = fma(x[nu * NB + si], w[pk(mu, nu) * PB + pk(la, si)], k);
+        const double f = H[(size_t)(oa + mu) * n + ob + la] - k;
+        out[(size_t)(oa + mu) * n + ob + la] = f;
+        out[(size_t)(ob + la) * n + oa + mu] = f;
+      }
+  }
+}
+
 // F = H + J(Pt) - K(Ps) (fock.rs:285-332). Pt = total density; for RHF Ps = Pt/2 (pb == null),
 // for UHF two spin Focks F (from Pa) and G (from Pb) are built in one pass.
 __device__ void build_fock(Ctx& c, const double* Pt, const double* Pa, const double* Pb, double* F, double* G) {
@@ -294,70 +352,33 @@ __device__ void build_fock(Ctx& c, const double* Pt, const double* Pa, const dou
   }
   __syncthreads();
   const int npairs = N * (N - 1) / 2;
-  for (int t = tid; t < npairs; t += kThreads) {
-    int u, v;
-    pair_uv(N, t, u, v);
-    const bool hu = heavy(c, u), hv = heavy(c, v);
-    const int a = (hu || !hv) ? u : v, b = a == u ? v : u;
-    const int na = A.elem[c.sz[a]].norb, nb = A.elem[c.sz[b]].norb;
-    const int pa = na == 4 ? 10 : 1, pb = nb == 4 ? 10 : 1;
-    const int oa = c.soff[a], ob = c.soff[b];
-    const double* w = c.W + woff(c, u, v);
-    double Xa[16], Xb[16];  // exchange densities of the (a, b) block
-    for (int i = 0; i < na; ++i)
-      for (int j = 0; j < nb; ++j) {
-        if (uhf) {
-          Xa[i * 4 + j] = Pa[(size_t)(oa + i) * n + ob + j];
-          Xb[i * 4 + j] = Pb[(size_t)(oa + i) * n + ob + j];
-        } else {
-          Xa[i * 4 + j] = 0.5 * Pt[(size_t)(oa + i) * n + ob + j];
-        }
-      }
-    double jb[10], Ka[16], Kb[16];
-    for (int q = 0; q < 10; ++q) jb[q] = 0.0;
-    for (int q = 0; q < 16; ++q) {
-      Ka[q] = 0.0;
-      Kb[q] = 0.0;
-    }
-    for (int p = 0; p < pa; ++p) {
-      double wr[10];
-      for (int q = 0; q < pb; ++q) wr[q] = w[p * pb + q];
-      const double da = c.dpk[a * 10 + p];
-      double acc = 0.0;
-      for (int q = 0; q < pb; ++q) {
-        acc = fma(c.dpk[b * 10 + q], wr[q], acc);
-        jb[q] = fma(da, wr[q], jb[q]);
-      }
-      atomicAdd(&c.jacc[a * 10 + p], acc);
-      int hi, lo;
-      unpk(p, hi, lo);
-      for (int o = 0; o < (hi == lo ? 1 : 2); ++o) {
-        const int mu = o == 0 ? hi : lo, nu = o == 0 ? lo : hi;
-        for (int la = 0; la < nb; ++la) {
-          double ka = 0.0, kb = 0.0;
-          for (int si = 0; si < nb; ++si) {
-            const double wv = wr[pk(la, si)];
-            ka = fma(Xa[nu * 4 + si], wv, ka);
-            if (uhf) kb = fma(Xb[nu * 4 + si], wv, kb);
-          }
-          Ka[mu * 4 + la] += ka;
-          Kb[mu * 4 + la] += kb;
-        }
+  {
+    const int* __restrict__ sprow = c.sprow;
+    const int* __restrict__ soff = c.soff;
+    const long long* __restrict__ sroff = c.sroff;
+    const double* __restrict__ W = c.W;
+    const double* __restrict__ H = c.H;
+    const double* __restrict__ dpk = c.dpk;
+    double* jacc = c.jacc;
+    for (int t = tid; t < npairs; t += kThreads) {
+      int u, v;
+      pair_uv(N, t, u, v);
+      const int su = sprow[u + 1] - sprow[u], sv = sprow[v + 1] - sprow[v];  // packed sizes: 10 sp, 1 s
+      const bool hu = su == 10, hv = sv == 10;
+      const int a = (hu || !hv) ? u : v, b = a == u ? v : u;
+      const double* w = W + sroff[u] + (long long)su * (sprow[v] - sprow[u + 1]);
+      const int oa = soff[a], ob = soff[b];
+      if (hu && hv) {
+        if (uhf) fock_pair<4, 4, true>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+        else fock_pair<4, 4, false>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+      } else if (hu || hv) {
+        if (uhf) fock_pair<4, 1, true>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+        else fock_pair<4, 1, false>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+      } else {
+        if (uhf) fock_pair<1, 1, true>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+        else fock_pair<1, 1, false>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
       }
     }
-    for (int q = 0; q < pb; ++q) atomicAdd(&c.jacc[b * 10 + q], jb[q]);
-    for (int i = 0; i < na; ++i)
-      for (int j = 0; j < nb; ++j) {
-        const double h = c.H[(size_t)(oa + i) * n + ob + j];
-        const double fa = h - Ka[i * 4 + j];
-        F[(size_t)(oa + i) * n + ob + j] = fa;
-        F[(size_t)(ob + j) * n + oa + i] = fa;
-        if (uhf) {
-          const double fb = h - Kb[i * 4 + j];
-          G[(size_t)(oa + i) * n + ob + j] = fb;
-          G[(size_t)(ob + j) * n + oa + i] = fb;
-        }
-      }
   }
   __syncthreads();
   // atom-diagonal blocks: H + one-centre J - K + two-centre J
@@ -467,15 +488,23 @@ __device__ bool cdiis_coeffs(int m, const double* gram, double* x) {
   return true;
 }
 
-// A-DIIS weights on the simplex by projected gradient (scf.rs:1152-1172, 1637-1693).
-__device__ void adiis_coeffs(int m, const double* mg, double* c) {
+// A-DIIS weights on the simplex by projected gradient (scf.rs:1152-1172, 1637-1693), one warp:
+// lane k owns weight c_k and its gradient component; the Euclidean projection onto the simplex
+// sorts the trial point (descending, ties by index, as a stable insertion sort does) and every
+// lane runs the reference's serial cumulative-sum scan over the sorted values, so the weights are
+// the ones the serial loop produces. `sm` is shared scratch of kMaxDepth * (kMaxDepth + 1) doubles.
+__device__ void adiis_coeffs_warp(int m, const double* mg, double* out, double* sm) {
+  const int k = threadIdx.x & 31;
   const int last = m - 1;
   const double mnn = mg[last * kMaxDepth + last];
-  double d[kMaxDepth], S[kMaxDepth * kMaxDepth];
-  for (int i = 0; i < m; ++i) d[i] = mg[i * kMaxDepth + last] - mnn;
-  for (int i = 0; i < m; ++i)
+  double* S = sm;                       // [kMaxDepth][kMaxDepth]
+  double* d = sm + kMaxDepth * kMaxDepth;  // [kMaxDepth]
+  if (k < m) {
+    d[k] = mg[k * kMaxDepth + last] - mnn;
     for (int j = 0; j < m; ++j)
-      S[i * kMaxDepth + j] = mg[i * kMaxDepth + j] - mg[i * kMaxDepth + last] - mg[last * kMaxDepth + j] + mnn;
+      S[k * kMaxDepth + j] = mg[k * kMaxDepth + j] - mg[k * kMaxDepth + last] - mg[last * kMaxDepth + j] + mnn;
+  }
+  __syncwarp();
   double L = 1.0e-12;
   for (int i = 0; i < m; ++i) {
     double row = 0.0;
@@ -483,39 +512,39 @@ __device__ void adiis_coeffs(int m, const double* mg, double* c) {
     L = fmax(L, row);
   }
   const double lr = 1.0 / L;
-  for (int i = 0; i < m; ++i) c[i] = i == last ? 1.0 : 0.0;
+  double ck = k == last ? 1.0 : 0.0;
   for (int it = 0; it < 400; ++it) {
-    double tr[kMaxDepth], u[kMaxDepth];
-    for (int k = 0; k < m; ++k) {
+    double tr = 0.0;
+    if (k < m) {
       double g = 2.0 * d[k];
-      for (int j = 0; j < m; ++j) g += (S[k * kMaxDepth + j] + S[j * kMaxDepth + k]) * c[j];
-      tr[k] = c[k] - lr * g;
-      u[k] = tr[k];
+      for (int j = 0; j < m; ++j) g += (S[k * kMaxDepth + j] + S[j * kMaxDepth + k]) * __shfl_sync(0xffffffffu, ck, j);
+      tr = ck - lr * g;
+    } else {
+      for (int j = 0; j < m; ++j) (void)__shfl_sync(0xffffffffu, ck, j);
     }
-    // sort descending (insertion sort, stable)
-    for (int i = 1; i < m; ++i) {
-      const double key = u[i];
-      int j = i - 1;
-      while (j >= 0 && u[j] < key) {
-        u[j + 1] = u[j];
-        --j;
-      }
-      u[j + 1] = key;
+    // rank of tr_k in descending order (ties: lower index first)
+    int rank = 0;
+    for (int j = 0; j < m; ++j) {
+      const double tj = __shfl_sync(0xffffffffu, tr, j);
+      rank += (tj > tr || (tj == tr && j < k)) ? 1 : 0;
     }
     double css = 0.0, theta = 0.0;
-    for (int j = 0; j < m; ++j) {
-      css += u[j];
-      const double t = (css - 1.0) / (double)(j + 1);
-      if (u[j] - t > 0.0) theta = t;
+    for (int p = 0; p < m; ++p) {
+      const unsigned who = __ballot_sync(0xffffffffu, k < m && rank == p);
+      const double up = __shfl_sync(0xffffffffu, tr, __ffs(who) - 1);
+      css += up;
+      const double t = (css - 1.0) / (double)(p + 1);
+      if (up - t > 0.0) theta = t;
     }
+    const double pk = k < m ? fmax(tr - theta, 0.0) : 0.0;
+    const double dk = k < m ? fabs(pk - ck) : 0.0;
     double delta = 0.0;
-    for (int i = 0; i < m; ++i) {
-      const double p = fmax(tr[i] - theta, 0.0);
-      delta += fabs(p - c[i]);
-      c[i] = p;
-    }
+    for (int i = 0; i < m; ++i) delta += __shfl_sync(0xffffffffu, dk, i);
+    ck = pk;
     if (delta < 1.0e-12) break;
   }
+  if (k < m) out[k] = ck;
+  __syncwarp();
 }
 
 // ------------------------------------------------------------------- eigensolve + density
@@ -539,7 +568,10 @@ __device__ double* pack_input(Ctx& c, const double* X, const double* Pproj, doub
 
 // Diagonalise the packed matrix: kval lowest eigenvalues into lam_out, kvec eigenvectors
 // into Y (rows). The tridiagonal (d, e) is saved to `tri_save` (2n) for the final MO energies.
-__device__ void eigensolve(Ctx& c, double* Ap, int kval, int kvec, double* Y, double* lam_out, double* tri_save) {
+// With `warm`, lam_out holds the same eigenvalues from the previous SCF iteration and `dlam`
+// their last change; both seed the eigenvalue search and are updated. Without it dlam is reset.
+__device__ void eigensolve(Ctx& c, double* Ap, int kval, int kvec, double* Y, double* lam_out, double* tri_save,
+                           bool warm = false, double* dlam = nullptr) {
   const int n = c.n;
   mark(c, kPhPack);
   tridiagonalize(n, Ap, c.es);
@@ -549,8 +581,12 @@ __device__ void eigensolve(Ctx& c, double* Ap, int kval, int kvec, double* Y, do
       tri_save[n + i] = c.es.e[i];
     }
   mark(c, kPhTridiag);
-  tridiag_eigenvalues(n, kval, c.es);
-  for (int j = threadIdx.x; j < kval; j += kThreads) lam_out[j] = c.es.lam[j];
+  const bool seeded = warm && dlam != nullptr;
+  tridiag_eigenvalues(n, kval, c.es, seeded ? lam_out : nullptr, seeded ? dlam : nullptr);
+  for (int j = threadIdx.x; j < kval; j += kThreads) {
+    if (dlam) dlam[j] = seeded ? c.es.lam[j] - lam_out[j] : 1.0e30;
+    lam_out[j] = c.es.lam[j];
+  }
   mark(c, kPhEigval);
   if (kvec > 0) {
     tridiag_vectors(n, kvec, Y, c.tf, c.es);
