@@ -96,18 +96,31 @@ __device__ void tridiagonalize(int n, double* __restrict__ A, const EigenScratch
       s.v[r] = vr;
     }
     __syncthreads();
-    // y_r = sum_c A(r, c) v_c over c > i: row segment (c <= r), then the column below r
+    // y_r = sum_c A(r, c) v_c over c > i: row segment (c <= r), then the column below r;
+    // four independent accumulators keep several shared-memory loads in flight
     double y = 0.0;
     if (mine) {
-      double y2 = 0.0;
+      double y0 = 0.0, y1 = 0.0, y2 = 0.0, y3 = 0.0;
+      const double* row = A + tr;
       int c = i + 1;
-      for (; c + 1 <= r; c += 2) {
-        y = fma(A[tr + c], s.v[c], y);
-        y2 = fma(A[tr + c + 1], s.v[c + 1], y2);
+      for (; c + 3 <= r; c += 4) {
+        y0 = fma(row[c], s.v[c], y0);
+        y1 = fma(row[c + 1], s.v[c + 1], y1);
+        y2 = fma(row[c + 2], s.v[c + 2], y2);
+        y3 = fma(row[c + 3], s.v[c + 3], y3);
       }
-      if (c <= r) y = fma(A[tr + c], s.v[c], y);
-      for (int q = r + 1, idx = tri(r + 1) + r; q < n; idx += q + 1, ++q) y2 = fma(A[idx], s.v[q], y2);
-      y = tau * (y + y2);
+      for (; c <= r; ++c) y0 = fma(row[c], s.v[c], y0);
+      int q = r + 1, idx = tri(r + 1) + r;
+      for (; q + 3 < n; q += 4) {
+        const int i1 = idx + q + 1, i2 = i1 + q + 2, i3 = i2 + q + 3;
+        y0 = fma(A[idx], s.v[q], y0);
+        y1 = fma(A[i1], s.v[q + 1], y1);
+        y2 = fma(A[i2], s.v[q + 2], y2);
+        y3 = fma(A[i3], s.v[q + 3], y3);
+        idx = i3 + q + 4;
+      }
+      for (; q < n; idx += q + 1, ++q) y1 = fma(A[idx], s.v[q], y1);
+      y = tau * ((y0 + y1) + (y2 + y3));
       s.p[r] = y;
     }
     const double a2 = -0.5 * tau * block_sum_alt(mine ? y * vr : 0.0, s.red, parity);
@@ -115,12 +128,24 @@ __device__ void tridiagonalize(int n, double* __restrict__ A, const EigenScratch
     double part = 0.0;
     if (mine) {
       const double wr = y + a2 * vr;
-      for (int c = i + 1; c <= r; ++c) {
+      double* row = A + tr;
+      int c = i + 1;
+      for (; c + 3 <= r; c += 4) {
+        const double v0 = s.v[c], v1 = s.v[c + 1], v2 = s.v[c + 2], v3 = s.v[c + 3];
+        const double w0 = s.p[c] + a2 * v0, w1 = s.p[c + 1] + a2 * v1, w2 = s.p[c + 2] + a2 * v2,
+                     w3 = s.p[c + 3] + a2 * v3;
+        const double a0 = row[c], a1 = row[c + 1], a2_ = row[c + 2], a3 = row[c + 3];
+        row[c] = a0 - (vr * w0 + wr * v0);
+        row[c + 1] = a1 - (vr * w1 + wr * v1);
+        row[c + 2] = a2_ - (vr * w2 + wr * v2);
+        row[c + 3] = a3 - (vr * w3 + wr * v3);
+      }
+      for (; c <= r; ++c) {
         const double vc = s.v[c], wc = s.p[c] + a2 * vc;
-        A[tr + c] -= vr * wc + wr * vc;
+        row[c] -= vr * wc + wr * vc;
       }
       if (r >= i + 3) {
-        const double x = A[tr + i + 1];
+        const double x = row[i + 1];
         part = x * x;
       }
     }
@@ -151,6 +176,61 @@ __device__ __forceinline__ int sturm(const double* d, const double* e2, int lo, 
     cnt += q < 0.0;
   }
   return cnt;
+}
+
+// Sturm counts at M shifts at once, without divisions (see the ratio form above for the
+// reference recurrence): p_i = (d_i - x) p_{i-1} - e_{i-1}^2 p_{i-2}; sign changes between
+// consecutive values count the eigenvalues below x. Pairs are rescaled by powers of two every
+// 8 steps (each step grows |p| by far less than 2^32 for the matrices here), exact for ratios.
+template <int M>
+__device__ __forceinline__ void sturm_multi(const double* __restrict__ d, const double* __restrict__ e2, int n,
+                                            const double (&x)[M], double pivmin, int (&cnt)[M]) {
+  (void)pivmin;
+  constexpr double kBig = 0x1p256, kSmall = 0x1p-256;
+  double p[M], pm[M];
+  unsigned sg[M];
+#pragma unroll
+  for (int t = 0; t < M; ++t) {
+    pm[t] = 1.0;
+    p[t] = d[0] - x[t];
+    sg[t] = __double_as_longlong(p[t]) < 0 ? 1u : 0u;
+    cnt[t] = (int)sg[t];
+  }
+  int i = 1;
+  for (; i + 8 <= n; i += 8) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const double di = d[i + u], ei = e2[i + u - 1];
+#pragma unroll
+      for (int t = 0; t < M; ++t) {
+        const double pn = fma(di - x[t], p[t], -ei * pm[t]);
+        const unsigned s = __double_as_longlong(pn) < 0 ? 1u : 0u;
+        cnt[t] += (int)(s ^ sg[t]);
+        sg[t] = s;
+        pm[t] = p[t];
+        p[t] = pn;
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < M; ++t) {
+      const double m = fmax(fabs(p[t]), fabs(pm[t]));
+      const double sc = m > kBig ? kSmall : (m < kSmall ? kBig : 1.0);
+      p[t] *= sc;
+      pm[t] *= sc;
+    }
+  }
+  for (; i < n; ++i) {
+    const double di = d[i], ei = e2[i - 1];
+#pragma unroll
+    for (int t = 0; t < M; ++t) {
+      const double pn = fma(di - x[t], p[t], -ei * pm[t]);
+      const unsigned s = __double_as_longlong(pn) < 0 ? 1u : 0u;
+      cnt[t] += (int)(s ^ sg[t]);
+      sg[t] = s;
+      pm[t] = p[t];
+      p[t] = pn;
+    }
+  }
 }
 
 // Splits T where the coupling is negligible and computes the lowest `kval` eigenvalues.
@@ -200,10 +280,13 @@ __device__ void tridiag_eigenvalues(int n, int kval, const EigenScratch& s_, con
   __syncthreads();
   const double pivmin = s.misc[0], tnorm = s.misc[1], glo = s.misc[2], ghi = s.misc[3];
   // Multisection: a group of g lanes (a power of two, g <= 32, kval * g <= kThreads) brackets
-  // one eigenvalue; each step the g lanes take Sturm counts at g interior points, which cuts
-  // the bracket by g + 1 instead of 2. Invariant: count(lo) <= j < count(hi).
+  // one eigenvalue; each step the group takes Sturm counts at P = g * kPts interior points (kPts
+  // per lane, evaluated together), which cuts the bracket by P + 1 instead of 2.
+  // Invariant: count(lo) <= j < count(hi).
+  constexpr int kPts = 2;
   int g = 1;
   while (g < 32 && kval * (2 * g) <= kThreads) g *= 2;
+  const int P = g * kPts;
   const int lane = tid & 31;
   const int gbase = lane & ~(g - 1), gl = lane & (g - 1);
   const unsigned gbits = g == 32 ? 0xffffffffu : ((1u << g) - 1u);
@@ -215,25 +298,23 @@ __device__ void tridiag_eigenvalues(int n, int kval, const EigenScratch& s_, con
       // warm bracket around the previous SCF iteration's value, widened until two Sturm
       // counts confirm that it holds eigenvalue j (else the Gershgorin interval stays)
       const double c0 = active ? prev[j] : 0.0;
-      double w = active ? fmax(4.0 * fabs(dprev[j]), 1.0e-9 * fmax(tnorm, 1.0)) : 0.0;
-      bool found = !active;
-      for (int tr = 0; tr < 3; ++tr) {
-        const double a = fmax(c0 - w, glo), b = fmin(c0 + w, ghi);
-        int ca, cb;
-        if (g == 1) {
-          ca = found ? 0 : sturm(s.d, s.e2, 0, n - 1, a, pivmin);
-          cb = found ? 0 : sturm(s.d, s.e2, 0, n - 1, b, pivmin);
-        } else {
-          const int cnt = found ? 0 : sturm(s.d, s.e2, 0, n - 1, gl == 0 ? a : b, pivmin);
-          ca = __shfl_sync(0xffffffffu, cnt, gbase);
-          cb = __shfl_sync(0xffffffffu, cnt, gbase + 1);
+      const double w0 = active ? fmax(4.0 * fabs(dprev[j]), 1.0e-9 * fmax(tnorm, 1.0)) : 0.0;
+      double x[4];
+      int cn[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {  // brackets w0 and 64 w0: lower ends on even t, upper on odd
+        const double w = w0 * (t >= 2 ? 64.0 : 1.0);
+        x[t] = (t & 1) ? fmin(c0 + w, ghi) : fmax(c0 - w, glo);
+      }
+      if (active) sturm_multi<4>(s.d, s.e2, n, x, pivmin, cn);
+      if (active) {
+        if (x[0] < x[1] && cn[0] <= j && cn[1] >= j + 1) {
+          lo = x[0];
+          hi = x[1];
+        } else if (x[2] < x[3] && cn[2] <= j && cn[3] >= j + 1) {
+          lo = x[2];
+          hi = x[3];
         }
-        if (!found && a < b && ca <= j && cb >= j + 1) {
-          lo = a;
-          hi = b;
-          found = true;
-        }
-        w *= 64.0;
       }
     }
     bool act = active;
@@ -243,19 +324,28 @@ __device__ void tridiag_eigenvalues(int n, int kval, const EigenScratch& s_, con
         if (hi - lo <= 2.0 * eps * fmax(fabs(lo), fabs(hi)) + 4.0 * pivmin || !(mid > lo && mid < hi)) act = false;
       }
       if (!__any_sync(0xffffffffu, act)) break;
-      const double x = lo + (hi - lo) * (double)(gl + 1) / (double)(g + 1);
-      const int cnt = act ? sturm(s.d, s.e2, 0, n - 1, x, pivmin) : 0;
-      const unsigned bal = __ballot_sync(0xffffffffu, act && cnt > j);
+      double x[kPts];
+      int cn[kPts];
+#pragma unroll
+      for (int t = 0; t < kPts; ++t) x[t] = lo + (hi - lo) * (double)(gl * kPts + t + 1) / (double)(P + 1);
+      if (act) sturm_multi<kPts>(s.d, s.e2, n, x, pivmin, cn);
+      int tf = kPts;  // this lane's first point above eigenvalue j
+#pragma unroll
+      for (int t = kPts - 1; t >= 0; --t)
+        if (act && cn[t] > j) tf = t;
+      const unsigned bal = __ballot_sync(0xffffffffu, act && tf < kPts);
       const unsigned mine = (bal >> gbase) & gbits;
+      const int src = mine ? gbase + __ffs(mine) - 1 : gbase;
+      const int tsrc = __shfl_sync(0xffffffffu, tf, src);
       if (act) {
         double nlo, nhi;
         if (mine == 0u) {  // every point is at or below eigenvalue j
-          nlo = lo + (hi - lo) * (double)g / (double)(g + 1);
+          nlo = lo + (hi - lo) * (double)P / (double)(P + 1);
           nhi = hi;
         } else {
-          const int f = __ffs(mine) - 1;  // first point above it
-          nlo = f > 0 ? lo + (hi - lo) * (double)f / (double)(g + 1) : lo;
-          nhi = lo + (hi - lo) * (double)(f + 1) / (double)(g + 1);
+          const int f = (src - gbase) * kPts + tsrc;  // first point above it
+          nlo = f > 0 ? lo + (hi - lo) * (double)f / (double)(P + 1) : lo;
+          nhi = lo + (hi - lo) * (double)(f + 1) / (double)(P + 1);
         }
         if (!(nhi - nlo < hi - lo)) act = false;
         else {
