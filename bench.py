@@ -166,6 +166,14 @@ def fp64_gemm_peak(dev):
     return best
 
 
+PHASES = ["core", "fock", "commutator", "diis_solve", "pack", "tridiagonalise", "eigenvalues", "eigenvectors",
+          "back_transform", "density", "final", "gradient"]
+# DRAM bytes (read + write) of one scf_batch_kernel launch per molecule of this workload, from an
+# ncu capture of a 256-molecule batch (7.43 GB); the per-CTA workspaces of 296 resident CTAs
+# exceed L2, so the SCF matrices stream from HBM. Scaled to a launch by the molecules it solves.
+DRAM_BYTES_PER_MOLECULE = 7.43e9 / 256
+
+
 def scf_flops(nao, n_occ, iters):
     """Algorithmic FP64 flops of the dense SCF algebra per molecule: per iteration
     tridiagonalisation 4/3 n^3 + back-transformation 2 n^3 + commutator 2 n^3 + density
@@ -183,7 +191,12 @@ def main():
     ap.add_argument("--n-mol", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--phases", action="store_true",
+                    help="after the timed steps, run one more (untimed) batch with per-phase SM-cycle counters "
+                         "and print the phase shares to stderr")
     args = ap.parse_args()
+    if args.phases:
+        os.environ["PM3GPU_PROFILE"] = "1"
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -334,11 +347,19 @@ def main():
         "e2e": {"value": e2e, "unit": "SCF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": DRAM_BYTES_PER_MOLECULE * n_mol,
                      "kernel": "scf_batch_kernel", "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run",
                      "flops_per_step": flops / args.steps, "kernel_ms_per_step": kern_ms / args.steps},
         "clocks": clocks,
     }
+    if args.phases:
+        run_device()
+        cyc = (ctypes.c_double * 16)()
+        k = lib.pm3gpu_last_phase_cycles(ctx.ptr, cyc, 16)
+        tot_c = sum(cyc[i] for i in range(k)) or 1.0
+        print(json.dumps({"phase_share": {PHASES[i]: round(cyc[i] / tot_c, 4) for i in range(min(k, len(PHASES)))},
+                          "cta_cycles": tot_c}), file=sys.stderr)
     if world == 1 and not args.no_cpu_baseline:
         sample = mols[: args.cpu_sample]
         r = cpu_throughput(sample, os.cpu_count() or 1, steps=1)
