@@ -199,6 +199,14 @@ int pm3gpu_last_transfer_bytes(pm3gpu_ctx* ctx, long long* h2d, long long* d2h);
 /* Number of this library's kernels launched by the last call. */
 int pm3gpu_last_kernel_launches(pm3gpu_ctx* ctx);
 
+/* Molecules with at least `nao` basis functions are solved one at a time on the whole GPU
+ * (grid-wide integral and Fock kernels, blocked eigensolver, cuBLAS DGEMM for the dense
+ * products) instead of one CTA each. Default and maximum 257: every molecule beyond one CTA's
+ * 256 basis functions. Lower values send smaller molecules to that path too (one molecule at a
+ * time, all SMs on it). Same run_pm3 semantics either way (no reference counterpart: the
+ * reference has one CPU path). */
+int pm3gpu_set_large_threshold(pm3gpu_ctx* ctx, int nao);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,768 @@
+// Host driver of the whole-GPU path for one large molecule: the run_job SCF loop (scf.rs:1179-1496)
+// with the work spread over the device (large_scf.cuh kernels, cuBLAS DGEMM for the dense
+// products). Included by pm3gpu.cu inside its private namespace, after the context definition.
+//
+// Matrices are row-major n x n FP64. cuBLAS sees a row-major matrix as its column-major
+// transpose; every call below is written in that view (comments give the row-major product).
+//
+// Eigensolver for large n: blocked Householder tridiagonalisation (panel kernels + two DGEMM
+// trailing updates per panel), division-free Sturm multisection for the lowest n_occ + 1
+// eigenvalues (warm-started from the previous iteration), twisted-factorisation eigenvectors of
+// the tridiagonal (one thread per vector), compact-WY back-transformation (DGEMM), then
+// Newton-Schulz steps X <- X (3I - X^T X)/2 until the occupied vectors are orthonormal to
+// 1e-13. Inside a cluster of close eigenvalues the twisted vectors are accurate only up to a
+// rotation within the cluster, and the polar step fixes their orthogonality without leaving the
+// cluster's invariant subspace, which is all the density P = w C_occ C_occ^T depends on.
+
+struct LargeBufs {
+  DevBuf ao, sprow, sroff;
+  DevBuf H, W, hacc, dpk, jacc, part, scal;
+  DevBuf P[2], Q[2], Pt, F, G, hist, A;
+  DevBuf d, e, e2, tau, lam, dlam, blk;
+  DevBuf V, Wp, y, wtmp, ps, s64;
+  DevBuf X, Xt, Dp, Lp, Um;
+  DevBuf Gm, Mm, Tm, Z1, Z2, blocks, Gk;
+  void release() {
+    for (DevBuf* b : {&ao, &sprow, &sroff, &H, &W, &hacc, &dpk, &jacc, &part, &scal, &P[0], &P[1], &Q[0], &Q[1], &Pt,
+                      &F, &G, &hist, &A, &d, &e, &e2, &tau, &lam, &dlam, &blk, &V, &Wp, &y, &wtmp, &ps, &s64, &X, &Xt,
+                      &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk})
+      b->release();
+  }
+};
+
+// Result of one large SCF (one pass of run_pm3's driver).
+struct LargeRun {
+  JobOut o;
+  bool uhf = false;
+  std::vector<double> eps_a, eps_b;      // eigenvalues of the last iteration (n_occ + 1 each)
+  std::vector<double> tri_a, tri_b;      // saved tridiagonals (d | e) of the last iteration
+  std::vector<double> charges;
+};
+
+#define BLAS_TRY(ctx, call)                                                                        \
+  do {                                                                                             \
+    cublasStatus_t s_ = (call);                                                                    \
+    if (s_ != CUBLAS_STATUS_SUCCESS) return fail((ctx), PM3GPU_CUDA_ERROR, std::string(#call ": cuBLAS status ") + std::to_string((int)s_)); \
+  } while (0)
+
+inline int grid_for(size_t work, int per_block = large::kBlock, int cap = large::kRedBlocks) {
+  const size_t g = (work + per_block - 1) / per_block;
+  return (int)std::max<size_t>(1, std::min<size_t>(g, (size_t)cap));
+}
+
+// A-DIIS weights (scf.rs:1152-1172, 1637-1693), serial form (the device path runs the same
+// iteration on one warp).
+void adiis_host(int m, const double* mg, double* c) {
+  const int last = m - 1;
+  const double mnn = mg[last * kMaxDepth + last];
+  double d[kMaxDepth], S[kMaxDepth * kMaxDepth];
+  for (int i = 0; i < m; ++i) d[i] = mg[i * kMaxDepth + last] - mnn;
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j)
+      S[i * kMaxDepth + j] = mg[i * kMaxDepth + j] - mg[i * kMaxDepth + last] - mg[last * kMaxDepth + j] + mnn;
+  double L = 1.0e-12;
+  for (int i = 0; i < m; ++i) {
+    double row = 0.0;
+    for (int j = 0; j < m; ++j) row += std::fabs(S[i * kMaxDepth + j] + S[j * kMaxDepth + i]);
+    L = std::max(L, row);
+  }
+  const double lr = 1.0 / L;
+  for (int i = 0; i < m; ++i) c[i] = i == last ? 1.0 : 0.0;
+  for (int it = 0; it < 400; ++it) {
+    double tr[kMaxDepth], u[kMaxDepth];
+    for (int k = 0; k < m; ++k) {
+      double g = 2.0 * d[k];
+      for (int j = 0; j < m; ++j) g += (S[k * kMaxDepth + j] + S[j * kMaxDepth + k]) * c[j];
+      tr[k] = c[k] - lr * g;
+      u[k] = tr[k];
+    }
+    for (int i = 1; i < m; ++i) {  // descending, stable
+      const double key = u[i];
+      int j = i - 1;
+      while (j >= 0 && u[j] < key) {
+        u[j + 1] = u[j];
+        --j;
+      }
+      u[j + 1] = key;
+    }
+    double css = 0.0, theta = 0.0;
+    for (int j = 0; j < m; ++j) {
+      css += u[j];
+      const double t = (css - 1.0) / (double)(j + 1);
+      if (u[j] - t > 0.0) theta = t;
+    }
+    double delta = 0.0;
+    for (int i = 0; i < m; ++i) {
+      const double p = std::max(tr[i] - theta, 0.0);
+      delta += std::fabs(p - c[i]);
+      c[i] = p;
+    }
+    if (delta < 1.0e-12) break;
+  }
+}
+
+class LargeSolver {
+ public:
+  LargeSolver(pm3gpu_ctx* c, LargeBufs& B) : c_(c), B_(B) {}
+
+  // Molecule setup: per-atom tables, H_core and the pair table. d_z / d_xyz: device copies.
+  int setup(const int32_t* h_z, const int32_t* d_z, const double* d_xyz, int natom, int nao, double* ecc) {
+    N_ = natom;
+    n_ = nao;
+    nn_ = (size_t)n_ * n_;
+    std::vector<int> ao(N_), sprow(N_ + 1);
+    std::vector<long long> sroff(N_);
+    int off = 0, pr = 0;
+    for (int a = 0; a < N_; ++a) {
+      ao[a] = off;
+      off += c_->h_elem[h_z[a]].norb;
+      sprow[a] = pr;
+      pr += c_->h_elem[h_z[a]].norb == 4 ? 10 : 1;
+    }
+    sprow[N_] = pr;
+    long long ro = 0;
+    for (int a = 0; a < N_; ++a) {
+      sroff[a] = ro;
+      ro += (long long)(sprow[a + 1] - sprow[a]) * (pr - sprow[a + 1]);
+    }
+    wcap_ = std::max<long long>(ro, 1);
+    CUDA_TRY(c_, B_.ao.ensure(4 * (size_t)N_));
+    CUDA_TRY(c_, B_.sprow.ensure(4 * (size_t)(N_ + 1)));
+    CUDA_TRY(c_, B_.sroff.ensure(8 * (size_t)N_));
+    CUDA_TRY(c_, cudaMemcpyAsync(B_.ao.p, ao.data(), 4 * (size_t)N_, cudaMemcpyHostToDevice, c_->stream));
+    CUDA_TRY(c_, cudaMemcpyAsync(B_.sprow.p, sprow.data(), 4 * (size_t)(N_ + 1), cudaMemcpyHostToDevice, c_->stream));
+    CUDA_TRY(c_, cudaMemcpyAsync(B_.sroff.p, sroff.data(), 8 * (size_t)N_, cudaMemcpyHostToDevice, c_->stream));
+    m_.elem = c_->elem.as<ElemDev>();
+    m_.pairs = c_->pairs.as<PairDev>();
+    m_.z = d_z;
+    m_.xyz = d_xyz;
+    m_.ao = B_.ao.as<int>();
+    m_.sprow = B_.sprow.as<int>();
+    m_.sroff = B_.sroff.as<long long>();
+    m_.N = N_;
+    m_.n = n_;
+    hz_ = h_z;
+    CUDA_TRY(c_, B_.H.ensure(8 * nn_));
+    CUDA_TRY(c_, B_.W.ensure(8 * (size_t)wcap_));
+    CUDA_TRY(c_, B_.hacc.ensure(80 * (size_t)N_));
+    CUDA_TRY(c_, B_.dpk.ensure(80 * (size_t)N_));
+    CUDA_TRY(c_, B_.jacc.ensure(80 * (size_t)N_));
+    CUDA_TRY(c_, B_.part.ensure(8 * (size_t)large::kRedBlocks));
+    CUDA_TRY(c_, B_.scal.ensure(8 * 128));
+    CUDA_TRY(c_, cudaMemsetAsync(B_.hacc.p, 0, 80 * (size_t)N_, c_->stream));
+    const long long np = (long long)N_ * (N_ - 1) / 2;
+    const int gp = grid_for((size_t)std::max<long long>(np, 1));
+    large::core_pairs_kernel<<<gp, large::kBlock, 0, c_->stream>>>(m_, B_.H.as<double>(), B_.W.as<double>(),
+                                                                  B_.hacc.as<double>(), B_.part.as<double>());
+    ++c_->launches;
+    large::finish_sum<<<1, large::kBlock, 0, c_->stream>>>(B_.part.as<double>(), gp, B_.scal.as<double>());
+    large::core_diag_kernel<<<grid_for((size_t)N_ * 16), large::kBlock, 0, c_->stream>>>(m_, B_.hacc.as<double>(),
+                                                                                        B_.H.as<double>());
+    c_->launches += 2;
+    CUDA_TRY(c_, cudaGetLastError());
+    CUDA_TRY(c_, cudaMemcpyAsync(ecc, B_.scal.p, 8, cudaMemcpyDeviceToHost, c_->stream));
+    CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+    return PM3GPU_OK;
+  }
+
+  // One SCF with job J (the first pass or a stability rung).
+  int scf(const JobDesc& J, LargeRun& R) {
+    const bool uhf = (J.flags & kJobUhf) != 0;
+    const int na = J.n_alpha, nb = J.n_beta;
+    const int n = n_;
+    R.uhf = uhf;
+    for (DevBuf* b : {&B_.P[0], &B_.P[1], &B_.F, &B_.A}) CUDA_TRY(c_, b->ensure(8 * nn_));
+    if (uhf)
+      for (DevBuf* b : {&B_.Q[0], &B_.Q[1], &B_.G, &B_.Pt}) CUDA_TRY(c_, b->ensure(8 * nn_));
+    const int depth = J.depth < 2 ? 2 : (J.depth > kMaxDepth ? kMaxDepth : J.depth);
+    const bool keep = (J.flags & kJobKeepDens) != 0;
+    const int slot_mats = uhf ? 4 : (keep ? 3 : 2);
+    if (J.accel != 0) CUDA_TRY(c_, B_.hist.ensure(8 * nn_ * (size_t)slot_mats * depth));
+    int cur = 0;
+    std::vector<double> lam_a, lam_b, dl_a, dl_b;
+    // ------------------------------------------------------------- initial density
+    double* Pa0 = B_.P[0].as<double>();
+    double* Pb0 = uhf ? B_.Q[0].as<double>() : nullptr;
+    if (J.guess == 2) {  // core-Hamiltonian orbitals (scf.rs:929-932, 969-975)
+      int rc = copy(B_.H.as<double>(), work_matrix());
+      if (rc) return rc;
+      rc = eigensolve(work_matrix(), std::min(n, na + 1), na, lam_a, dl_a, false, nullptr);
+      if (rc) return rc;
+      rc = density_from_x(na, na, uhf ? 1.0 : 2.0, Pa0);
+      if (rc) return rc;
+      if (uhf) {
+        rc = density_from_x(nb, na, 1.0, Pb0);
+        if (rc) return rc;
+      }
+      lam_a.clear();
+      dl_a.clear();
+    } else {
+      double fa = 1.0, fb = 0.0;
+      if (uhf) {
+        const double ne = (double)(na + nb);
+        fa = ne > 0.0 ? na / ne : 0.5;
+        fb = ne > 0.0 ? nb / ne : 0.5;
+      }
+      int tilt = -1;
+      if (J.guess == 3) {
+        double best = 0.0;
+        for (int a = 0; a < N_; ++a) {
+          const ElemDev& el = c_->h_elem[hz_[a]];
+          if (el.norb == 4 && el.occ_p > best) {
+            best = el.occ_p;
+            tilt = a;
+          }
+        }
+      }
+      CUDA_TRY(c_, cudaMemsetAsync(Pa0, 0, 8 * nn_, c_->stream));
+      large::sad_kernel<<<grid_for(N_), large::kBlock, 0, c_->stream>>>(m_, Pa0, fa, tilt);
+      ++c_->launches;
+      if (uhf) {
+        CUDA_TRY(c_, cudaMemsetAsync(Pb0, 0, 8 * nn_, c_->stream));
+        large::sad_kernel<<<grid_for(N_), large::kBlock, 0, c_->stream>>>(m_, Pb0, fb, tilt);
+        ++c_->launches;
+      }
+    }
+    // ------------------------------------------------------------- SCF iteration
+    double bg[kMaxDepth * kMaxDepth] = {}, mg[kMaxDepth * kMaxDepth] = {}, coef[kMaxDepth + 1] = {};
+    int len = 0, head = 0, iterations = 0;
+    double e_old = 0.0, last_change = INFINITY;
+    bool converged = false;
+    const int kva = std::min(n, na + 1), kvb = std::min(n, nb + 1);
+    for (int iter = 0; iter < J.max_scf; ++iter) {
+      iterations = iter + 1;
+      double* Pc = B_.P[cur].as<double>();
+      double* Pn = B_.P[1 - cur].as<double>();
+      double* Qc = uhf ? B_.Q[cur].as<double>() : nullptr;
+      double* Qn = uhf ? B_.Q[1 - cur].as<double>() : nullptr;
+      double* Fa = B_.F.as<double>();
+      double* Fb = uhf ? B_.G.as<double>() : nullptr;
+      double *Ea = nullptr, *Eb = nullptr, *Dh = nullptr;
+      if (J.accel != 0) {
+        if (len == depth) {
+          for (int i = 0; i + 1 < len; ++i)
+            for (int j = 0; j + 1 < len; ++j) {
+              bg[i * kMaxDepth + j] = bg[(i + 1) * kMaxDepth + j + 1];
+              mg[i * kMaxDepth + j] = mg[(i + 1) * kMaxDepth + j + 1];
+            }
+          head = (head + 1) % depth;
+          --len;
+        }
+        double* base = slot(head, len, depth, slot_mats);
+        Fa = base;
+        Ea = base + nn_;
+        if (uhf) {
+          Fb = base + 2 * nn_;
+          Eb = base + 3 * nn_;
+        } else if (keep) {
+          Dh = base + 2 * nn_;
+        }
+      }
+      double e_elec = 0.0;
+      if (!uhf) {
+        int rc = fock(Pc, nullptr, nullptr, Fa, nullptr);
+        if (rc) return rc;
+        double h1, h2;
+        if ((rc = dot(Pc, B_.H.as<double>(), nullptr, nullptr, &h1)) || (rc = dot(Pc, Fa, nullptr, nullptr, &h2)))
+          return rc;
+        e_elec = 0.5 * (h1 + h2);
+      } else {
+        double* Pt = B_.Pt.as<double>();
+        large::add_kernel<<<grid_for(nn_), large::kBlock, 0, c_->stream>>>(Pc, Qc, Pt, nn_);
+        ++c_->launches;
+        int rc = fock(Pt, Pc, Qc, Fa, Fb);
+        if (rc) return rc;
+        double h1, h2;
+        if ((rc = dot(Pt, B_.H.as<double>(), nullptr, nullptr, &h1)) || (rc = dot(Pc, Fa, Qc, Fb, &h2))) return rc;
+        e_elec = 0.5 * (h1 + h2);
+      }
+      // ---- accelerator (scf.rs:1240-1259 RHF; 1398-1413 UHF)
+      bool use_hist = false;
+      if (J.accel != 0) {
+        int rc = commutator(Fa, Pc, Ea);
+        if (rc) return rc;
+        if (uhf && (rc = commutator(Fb, Qc, Eb))) return rc;
+        if (keep && (rc = copy(Pc, Dh))) return rc;
+        double ee;
+        if ((rc = dot(Ea, Ea, Eb, Eb, &ee))) return rc;
+        double dnf = 0.0;
+        if (keep && (rc = dot(Dh, Fa, nullptr, nullptr, &dnf))) return rc;
+        for (int l = 0; l < len; ++l) {
+          double* bl = slot(head, l, depth, slot_mats);
+          double v;
+          if ((rc = dot(bl + nn_, Ea, uhf ? bl + 3 * nn_ : nullptr, Eb, &v))) return rc;
+          bg[l * kMaxDepth + len] = v;
+          bg[len * kMaxDepth + l] = v;
+          if (keep) {
+            double a1, a2;
+            if ((rc = dot(Dh, bl, nullptr, nullptr, &a1)) || (rc = dot(bl + 2 * nn_, Fa, nullptr, nullptr, &a2)))
+              return rc;
+            mg[len * kMaxDepth + l] = a1;  // <D_new, F_l>
+            mg[l * kMaxDepth + len] = a2;  // <D_l, F_new>
+          }
+        }
+        bg[len * kMaxDepth + len] = ee;
+        mg[len * kMaxDepth + len] = dnf;
+        const int m = len + 1;
+        const double err = std::sqrt(ee);
+        bool ok;
+        if (!uhf && J.accel == 2 && err > J.adiis_switch) {
+          ok = keep && m >= 2;
+          if (ok) adiis_host(m, mg, coef);
+        } else {
+          ok = cdiis_coeffs(m, bg, coef);
+        }
+        ++len;
+        use_hist = ok;
+      }
+      // ---- diagonalise (level shift for UHF only, scf.rs:1416-1418) and rebuild densities
+      double sq_a = 0.0, sq_b = 0.0;
+      for (int spin = 0; spin < (uhf ? 2 : 1); ++spin) {
+        large::Comb cb{};
+        if (use_hist) {
+          cb.len = len;
+          for (int l = 0; l < len; ++l) {
+            cb.m[l] = slot(head, l, depth, slot_mats) + (spin == 0 ? 0 : 2 * nn_);
+            cb.c[l] = coef[l];
+          }
+        } else {
+          cb.len = 1;
+          cb.m[0] = spin == 0 ? Fa : Fb;
+          cb.c[0] = 1.0;
+        }
+        const double shift = uhf ? J.shift : 0.0;
+        large::combine_kernel<<<grid_for(nn_), large::kBlock, 0, c_->stream>>>(cb, spin == 0 ? Pc : Qc, shift, n,
+                                                                              work_matrix());
+        ++c_->launches;
+        const int kv = spin == 0 ? kva : kvb, occ = spin == 0 ? na : nb;
+        std::vector<double>& lam = spin == 0 ? lam_a : lam_b;
+        std::vector<double>& dl = spin == 0 ? dl_a : dl_b;
+        std::vector<double>& tri = spin == 0 ? R.tri_a : R.tri_b;
+        int rc = eigensolve(work_matrix(), kv, occ, lam, dl, iter > 0, &tri);
+        if (rc) return rc;
+        double* Pold = spin == 0 ? Pc : Qc;
+        double* Pnew = spin == 0 ? Pn : Qn;
+        rc = density_from_x(occ, occ, uhf ? 1.0 : 2.0, Pnew);
+        if (rc) return rc;
+        double sq;
+        if ((rc = sqdiff(Pnew, Pold, &sq))) return rc;
+        (spin == 0 ? sq_a : sq_b) = sq;
+        const double damp = uhf ? J.damping : 0.0;
+        if (damp > 0.0) {  // stored density (1 - lam) Pnew + lam Pold; the RMS used the undamped Pnew
+          large::damp_kernel<<<grid_for(nn_), large::kBlock, 0, c_->stream>>>(Pnew, Pold, damp, nn_);
+          ++c_->launches;
+          if ((rc = copy(Pold, Pnew))) return rc;
+        }
+      }
+      const double dp = uhf ? std::sqrt(sq_a / (double)nn_) + std::sqrt(sq_b / (double)nn_)
+                            : std::sqrt(sq_a / (double)nn_);
+      const double de = std::fabs(e_elec - e_old);
+      last_change = dp;
+      e_old = e_elec;
+      cur = 1 - cur;
+      if (iter > 0 && de < J.e_tol && dp < J.p_tol) {
+        converged = true;
+        break;
+      }
+    }
+    // ------------------------------------------------------------- closing energy
+    double* Pf = B_.P[cur].as<double>();
+    double* Qf = uhf ? B_.Q[cur].as<double>() : nullptr;
+    double* Pt = Pf;
+    JobOut& o = R.o;
+    std::memset(&o, 0, sizeof(o));
+    if (!uhf) {
+      int rc = fock(Pf, nullptr, nullptr, B_.F.as<double>(), nullptr);
+      if (rc) return rc;
+      double h1, h2;
+      if ((rc = dot(Pf, B_.H.as<double>(), nullptr, nullptr, &h1)) ||
+          (rc = dot(Pf, B_.F.as<double>(), nullptr, nullptr, &h2)))
+        return rc;
+      o.electronic = 0.5 * (h1 + h2);
+      o.spin_max = 0.0;
+    } else {
+      Pt = B_.Pt.as<double>();
+      large::add_kernel<<<grid_for(nn_), large::kBlock, 0, c_->stream>>>(Pf, Qf, Pt, nn_);
+      large::absdiff_max_kernel<<<large::kRedBlocks, large::kBlock, 0, c_->stream>>>(Pf, Qf, nn_, B_.part.as<double>());
+      c_->launches += 2;
+      std::vector<double> mx(large::kRedBlocks);
+      CUDA_TRY(c_, cudaMemcpyAsync(mx.data(), B_.part.p, 8 * mx.size(), cudaMemcpyDeviceToHost, c_->stream));
+      CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+      o.spin_max = 0.0;
+      for (double v : mx) o.spin_max = std::max(o.spin_max, v);
+      int rc = fock(Pt, Pf, Qf, B_.F.as<double>(), B_.G.as<double>());
+      if (rc) return rc;
+      double h1, h2;
+      if ((rc = dot(Pt, B_.H.as<double>(), nullptr, nullptr, &h1)) ||
+          (rc = dot(Pf, B_.F.as<double>(), Qf, B_.G.as<double>(), &h2)))
+        return rc;
+      o.electronic = 0.5 * (h1 + h2);
+    }
+    final_pt_ = Pt;
+    final_pa_ = uhf ? Pf : nullptr;
+    final_pb_ = Qf;
+    o.converged = converged ? 1 : 0;
+    o.iterations = iterations;
+    o.last_change = last_change;
+    o.status = converged ? 0 : 4;
+    // frontier of the last iteration's orbitals (scf.rs:106-124, 804-822)
+    o.has_homo_a = na >= 1;
+    o.has_lumo_a = na < n;
+    o.homo_a = na >= 1 ? lam_a[na - 1] : 0.0;
+    o.lumo_a = na < n ? lam_a[na] : 0.0;
+    o.homo = o.homo_a;
+    o.lumo = o.lumo_a;
+    o.has_homo = o.has_homo_a;
+    o.has_lumo = o.has_lumo_a;
+    if (uhf) {
+      if (nb >= 1) {
+        o.homo = o.has_homo ? std::max(o.homo, lam_b[nb - 1]) : lam_b[nb - 1];
+        o.has_homo = 1;
+      }
+      if (nb < n) {
+        o.lumo = o.has_lumo ? std::min(o.lumo, lam_b[nb]) : lam_b[nb];
+        o.has_lumo = 1;
+      }
+    }
+    o.gap = (o.has_homo && o.has_lumo) ? o.lumo - o.homo : INFINITY;
+    R.eps_a = lam_a;
+    R.eps_b = lam_b;
+    return properties(Pt, R);
+  }
+
+  // Final densities of the last scf() call (device pointers into this solver's buffers).
+  const double* final_pt() const { return final_pt_; }
+  const double* final_pa() const { return final_pa_; }
+  const double* final_pb() const { return final_pb_; }
+
+  // All n eigenvalues of a saved tridiagonal (d | e) -- the MO energies output.
+  int all_eigenvalues(const std::vector<double>& tri, std::vector<double>& out) {
+    CUDA_TRY(c_, B_.d.ensure(8 * (size_t)n_));
+    CUDA_TRY(c_, B_.e.ensure(8 * (size_t)n_));
+    CUDA_TRY(c_, cudaMemcpyAsync(B_.d.p, tri.data(), 8 * (size_t)n_, cudaMemcpyHostToDevice, c_->stream));
+    CUDA_TRY(c_, cudaMemcpyAsync(B_.e.p, tri.data() + n_, 8 * (size_t)n_, cudaMemcpyHostToDevice, c_->stream));
+    std::vector<double> none;
+    return eigenvalues(n_, out, none, false);
+  }
+
+ private:
+  pm3gpu_ctx* c_;
+  LargeBufs& B_;
+  large::Mol m_{};
+  const int32_t* hz_ = nullptr;
+  int N_ = 0, n_ = 0;
+  size_t nn_ = 0;
+  long long wcap_ = 1;
+  const double* final_pt_ = nullptr;
+  const double* final_pa_ = nullptr;
+  const double* final_pb_ = nullptr;
+  std::vector<int> hblk_;
+
+  double* work_matrix() { return B_.A.as<double>(); }
+  double* slot(int head, int l, int depth, int mats) {
+    return B_.hist.as<double>() + (size_t)((head + l) % depth) * mats * nn_;
+  }
+  int copy(const double* src, double* dst) {
+    CUDA_TRY(c_, cudaMemcpyAsync(dst, src, 8 * nn_, cudaMemcpyDeviceToDevice, c_->stream));
+    return PM3GPU_OK;
+  }
+  cublasHandle_t blas() { return c_->blas; }
+
+  int finish(double* out) {
+    large::finish_sum<<<1, large::kBlock, 0, c_->stream>>>(B_.part.as<double>(), large::kRedBlocks, B_.scal.as<double>());
+    ++c_->launches;
+    CUDA_TRY(c_, cudaMemcpyAsync(out, B_.scal.p, 8, cudaMemcpyDeviceToHost, c_->stream));
+    CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+    return PM3GPU_OK;
+  }
+  int dot(const double* x, const double* y, const double* x2, const double* y2, double* out) {
+    large::dot_kernel<<<large::kRedBlocks, large::kBlock, 0, c_->stream>>>(x, y, x2, y2, nn_, B_.part.as<double>());
+    ++c_->launches;
+    return finish(out);
+  }
+  int sqdiff(const double* x, const double* y, double* out) {
+    large::sqdiff_kernel<<<large::kRedBlocks, large::kBlock, 0, c_->stream>>>(x, y, nn_, B_.part.as<double>());
+    ++c_->launches;
+    return finish(out);
+  }
+
+  // F = H + J(Pt) - K (fock.rs:285-332); RHF exchange from Pt/2, UHF from Pa / Pb.
+  int fock(const double* Pt, const double* Pa, const double* Pb, double* F, double* G) {
+    const int gN = grid_for((size_t)N_ * 16);
+    large::pack_density_kernel<<<gN, large::kBlock, 0, c_->stream>>>(m_, Pt, B_.dpk.as<double>(), B_.jacc.as<double>());
+    const long long np = (long long)N_ * (N_ - 1) / 2;
+    const int gp = grid_for((size_t)std::max<long long>(np, 1));
+    if (Pb)
+      large::fock_pairs_kernel<true><<<gp, large::kBlock, 0, c_->stream>>>(
+          m_, B_.W.as<double>(), B_.H.as<double>(), B_.dpk.as<double>(), B_.jacc.as<double>(), Pt, Pa, Pb, F, G);
+    else
+      large::fock_pairs_kernel<false><<<gp, large::kBlock, 0, c_->stream>>>(
+          m_, B_.W.as<double>(), B_.H.as<double>(), B_.dpk.as<double>(), B_.jacc.as<double>(), Pt, Pa, Pb, F, G);
+    large::fock_diag_kernel<<<gN, large::kBlock, 0, c_->stream>>>(m_, B_.H.as<double>(), B_.jacc.as<double>(), Pt, Pa,
+                                                                  Pb, F, G);
+    c_->launches += 3;
+    CUDA_TRY(c_, cudaGetLastError());
+    return PM3GPU_OK;
+  }
+  // E = F P - P F (scf.rs:1039-1054): row-major F P is cuBLAS's column-major P F.
+  int commutator(const double* F, const double* P, double* E) {
+    const double one = 1.0, zero = 0.0;
+    BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, n_, n_, n_, &one, P, n_, F, n_, &zero, E, n_));
+    large::antisym_kernel<<<grid_for(nn_), large::kBlock, 0, c_->stream>>>(E, n_);
+    ++c_->launches;
+    return PM3GPU_OK;
+  }
+  // P = w X X^T over the first k eigenvectors of the last eigensolve (X is n x ld, row-major).
+  int density_from_x(int k, int ld, double w, double* P) {
+    if (k == 0) {
+      CUDA_TRY(c_, cudaMemsetAsync(P, 0, 8 * nn_, c_->stream));
+      return PM3GPU_OK;
+    }
+    const double zero = 0.0;
+    BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, n_, n_, k, &w, B_.X.as<double>(), ld,
+                             B_.X.as<double>(), ld, &zero, P, n_));
+    return PM3GPU_OK;
+  }
+
+  // Lowest kval eigenvalues of the tridiagonal in B_.d / B_.e (host bookkeeping of splits).
+  int eigenvalues(int kval, std::vector<double>& lam, std::vector<double>& dl, bool warm) {
+    const int n = n_;
+    std::vector<double> d(n), e(n);
+    CUDA_TRY(c_, cudaMemcpyAsync(d.data(), B_.d.p, 8 * (size_t)n, cudaMemcpyDeviceToHost, c_->stream));
+    CUDA_TRY(c_, cudaMemcpyAsync(e.data(), B_.e.p, 8 * (size_t)n, cudaMemcpyDeviceToHost, c_->stream));
+    CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+    return eigenvalues_host(d, e, kval, lam, dl, warm);
+  }
+  int eigenvalues_host(std::vector<double>& d, std::vector<double>& e, int kval, std::vector<double>& lam,
+                       std::vector<double>& dl, bool warm) {
+    const int n = n_;
+    constexpr double eps = 2.220446049250313e-16;
+    double gl = d[0], gu = d[0];
+    for (int i = 0; i < n; ++i) {
+      const double rad = (i + 1 < n ? std::fabs(e[i]) : 0.0) + (i > 0 ? std::fabs(e[i - 1]) : 0.0);
+      gl = std::min(gl, d[i] - rad);
+      gu = std::max(gu, d[i] + rad);
+    }
+    const double tnorm = std::max(std::fabs(gl), std::fabs(gu));
+    const double cut = 1000.0 * eps * tnorm;
+    std::vector<double> e2(n);
+    hblk_.assign(1, 0);
+    double emax = 0.0;
+    for (int i = 0; i < n; ++i) {
+      double ei = (i + 1 < n) ? e[i] : 0.0;
+      if (i + 1 < n && std::fabs(ei) <= cut) {
+        ei = 0.0;
+        e[i] = 0.0;
+        hblk_.push_back(i + 1);
+      }
+      e2[i] = ei * ei;
+      emax = std::max(emax, ei * ei);
+    }
+    hblk_.push_back(n);
+    pivmin_ = 2.2250738585072014e-308 * std::max(1.0, emax);
+    tnorm_ = tnorm;
+    const double glo = gl - 4.0 * eps * tnorm * n - 1.0e-300, ghi = gu + 4.0 * eps * tnorm * n + 1.0e-300;
+    CUDA_TRY(c_, B_.e2.ensure(8 * (size_t)n));
+    CUDA_TRY(c_, B_.blk.ensure(4 * hblk_.size()));
+    CUDA_TRY(c_, B_.lam.ensure(8 * (size_t)n));
+    CUDA_TRY(c_, B_.dlam.ensure(16 * (size_t)n));
+    CUDA_TRY(c_, cudaMemcpyAsync(B_.e.p, e.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, c_->stream));
+    CUDA_TRY(c_, cudaMemcpyAsync(B_.e2.p, e2.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, c_->stream));
+    CUDA_TRY(c_, cudaMemcpyAsync(B_.blk.p, hblk_.data(), 4 * hblk_.size(), cudaMemcpyHostToDevice, c_->stream));
+    const bool seeded = warm && (int)lam.size() == kval && (int)dl.size() == kval;
+    double* prev = B_.dlam.as<double>();
+    double* dprev = prev + n;
+    if (seeded) {
+      CUDA_TRY(c_, cudaMemcpyAsync(prev, lam.data(), 8 * (size_t)kval, cudaMemcpyHostToDevice, c_->stream));
+      CUDA_TRY(c_, cudaMemcpyAsync(dprev, dl.data(), 8 * (size_t)kval, cudaMemcpyHostToDevice, c_->stream));
+    }
+    int g = 32;
+    while (g > 1 && (size_t)kval * g > 65536) g >>= 1;
+    const int threads = kval * g;
+    large::multisect_kernel<<<(threads + large::kBlock - 1) / large::kBlock, large::kBlock, 0, c_->stream>>>(
+        B_.d.as<double>(), B_.e2.as<double>(), n, kval, g, glo, ghi, pivmin_, tnorm_, seeded ? prev : nullptr,
+        seeded ? dprev : nullptr, B_.lam.as<double>());
+    ++c_->launches;
+    CUDA_TRY(c_, cudaGetLastError());
+    std::vector<double> nl(kval);
+    CUDA_TRY(c_, cudaMemcpyAsync(nl.data(), B_.lam.p, 8 * (size_t)kval, cudaMemcpyDeviceToHost, c_->stream));
+    CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+    dl.assign(kval, 1.0e30);
+    if (seeded)
+      for (int j = 0; j < kval; ++j) dl[j] = nl[j] - lam[j];
+    lam.swap(nl);
+    return PM3GPU_OK;
+  }
+
+  // Eigen-decomposition of the symmetric matrix in A (destroyed): kval lowest eigenvalues into
+  // lam, kvec eigenvectors into B_.X (n x kvec, row-major). `tri` receives the tridiagonal.
+  int eigensolve(double* A, int kval, int kvec, std::vector<double>& lam, std::vector<double>& dl, bool warm,
+                 std::vector<double>* tri) {
+    const int n = n_;
+    const size_t K = (size_t)std::max(kvec, 1);
+    for (DevBuf* b : {&B_.d, &B_.e, &B_.tau, &B_.y, &B_.wtmp}) CUDA_TRY(c_, b->ensure(8 * (size_t)n));
+    CUDA_TRY(c_, B_.V.ensure(8 * (size_t)n * large::kPanel));
+    CUDA_TRY(c_, B_.Wp.ensure(8 * (size_t)n * large::kPanel));
+    CUDA_TRY(c_, B_.ps.ensure(8 * 64 * (size_t)large::kRedBlocks));
+    CUDA_TRY(c_, B_.s64.ensure(8 * 64));
+    double* d = B_.d.as<double>();
+    double* e = B_.e.as<double>();
+    double* tau = B_.tau.as<double>();
+    double* V = B_.V.as<double>();
+    double* W = B_.Wp.as<double>();
+    const double one = 1.0, mone = -1.0, zero = 0.0;
+    // ---- 1. Householder tridiagonalisation (sytrd/latrd, lower)
+    const int smem_max = 8 * n;
+    CUDA_TRY(c_, cudaFuncSetAttribute(large::panel_symv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      std::max(smem_max, 1024)));
+    for (int p = 0; p < n - 2; p += large::kPanel) {
+      const int b = std::min(large::kPanel, n - 2 - p);
+      for (int j = 0; j < b; ++j) {
+        const int i = p + j;
+        const int m = n - i - 1;
+        large::panel_column_kernel<<<1, large::kColThreads, 0, c_->stream>>>(A, n, i, j, V, W, d, e, tau);
+        const int gs = std::max(1, std::min((m + 7) / 8, 4 * c_->sms));
+        large::panel_symv_kernel<<<gs, large::kBlock, 8 * (size_t)m, c_->stream>>>(A, n, i, j, V, W, B_.y.as<double>(),
+                                                                                    B_.ps.as<double>());
+        large::panel_reduce_kernel<<<1, 64, 0, c_->stream>>>(B_.ps.as<double>(), gs, B_.s64.as<double>());
+        const int gw = grid_for((size_t)m, large::kBlock, 4 * c_->sms);
+        large::panel_wfix_kernel<<<gw, large::kBlock, 0, c_->stream>>>(n, i, j, V, W, B_.y.as<double>(),
+                                                                        B_.s64.as<double>(), tau + i,
+                                                                        B_.wtmp.as<double>(), B_.part.as<double>());
+        large::panel_wfinal_kernel<<<grid_for((size_t)n, large::kBlock, 4 * c_->sms), large::kBlock, 0, c_->stream>>>(
+            n, i, j, V, W, B_.wtmp.as<double>(), B_.part.as<double>(), gw, tau + i);
+        c_->launches += 5;
+      }
+      const int q = p + b, m = n - q;
+      if (m > 0) {  // A[q:, q:] -= V W^T + W V^T (row-major); column-major: C -= Wc^T Vc + Vc^T Wc
+        double* C = A + (size_t)q * n + q;
+        const double* Vq = V + (size_t)q * large::kPanel;
+        const double* Wq = W + (size_t)q * large::kPanel;
+        BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Wq, large::kPanel, Vq, large::kPanel,
+                                 &one, C, n));
+        BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Vq, large::kPanel, Wq, large::kPanel,
+                                 &one, C, n));
+      }
+    }
+    large::tail_kernel<<<1, 1, 0, c_->stream>>>(A, n, d, e, tau);
+    ++c_->launches;
+    CUDA_TRY(c_, cudaGetLastError());
+    // ---- 2. eigenvalues (host split bookkeeping, device multisection)
+    {
+      std::vector<double> hd(n), he(n);
+      CUDA_TRY(c_, cudaMemcpyAsync(hd.data(), d, 8 * (size_t)n, cudaMemcpyDeviceToHost, c_->stream));
+      CUDA_TRY(c_, cudaMemcpyAsync(he.data(), e, 8 * (size_t)n, cudaMemcpyDeviceToHost, c_->stream));
+      CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+      if (tri) {
+        tri->assign(2 * (size_t)n, 0.0);
+        std::copy(hd.begin(), hd.end(), tri->begin());
+        std::copy(he.begin(), he.end(), tri->begin() + n);
+      }
+      int rc = eigenvalues_host(hd, he, kval, lam, dl, warm);
+      if (rc) return rc;
+    }
+    if (kvec <= 0) return PM3GPU_OK;
+    // ---- 3. eigenvectors of the tridiagonal
+    CUDA_TRY(c_, B_.X.ensure(8 * (size_t)n * K));
+    CUDA_TRY(c_, B_.Xt.ensure(8 * (size_t)n * K));
+    for (DevBuf* bf : {&B_.Dp, &B_.Lp, &B_.Um}) CUDA_TRY(c_, bf->ensure(8 * (size_t)n * K));
+    double* X = B_.X.as<double>();
+    large::twisted_kernel<<<(kvec + large::kBlock - 1) / large::kBlock, large::kBlock, 0, c_->stream>>>(
+        d, e, B_.e2.as<double>(), n, kvec, B_.lam.as<double>(), B_.blk.as<int>(), (int)hblk_.size() - 1, pivmin_, tnorm_,
+        X, B_.Dp.as<double>(), B_.Lp.as<double>(), B_.Um.as<double>());
+    ++c_->launches;
+    CUDA_TRY(c_, cudaGetLastError());
+    // ---- 4. back-transformation X <- Q X, panels from the last to the first
+    CUDA_TRY(c_, B_.Gm.ensure(8 * (size_t)large::kPanel * large::kPanel));
+    CUDA_TRY(c_, B_.Tm.ensure(8 * (size_t)large::kPanel * large::kPanel));
+    CUDA_TRY(c_, B_.Z1.ensure(8 * K * large::kPanel));
+    CUDA_TRY(c_, B_.Z2.ensure(8 * K * large::kPanel));
+    const int np = n - 2 > 0 ? (n - 2 + large::kPanel - 1) / large::kPanel : 0;
+    for (int pi = np - 1; pi >= 0; --pi) {
+      const int p = pi * large::kPanel, b = std::min(large::kPanel, n - 2 - p);
+      large::panel_v_kernel<<<grid_for((size_t)n * large::kPanel), large::kBlock, 0, c_->stream>>>(A, n, p, b, V);
+      ++c_->launches;
+      const int r0 = p + 1, m = n - r0;
+      const double* Vr = V + (size_t)r0 * large::kPanel;
+      double* Xr = X + (size_t)r0 * K;
+      // G = V^T V (b x b); column-major: Vc Vc^T
+      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_T, b, b, m, &one, Vr, large::kPanel, Vr, large::kPanel,
+                               &zero, B_.Gm.as<double>(), b));
+      large::wy_t_kernel<<<1, 1, 0, c_->stream>>>(B_.Gm.as<double>(), tau, p, b, B_.Tm.as<double>());
+      ++c_->launches;
+      // Z = V^T X  -> column-major Zc = Xc Vc^T (K x b)
+      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_T, (int)K, b, m, &one, Xr, (int)K, Vr, large::kPanel,
+                               &zero, B_.Z1.as<double>(), (int)K));
+      // Z2 = T Z -> Z2c = Zc T^T, T row-major = column-major T^T
+      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, (int)K, b, b, &one, B_.Z1.as<double>(), (int)K,
+                               B_.Tm.as<double>(), large::kPanel, &zero, B_.Z2.as<double>(), (int)K));
+      // X -= V Z2 -> Xc -= Z2c Vc
+      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, (int)K, m, b, &mone, B_.Z2.as<double>(), (int)K, Vr,
+                               large::kPanel, &one, Xr, (int)K));
+    }
+    // ---- 5. orthonormalise: X <- X (3I - X^T X) / 2 until max |X^T X - I| < 1e-13
+    CUDA_TRY(c_, B_.Mm.ensure(8 * K * K));
+    CUDA_TRY(c_, B_.Gk.ensure(8 * K * K));
+    double* Gk = B_.Gk.as<double>();
+    for (int step = 0; step < 4; ++step) {
+      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_T, (int)K, (int)K, n, &one, X, (int)K, X, (int)K, &zero,
+                               Gk, (int)K));
+      large::orth_defect_kernel<<<large::kRedBlocks, large::kBlock, 0, c_->stream>>>(Gk, (int)K, B_.part.as<double>());
+      ++c_->launches;
+      std::vector<double> mx(large::kRedBlocks);
+      CUDA_TRY(c_, cudaMemcpyAsync(mx.data(), B_.part.p, 8 * mx.size(), cudaMemcpyDeviceToHost, c_->stream));
+      CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+      double defect = 0.0;
+      for (double v : mx) defect = std::max(defect, v);
+      if (!(defect < 0.5)) return fail(c_, PM3GPU_LINALG, "large eigensolver: eigenvectors far from orthonormal");
+      if (defect < 1.0e-13) break;
+      large::ns_matrix_kernel<<<grid_for(K * K), large::kBlock, 0, c_->stream>>>(Gk, B_.Mm.as<double>(), (int)K);
+      ++c_->launches;
+      // X M (row-major) -> column-major M Xc (M symmetric)
+      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, (int)K, n, (int)K, &one, B_.Mm.as<double>(), (int)K, X,
+                               (int)K, &zero, B_.Xt.as<double>(), (int)K));
+      std::swap(B_.X, B_.Xt);
+      X = B_.X.as<double>();
+    }
+    return PM3GPU_OK;
+  }
+
+  // Mulliken charges and the dipole about the centre of mass (dipole.rs:64-144) from the atom
+  // blocks of the total density.
+  int properties(const double* Pt, LargeRun& R) {
+    CUDA_TRY(c_, B_.blocks.ensure(8 * 16 * (size_t)N_));
+    large::atom_blocks_kernel<<<grid_for((size_t)N_ * 16), large::kBlock, 0, c_->stream>>>(m_, Pt, B_.blocks.as<double>());
+    ++c_->launches;
+    std::vector<double> blk(16 * (size_t)N_), xyz(3 * (size_t)N_);
+    CUDA_TRY(c_, cudaMemcpyAsync(blk.data(), B_.blocks.p, 8 * blk.size(), cudaMemcpyDeviceToHost, c_->stream));
+    CUDA_TRY(c_, cudaMemcpyAsync(xyz.data(), m_.xyz, 8 * xyz.size(), cudaMemcpyDeviceToHost, c_->stream));
+    CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+    R.charges.assign(N_, 0.0);
+    double mt = 0.0, cm[3] = {0, 0, 0};
+    for (int a = 0; a < N_; ++a) {
+      const ElemDev& el = c_->h_elem[hz_[a]];
+      double pop = 0.0;
+      for (int k = 0; k < el.norb; ++k) pop += blk[16 * (size_t)a + 5 * k];
+      R.charges[a] = el.core - pop;
+      mt += el.mass;
+      for (int k = 0; k < 3; ++k) cm[k] += el.mass * xyz[3 * (size_t)a + k];
+    }
+    for (int k = 0; k < 3; ++k) cm[k] = mt > 0.0 ? cm[k] / mt : 0.0;
+    double mu[3] = {0, 0, 0};
+    for (int a = 0; a < N_; ++a) {
+      const ElemDev& el = c_->h_elem[hz_[a]];
+      double pop = 0.0;
+      for (int k = 0; k < el.norb; ++k) pop += blk[16 * (size_t)a + 5 * k];
+      for (int ax = 0; ax < 3; ++ax) {
+        const double disp = xyz[3 * (size_t)a + ax] - cm[ax];
+        double elc = pop * disp;
+        if (el.norb == 4) elc += 2.0 * blk[16 * (size_t)a + ax + 1] * el.dd;
+        mu[ax] += disp * el.core - elc;
+      }
+    }
+    for (int ax = 0; ax < 3; ++ax) R.o.dipole[ax] = mu[ax] * kAuDipoleToDebye;
+    return PM3GPU_OK;
+  }
+
+  double pivmin_ = 0.0, tnorm_ = 0.0;
+};

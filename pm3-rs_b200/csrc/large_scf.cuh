@@ -1,0 +1,616 @@
+// Whole-GPU kernels for one large molecule (basis beyond one CTA): the same run_pm3 SCF as the
+// per-CTA path, with every step spread over the device. Pair integrals, H_core and the Fock
+// build run one thread per atom pair (src/hamiltonian.rs:191-344, src/fock.rs:93-332); the dense
+// products (commutator, density, the eigensolver's trailing updates and back-transformation) are
+// cuBLAS DGEMMs issued by the host driver; the Householder panel, the Sturm multisection, the
+// twisted-factorisation eigenvectors, the compact-WY factors and all reductions are here.
+#pragma once
+#include "scf_kernel.cuh"
+
+namespace pm3gpu {
+namespace large {
+
+constexpr int kBlock = 256;   // threads per block of the grid kernels (matches the CTA helpers)
+constexpr int kPanel = 32;    // Householder panel width
+constexpr int kRedBlocks = 1184;  // partial-sum slots of the grid reductions (8 per SM)
+
+// Device view of one molecule.
+struct Mol {
+  const ElemDev* elem;
+  const PairDev* pairs;
+  const int* z;             // [N]
+  const double* xyz;        // [3N] Bohr
+  const int* ao;            // [N] first AO of each atom
+  const int* sprow;         // [N+1] prefix sums of packed orbital-pair sizes (10 sp, 1 s)
+  const long long* sroff;   // [N] pair-table row offsets
+  int N, n;
+};
+
+__device__ __forceinline__ long long pair_count(int N) { return (long long)N * (N - 1) / 2; }
+__device__ __forceinline__ const double* pair_block(const Mol& m, const double* W, int u, int v) {
+  const int su = m.sprow[u + 1] - m.sprow[u];
+  return W + m.sroff[u] + (long long)su * (m.sprow[v] - m.sprow[u + 1]);
+}
+
+// ---------------------------------------------------------------- reductions (deterministic)
+// Each block writes one partial; finish_sum adds the partials in a fixed order.
+__device__ __forceinline__ void block_partial(double v, double* partial) {
+  __shared__ double red[kBlock / 32];
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < kBlock / 32; ++i) t += red[i];
+    partial[blockIdx.x] = t;
+  }
+}
+__global__ void __launch_bounds__(kBlock) finish_sum(const double* partial, int np, double* out) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < np; i += kBlock) v += partial[i];
+  __shared__ double red[kBlock / 32];
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < kBlock / 32; ++i) t += red[i];
+    *out = t;
+  }
+}
+// sum_k x_k y_k (+ sum_k x2_k y2_k when x2 is given)
+__global__ void __launch_bounds__(kBlock) dot_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                                     const double* __restrict__ x2, const double* __restrict__ y2,
+                                                     size_t cnt, double* partial) {
+  double s = 0.0;
+  for (size_t k = blockIdx.x * (size_t)kBlock + threadIdx.x; k < cnt; k += (size_t)gridDim.x * kBlock) {
+    s = fma(x[k], y[k], s);
+    if (x2) s = fma(x2[k], y2[k], s);
+  }
+  block_partial(s, partial);
+}
+// sum_k (x_k - y_k)^2
+__global__ void __launch_bounds__(kBlock) sqdiff_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                                        size_t cnt, double* partial) {
+  double s = 0.0;
+  for (size_t k = blockIdx.x * (size_t)kBlock + threadIdx.x; k < cnt; k += (size_t)gridDim.x * kBlock) {
+    const double d = x[k] - y[k];
+    s = fma(d, d, s);
+  }
+  block_partial(s, partial);
+}
+// max_k |x_k - y_k| (one partial per block)
+__global__ void __launch_bounds__(kBlock) absdiff_max_kernel(const double* __restrict__ x,
+                                                             const double* __restrict__ y, size_t cnt,
+                                                             double* partial) {
+  double s = 0.0;
+  for (size_t k = blockIdx.x * (size_t)kBlock + threadIdx.x; k < cnt; k += (size_t)gridDim.x * kBlock)
+    s = fmax(s, fabs(x[k] - y[k]));
+  s = warp_max(s);
+  __shared__ double red[kBlock / 32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < kBlock / 32; ++i) t = fmax(t, red[i]);
+    partial[blockIdx.x] = t;
+  }
+}
+
+// ---------------------------------------------------------------- H_core and the pair table
+__global__ void __launch_bounds__(kBlock) core_pairs_kernel(Mol m, double* H, double* W, double* hacc,
+                                                            double* partial) {
+  const long long np = pair_count(m.N);
+  double ecc = 0.0;
+  for (long long t = blockIdx.x * (long long)kBlock + threadIdx.x; t < np; t += (long long)gridDim.x * kBlock) {
+    int u, v;
+    pair_uv(m.N, (int)t, u, v);
+    const ElemDev& eu = m.elem[m.z[u]];
+    const ElemDev& ev = m.elem[m.z[v]];
+    const bool hu = eu.norb == 4, hv = ev.norb == 4;
+    const int a = (hu || !hv) ? u : v, b = a == u ? v : u;
+    double* w = const_cast<double*>(pair_block(m, W, u, v));
+    ecc += core_pair(m.elem[m.z[a]], m.elem[m.z[b]], eu, ev, *m.pairs, m.xyz + 3 * (size_t)a, m.xyz + 3 * (size_t)b,
+                     m.ao[a], m.ao[b], (size_t)m.n, hacc + 10 * (size_t)a, hacc + 10 * (size_t)b, w, H);
+  }
+  block_partial(ecc, partial);
+}
+// atom-diagonal blocks of H: U + the summed electron-core attractions
+__global__ void __launch_bounds__(kBlock) core_diag_kernel(Mol m, const double* hacc, double* H) {
+  for (int k = blockIdx.x * kBlock + threadIdx.x; k < m.N * 16; k += gridDim.x * kBlock) {
+    const int a = k >> 4, mu = (k >> 2) & 3, nu = k & 3;
+    const ElemDev& e = m.elem[m.z[a]];
+    if (mu >= e.norb || nu >= e.norb) continue;
+    double h = hacc[a * 10 + pk(mu, nu)];
+    if (mu == nu) h += mu == 0 ? e.uss : e.upp;
+    H[(size_t)(m.ao[a] + mu) * m.n + m.ao[a] + nu] = h;
+  }
+}
+// SAD guess (scf.rs:855-881) into a zeroed P; `tilt` = atom of the symmetry-broken tilt or -1
+__global__ void __launch_bounds__(kBlock) sad_kernel(Mol m, double* P, double scale, int tilt) {
+  for (int a = blockIdx.x * kBlock + threadIdx.x; a < m.N; a += gridDim.x * kBlock) {
+    const ElemDev& e = m.elem[m.z[a]];
+    const int o = m.ao[a];
+    P[(size_t)o * m.n + o] = e.occ_s * scale;
+    if (e.norb == 4) {
+      double pz = e.occ_p / 3.0;
+      for (int k = 1; k < 4; ++k) P[(size_t)(o + k) * m.n + o + k] = pz * scale;
+      if (a == tilt) {  // scf.rs:894-916: 0.2 e from pz to px on the most p-rich atom
+        const double t = fmin(0.2, pz);
+        P[(size_t)(o + 3) * m.n + o + 3] = (pz - t) * scale;
+        P[(size_t)(o + 1) * m.n + o + 1] = (pz + t) * scale;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- Fock build
+// packed atomic densities (fock.rs:93-100) and zeroed Coulomb accumulators
+__global__ void __launch_bounds__(kBlock) pack_density_kernel(Mol m, const double* Pt, double* dpk, double* jacc) {
+  for (int k = blockIdx.x * kBlock + threadIdx.x; k < m.N * 10; k += gridDim.x * kBlock) {
+    const int a = k / 10, p = k % 10;
+    const int no = m.elem[m.z[a]].norb;
+    jacc[k] = 0.0;
+    double v = 0.0;
+    if (no == 4 || p == 0) {
+      int hi, lo;
+      unpk(p, hi, lo);
+      const int oa = m.ao[a];
+      v = Pt[(size_t)(oa + hi) * m.n + oa + lo];
+      if (hi != lo) v *= 2.0;
+    }
+    dpk[k] = v;
+  }
+}
+template <bool UHF>
+__global__ void __launch_bounds__(kBlock) fock_pairs_kernel(Mol m, const double* W, const double* H, const double* dpk,
+                                                            double* jacc, const double* Pt, const double* Pa,
+                                                            const double* Pb, double* F, double* G) {
+  const long long np = pair_count(m.N);
+  for (long long t = blockIdx.x * (long long)kBlock + threadIdx.x; t < np; t += (long long)gridDim.x * kBlock) {
+    int u, v;
+    pair_uv(m.N, (int)t, u, v);
+    const int su = m.sprow[u + 1] - m.sprow[u], sv = m.sprow[v + 1] - m.sprow[v];
+    const bool hu = su == 10, hv = sv == 10;
+    const int a = (hu || !hv) ? u : v, b = a == u ? v : u;
+    const double* w = pair_block(m, W, u, v);
+    const int oa = m.ao[a], ob = m.ao[b];
+    if (hu && hv) fock_pair<4, 4, UHF>(m.n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+    else if (hu || hv) fock_pair<4, 1, UHF>(m.n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+    else fock_pair<1, 1, UHF>(m.n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+  }
+}
+// atom-diagonal blocks: H + one-centre J - K + two-centre J
+__global__ void __launch_bounds__(kBlock) fock_diag_kernel(Mol m, const double* H, const double* jacc, const double* Pt,
+                                                           const double* Pa, const double* Pb, double* F, double* G) {
+  const bool uhf = Pb != nullptr;
+  for (int k = blockIdx.x * kBlock + threadIdx.x; k < m.N * 16; k += gridDim.x * kBlock) {
+    const int a = k >> 4, mu = (k >> 2) & 3, nu = k & 3;
+    const ElemDev& e = m.elem[m.z[a]];
+    const int no = e.norb;
+    if (mu >= no || nu >= no) continue;
+    const int oa = m.ao[a];
+    double ja = 0.0, ka = 0.0, kb = 0.0;
+    for (int la = 0; la < no; ++la)
+      for (int si = 0; si < no; ++si) {
+        const double coul = oc_integral(e, mu, nu, la, si), exch = oc_integral(e, mu, la, nu, si);
+        const size_t ix = (size_t)(oa + la) * m.n + oa + si;
+        ja = fma(Pt[ix], coul, ja);
+        if (uhf) {
+          ka = fma(Pa[ix], exch, ka);
+          kb = fma(Pb[ix], exch, kb);
+        } else {
+          ka = fma(0.5 * Pt[ix], exch, ka);
+        }
+      }
+    const size_t ix = (size_t)(oa + mu) * m.n + oa + nu;
+    const double base = H[ix] + jacc[a * 10 + pk(mu, nu)] + ja;
+    F[ix] = base - ka;
+    if (uhf) G[ix] = base - kb;
+  }
+}
+
+// ---------------------------------------------------------------- elementwise helpers
+// E <- E - E^T, zero diagonal (the commutator FP - PF from the product FP)
+__global__ void __launch_bounds__(kBlock) antisym_kernel(double* E, int n) {
+  const size_t nn = (size_t)n * n;
+  for (size_t k = blockIdx.x * (size_t)kBlock + threadIdx.x; k < nn; k += (size_t)gridDim.x * kBlock) {
+    const int i = (int)(k / n), j = (int)(k % n);
+    if (j < i) {
+      const double lo = E[k], up = E[(size_t)j * n + i];
+      E[k] = lo - up;
+      E[(size_t)j * n + i] = up - lo;
+    } else if (j == i) {
+      E[k] = 0.0;
+    }
+  }
+}
+struct Comb {
+  const double* m[8];
+  double c[8];
+  int len;
+};
+// out = sum_l c_l M_l (+ shift (I - Pproj) when shift != 0)
+__global__ void __launch_bounds__(kBlock) combine_kernel(Comb cb, const double* Pproj, double shift, int n, double* out) {
+  const size_t nn = (size_t)n * n;
+  for (size_t k = blockIdx.x * (size_t)kBlock + threadIdx.x; k < nn; k += (size_t)gridDim.x * kBlock) {
+    double v = 0.0;
+    for (int l = 0; l < cb.len; ++l) v = fma(cb.c[l], cb.m[l][k], v);
+    if (shift != 0.0) v += shift * (((k / n) == (k % n) ? 1.0 : 0.0) - Pproj[k]);
+    out[k] = v;
+  }
+}
+// P <- (1 - lam) Pn + lam P (damping, scf.rs:1440-1448); Pn kept
+__global__ void __launch_bounds__(kBlock) damp_kernel(const double* Pn, double* P, double lam, size_t cnt) {
+  for (size_t k = blockIdx.x * (size_t)kBlock + threadIdx.x; k < cnt; k += (size_t)gridDim.x * kBlock)
+    P[k] = (1.0 - lam) * Pn[k] + lam * P[k];
+}
+__global__ void __launch_bounds__(kBlock) add_kernel(const double* a, const double* b, double* out, size_t cnt) {
+  for (size_t k = blockIdx.x * (size_t)kBlock + threadIdx.x; k < cnt; k += (size_t)gridDim.x * kBlock)
+    out[k] = a[k] + b[k];
+}
+// M = 1.5 I - 0.5 G (one Newton-Schulz step towards the orthogonal polar factor)
+__global__ void __launch_bounds__(kBlock) ns_matrix_kernel(const double* G, double* M, int k) {
+  const size_t kk = (size_t)k * k;
+  for (size_t q = blockIdx.x * (size_t)kBlock + threadIdx.x; q < kk; q += (size_t)gridDim.x * kBlock)
+    M[q] = ((q / k) == (q % k) ? 1.5 : 0.0) - 0.5 * G[q];
+}
+// max |G - I|
+__global__ void __launch_bounds__(kBlock) orth_defect_kernel(const double* G, int k, double* partial) {
+  const size_t kk = (size_t)k * k;
+  double s = 0.0;
+  for (size_t q = blockIdx.x * (size_t)kBlock + threadIdx.x; q < kk; q += (size_t)gridDim.x * kBlock)
+    s = fmax(s, fabs(G[q] - ((q / k) == (q % k) ? 1.0 : 0.0)));
+  s = warp_max(s);
+  __shared__ double red[kBlock / 32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < kBlock / 32; ++i) t = fmax(t, red[i]);
+    partial[blockIdx.x] = t;
+  }
+}
+
+// ---------------------------------------------------------------- Householder tridiagonalisation
+// Blocked lower reduction (the LAPACK sytrd/latrd scheme) of a full symmetric row-major A. For
+// the panel starting at p, V and W (n x kPanel, row-major) hold the panel's reflectors and the
+// vectors w_j such that the trailing matrix becomes A - V W^T - W V^T after the panel.
+//
+// Column i = p + j: bring it up to date with the panel's earlier columns, form the reflector
+// (norm over rows > i+1), store v in V[:, j] and below the subdiagonal of column i, and write
+// d_i, e_i, tau_i. One block.
+constexpr int kColThreads = 1024;
+__global__ void __launch_bounds__(kColThreads) panel_column_kernel(double* A, int n, int i, int j, double* V,
+                                                                   const double* W, double* d, double* e,
+                                                                   double* tau) {
+  __shared__ double red[kColThreads / 32];
+  __shared__ double bc[2];
+  // updated column into place, partial norm
+  double part = 0.0;
+  for (int r = i + threadIdx.x; r < n; r += kColThreads) {
+    double a = A[(size_t)r * n + i];
+    for (int k = 0; k < j; ++k) a -= V[(size_t)r * kPanel + k] * W[(size_t)i * kPanel + k] +
+                                     W[(size_t)r * kPanel + k] * V[(size_t)i * kPanel + k];
+    A[(size_t)r * n + i] = a;
+    if (r >= i + 2) part = fma(a, a, part);
+  }
+  part = warp_sum(part);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double xn2 = 0.0;
+    for (int w = 0; w < kColThreads / 32; ++w) xn2 += red[w];
+    const double alpha = A[(size_t)(i + 1) * n + i];
+    double beta = alpha, t = 0.0, sc = 0.0;
+    if (xn2 > 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+      t = (beta - alpha) / beta;
+      sc = 1.0 / (alpha - beta);
+    }
+    d[i] = A[(size_t)i * n + i];
+    e[i] = beta;
+    tau[i] = t;
+    bc[0] = sc;
+    bc[1] = xn2 > 0.0 ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const double sc = bc[0];
+  const bool apply = bc[1] != 0.0;
+  for (int r = threadIdx.x; r < n; r += kColThreads) {
+    double v = 0.0;
+    if (r == i + 1) v = apply ? 1.0 : 0.0;
+    else if (r > i + 1) {
+      v = apply ? A[(size_t)r * n + i] * sc : 0.0;
+      A[(size_t)r * n + i] = v;
+    }
+    V[(size_t)r * kPanel + j] = v;
+  }
+}
+// y = A22 v over rows/cols > i (A22 as of the panel start), one warp per row with v staged in
+// shared memory; also the block partials of s1 = W[:, :j]^T v and s2 = V[:, :j]^T v.
+__global__ void __launch_bounds__(kBlock) panel_symv_kernel(const double* A, int n, int i, int j, const double* V,
+                                                            const double* W, double* y, double* partial_s) {
+  extern __shared__ double vs[];  // n - i - 1 values
+  const int m = n - i - 1;
+  for (int c = threadIdx.x; c < m; c += kBlock) vs[c] = V[(size_t)(i + 1 + c) * kPanel + j];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double s1 = 0.0, s2 = 0.0;  // lane k < j accumulates component k
+  for (int rr = blockIdx.x * (kBlock / 32) + warp; rr < m; rr += gridDim.x * (kBlock / 32)) {
+    const double* row = A + (size_t)(i + 1 + rr) * n + i + 1;
+    double acc0 = 0.0, acc1 = 0.0;
+    int c = lane;
+    for (; c + 32 < m; c += 64) {
+      acc0 = fma(row[c], vs[c], acc0);
+      acc1 = fma(row[c + 32], vs[c + 32], acc1);
+    }
+    if (c < m) acc0 = fma(row[c], vs[c], acc0);
+    const double yr = warp_sum(acc0 + acc1);
+    if (lane == 0) y[rr] = yr;
+    const double vr = vs[rr];
+    if (lane < j) {
+      const size_t ix = (size_t)(i + 1 + rr) * kPanel + lane;
+      s1 = fma(W[ix], vr, s1);
+      s2 = fma(V[ix], vr, s2);
+    }
+  }
+  __shared__ double red[2][kBlock / 32][32];
+  red[0][warp][lane] = s1;
+  red[1][warp][lane] = s2;
+  __syncthreads();
+  if (threadIdx.x < 64) {
+    const int which = threadIdx.x >> 5, k = threadIdx.x & 31;
+    double t = 0.0;
+    for (int w = 0; w < kBlock / 32; ++w) t += red[which][w][k];
+    partial_s[(size_t)blockIdx.x * 64 + threadIdx.x] = t;
+  }
+}
+// s[0..63] = sum over blocks of the symv partials (s1 in 0..31, s2 in 32..63)
+__global__ void __launch_bounds__(64) panel_reduce_kernel(const double* partial_s, int nblocks, double* s) {
+  double t = 0.0;
+  for (int b = 0; b < nblocks; ++b) t += partial_s[(size_t)b * 64 + threadIdx.x];
+  s[threadIdx.x] = t;
+}
+// w = tau (y - V s1 - W s2) over rows > i; block partials of w . v
+__global__ void __launch_bounds__(kBlock) panel_wfix_kernel(int n, int i, int j, const double* V, const double* W,
+                                                            const double* y, const double* s, const double* tau_i,
+                                                            double* wtmp, double* partial) {
+  const int m = n - i - 1;
+  const double t = *tau_i;
+  double dp = 0.0;
+  for (int rr = blockIdx.x * kBlock + threadIdx.x; rr < m; rr += gridDim.x * kBlock) {
+    const size_t r = (size_t)(i + 1 + rr);
+    double w = y[rr];
+    for (int k = 0; k < j; ++k) w -= V[r * kPanel + k] * s[k] + W[r * kPanel + k] * s[32 + k];
+    w *= t;
+    wtmp[rr] = w;
+    dp = fma(w, V[r * kPanel + j], dp);
+  }
+  block_partial(dp, partial);
+}
+// W[:, j] = w - (tau/2)(w . v) v over rows > i (zero above)
+__global__ void __launch_bounds__(kBlock) panel_wfinal_kernel(int n, int i, int j, const double* V, double* W,
+                                                              const double* wtmp, const double* partial, int np,
+                                                              const double* tau_i) {
+  __shared__ double a2s;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int b = 0; b < np; ++b) t += partial[b];
+    a2s = -0.5 * (*tau_i) * t;
+  }
+  __syncthreads();
+  const double a2 = a2s;
+  for (int r = blockIdx.x * kBlock + threadIdx.x; r < n; r += gridDim.x * kBlock) {
+    double w = 0.0;
+    if (r > i) w = wtmp[r - i - 1] + a2 * V[(size_t)r * kPanel + j];
+    W[(size_t)r * kPanel + j] = w;
+  }
+}
+// The last 2 x 2 of the tridiagonal after the final trailing update.
+__global__ void tail_kernel(const double* A, int n, double* d, double* e, double* tau) {
+  if (n >= 2) {
+    d[n - 2] = A[(size_t)(n - 2) * n + n - 2];
+    e[n - 2] = A[(size_t)(n - 1) * n + n - 2];
+    tau[n - 2] = 0.0;
+  }
+  d[n - 1] = A[(size_t)(n - 1) * n + n - 1];
+  e[n - 1] = 0.0;
+}
+// V of the panel [p, p+b) rebuilt from the stored reflectors (for the back-transformation)
+__global__ void __launch_bounds__(kBlock) panel_v_kernel(const double* A, int n, int p, int b, double* V) {
+  for (size_t q = blockIdx.x * (size_t)kBlock + threadIdx.x; q < (size_t)n * kPanel; q += (size_t)gridDim.x * kBlock) {
+    const int r = (int)(q / kPanel), k = (int)(q % kPanel);
+    const int i = p + k;
+    double v = 0.0;
+    if (k < b) v = r <= i ? 0.0 : (r == i + 1 ? 1.0 : A[(size_t)r * n + i]);
+    V[q] = v;
+  }
+}
+// T of the compact WY form H(p) ... H(p+b-1) = I - V T V^T (forward, column-wise), from the
+// Gram G = V^T V (b x b, row-major) and tau; one thread (b <= kPanel).
+__global__ void wy_t_kernel(const double* G, const double* tau, int p, int b, double* T) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int q = 0; q < kPanel * kPanel; ++q) T[q] = 0.0;
+  for (int k = 0; k < b; ++k) {
+    const double tk = tau[p + k];
+    for (int mm = 0; mm < k; ++mm) {
+      double acc = 0.0;
+      for (int l = mm; l < k; ++l) acc = fma(T[mm * kPanel + l], G[l * b + k], acc);
+      T[mm * kPanel + k] = -tk * acc;
+    }
+    T[k * kPanel + k] = tk;
+  }
+}
+
+// ---------------------------------------------------------------- tridiagonal eigenproblem
+// Lowest kval eigenvalues of T (d, e2 with splits already zeroed) by division-free multisection,
+// a group of g lanes per eigenvalue (the per-CTA scheme of cta_eigen.cuh over a whole grid).
+__global__ void __launch_bounds__(kBlock) multisect_kernel(const double* d, const double* e2, int n, int kval,
+                                                           int g, double glo, double ghi, double pivmin, double tnorm,
+                                                           const double* prev, const double* dprev, double* lam) {
+  constexpr double eps = 2.220446049250313e-16;
+  constexpr int kPts = 2;
+  const int gt = blockIdx.x * kBlock + threadIdx.x;
+  const int j = gt / g, gl = gt % g;
+  const int lane = threadIdx.x & 31;
+  const int gbase = lane & ~(g - 1);
+  const unsigned gbits = g == 32 ? 0xffffffffu : ((1u << g) - 1u);
+  const int P = g * kPts;
+  const bool active = j < kval;
+  double lo = glo, hi = ghi;
+  if (prev) {
+    const double c0 = active ? prev[j] : 0.0;
+    const double w0 = active ? fmax(4.0 * fabs(dprev[j]), 1.0e-9 * fmax(tnorm, 1.0)) : 0.0;
+    double x[4];
+    int cn[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const double w = w0 * (t >= 2 ? 64.0 : 1.0);
+      x[t] = (t & 1) ? fmin(c0 + w, ghi) : fmax(c0 - w, glo);
+    }
+    if (active) {
+      sturm_multi<4>(d, e2, n, x, pivmin, cn);
+      if (x[0] < x[1] && cn[0] <= j && cn[1] >= j + 1) {
+        lo = x[0];
+        hi = x[1];
+      } else if (x[2] < x[3] && cn[2] <= j && cn[3] >= j + 1) {
+        lo = x[2];
+        hi = x[3];
+      }
+    }
+  }
+  bool act = active;
+  for (int it = 0; it < 160; ++it) {
+    if (act) {
+      const double mid = 0.5 * (lo + hi);
+      if (hi - lo <= 2.0 * eps * fmax(fabs(lo), fabs(hi)) + 4.0 * pivmin || !(mid > lo && mid < hi)) act = false;
+    }
+    if (!__any_sync(0xffffffffu, act)) break;
+    double x[kPts];
+    int cn[kPts];
+#pragma unroll
+    for (int t = 0; t < kPts; ++t) x[t] = lo + (hi - lo) * (double)(gl * kPts + t + 1) / (double)(P + 1);
+    if (act) sturm_multi<kPts>(d, e2, n, x, pivmin, cn);
+    int tf = kPts;
+#pragma unroll
+    for (int t = kPts - 1; t >= 0; --t)
+      if (act && cn[t] > j) tf = t;
+    const unsigned bal = __ballot_sync(0xffffffffu, act && tf < kPts);
+    const unsigned mine = (bal >> gbase) & gbits;
+    const int src = mine ? gbase + __ffs(mine) - 1 : gbase;
+    const int tsrc = __shfl_sync(0xffffffffu, tf, src);
+    if (act) {
+      double nlo, nhi;
+      if (mine == 0u) {
+        nlo = lo + (hi - lo) * (double)P / (double)(P + 1);
+        nhi = hi;
+      } else {
+        const int f = (src - gbase) * kPts + tsrc;
+        nlo = f > 0 ? lo + (hi - lo) * (double)f / (double)(P + 1) : lo;
+        nhi = lo + (hi - lo) * (double)(f + 1) / (double)(P + 1);
+      }
+      if (!(nhi - nlo < hi - lo)) act = false;
+      else {
+        lo = nlo;
+        hi = nhi;
+      }
+    }
+  }
+  if (active && gl == 0) lam[j] = 0.5 * (lo + hi);
+}
+// Eigenvector j < kvec of T by twisted factorisation (thread per vector), written as column j of
+// Y (n x kvec, row-major); zero outside the unreduced block that holds eigenvalue j. Scratch
+// arrays are interleaved by vector (element i of vector j at i * kvec + j) so a warp's accesses
+// coalesce. `blk` lists the nb + 1 block starts.
+__global__ void __launch_bounds__(kBlock) twisted_kernel(const double* d, const double* e, const double* e2, int n,
+                                                         int kvec, const double* lam, const int* blk, int nb,
+                                                         double pivmin, double tnorm, double* Y, double* Dp, double* Lp,
+                                                         double* Um) {
+  const int j = blockIdx.x * kBlock + threadIdx.x;
+  if (j >= kvec) return;
+  const double lj = lam[j];
+  const double win = 1.0e-11 * fmax(tnorm, 1.0);
+  const size_t K = (size_t)kvec;
+  // which unreduced block holds this eigenvalue (equal eigenvalues go to successive blocks)
+  int pos = j - sturm(d, e2, 0, n - 1, lj - win, pivmin);
+  int b = -1;
+  for (int q = 0; q < nb && b < 0; ++q) {
+    const int lo = blk[q], hi = blk[q + 1] - 1;
+    const int cnt = sturm(d, e2, lo, hi, lj + win, pivmin) - sturm(d, e2, lo, hi, lj - win, pivmin);
+    if (pos < cnt) b = q;
+    else pos -= cnt;
+  }
+  if (b < 0) b = 0;
+  const int lo = blk[b], hi = blk[b + 1] - 1, m = hi - lo + 1;
+  for (int i = 0; i < n; ++i) Y[i * K + j] = 0.0;
+  if (m == 1) {
+    Y[(size_t)lo * K + j] = 1.0;
+    return;
+  }
+  double dp = d[lo] - lj;
+  for (int i = 0; i < m - 1; ++i) {
+    if (fabs(dp) < pivmin) dp = dp < 0.0 ? -pivmin : pivmin;
+    Dp[(lo + i) * K + j] = dp;
+    const double ei = e[lo + i];
+    const double l = ei / dp;
+    Lp[(lo + i) * K + j] = l;
+    dp = (d[lo + i + 1] - lj) - l * ei;
+  }
+  if (fabs(dp) < pivmin) dp = dp < 0.0 ? -pivmin : pivmin;
+  Dp[(size_t)hi * K + j] = dp;
+  double dm = d[hi] - lj;
+  if (fabs(dm) < pivmin) dm = dm < 0.0 ? -pivmin : pivmin;
+  double best = fabs(Dp[(size_t)hi * K + j] + dm - (d[hi] - lj));
+  int r = m - 1;
+  for (int i = m - 2; i >= 0; --i) {
+    const double ei = e[lo + i];
+    const double u = ei / dm;
+    Um[(lo + i) * K + j] = u;
+    dm = (d[lo + i] - lj) - u * ei;
+    if (fabs(dm) < pivmin) dm = dm < 0.0 ? -pivmin : pivmin;
+    const double gm = fabs(Dp[(lo + i) * K + j] + dm - (d[lo + i] - lj));
+    if (gm < best) {
+      best = gm;
+      r = i;
+    }
+  }
+  // N_r D_r N_r^T y = gamma_r e_r
+  double ynext = 1.0, ynext2 = 0.0;  // y[i+1], y[i+2] going up
+  double yrm1 = 0.0;                 // y[r-1], seeds the downward sweep
+  Y[(size_t)(lo + r) * K + j] = 1.0;
+  double nrm = 1.0;
+  for (int i = r - 1; i >= 0; --i) {
+    double zv = -Lp[(lo + i) * K + j] * ynext;
+    if (ynext == 0.0 && i + 2 < m) zv = -(e[lo + i + 1] / e[lo + i]) * ynext2;
+    Y[(size_t)(lo + i) * K + j] = zv;
+    nrm = fma(zv, zv, nrm);
+    if (i == r - 1) yrm1 = zv;
+    ynext2 = ynext;
+    ynext = zv;
+  }
+  double yprev = 1.0, yprev2 = yrm1;  // y[i], y[i-1] going down
+  for (int i = r; i < m - 1; ++i) {
+    double zv = -Um[(lo + i) * K + j] * yprev;
+    if (yprev == 0.0 && i >= 1) zv = -(e[lo + i - 1] / e[lo + i]) * yprev2;
+    Y[(size_t)(lo + i + 1) * K + j] = zv;
+    nrm = fma(zv, zv, nrm);
+    yprev2 = yprev;
+    yprev = zv;
+  }
+  const double sc = 1.0 / sqrt(nrm);
+  for (int i = lo; i <= hi; ++i) Y[(size_t)i * K + j] *= sc;
+}
+
+// ---------------------------------------------------------------- properties
+// per-atom diagonal density blocks (16 per atom, row-major 4 x 4) for charges and dipole
+__global__ void __launch_bounds__(kBlock) atom_blocks_kernel(Mol m, const double* P, double* out) {
+  for (int k = blockIdx.x * kBlock + threadIdx.x; k < m.N * 16; k += gridDim.x * kBlock) {
+    const int a = k >> 4, mu = (k >> 2) & 3, nu = k & 3;
+    const int no = m.elem[m.z[a]].norb;
+    out[k] = (mu < no && nu < no) ? P[(size_t)(m.ao[a] + mu) * m.n + m.ao[a] + nu] : 0.0;
+  }
+}
+
+}  // namespace large
+}  // namespace pm3gpu

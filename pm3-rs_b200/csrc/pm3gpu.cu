@@ -1,5 +1,6 @@
 // Host side of the pm3gpu C ABI: context, job planning, launches and the stability-search
 // driver of run_pm3 (pm3-rs src/scf.rs:450-848).
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -13,6 +14,7 @@
 
 #include "../../include/pm3gpu.h"
 #include "gradient_kernel.cuh"
+#include "large_scf.cuh"
 #include "scf_job.cuh"
 
 using namespace pm3gpu;
@@ -40,6 +42,7 @@ struct DevBuf {
 };
 
 constexpr int kMaxDiisDepthHost = 8;
+constexpr int kMaxLargeAtoms = 30000;  // pair indices of the whole-GPU kernels stay in 32 bits
 // scf.rs:309-331
 int diis_depth(int nao, int mats, int budget_mb) {
   if (budget_mb == 0) return kMaxDiisDepthHost;
@@ -58,7 +61,10 @@ struct Rung {
   bool unrestricted;
 };
 
+struct LargeBufs;
+
 struct MolPlan {
+  bool large = false;  // solved on the whole-GPU path
   int status = 0;
   std::string msg;
   int natom = 0, nao = 0, atom0 = 0;
@@ -89,6 +95,11 @@ struct pm3gpu_ctx {
   bool profile = false;
   DevBuf prof;
   double phase_cycles[kPhases] = {};
+  // whole-GPU path for large molecules
+  cublasHandle_t blas = nullptr;
+  int large_min = kMaxN + 1;  // molecules with at least this many basis functions
+  LargeBufs* lbuf = nullptr;
+  DevBuf lsel;                // densities of the selected state (P_tot | P_alpha | P_beta)
 };
 
 namespace {
@@ -172,11 +183,12 @@ void plan_molecule(const pm3gpu_ctx* c, const int32_t* z, const double* xyz, int
     return;
   }
   m.use_uhf = o->reference == PM3GPU_REF_UHF || (o->reference == PM3GPU_REF_AUTO && m.n_alpha != m.n_beta);
-  if (nao > kMaxN || natom > kMaxN) {
+  if (natom > kMaxLargeAtoms) {
     m.status = PM3GPU_UNSUPPORTED;
-    m.msg = "molecule exceeds the per-CTA path (nao <= " + std::to_string(kMaxN) + ")";
+    m.msg = "molecule exceeds " + std::to_string(kMaxLargeAtoms) + " atoms";
     return;
   }
+  m.large = nao >= c->large_min || nao > kMaxN || natom > kMaxN;
   m.steered = o->level_shift_ev != 0.0 || o->damping != 0.0;
 }
 
@@ -409,7 +421,8 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
 
 // Gradients of the selected states of `mols` (one thread per atom pair of the whole batch).
 int launch_gradients(pm3gpu_ctx* c, const std::vector<GradMol>& mols, const std::vector<int32_t>& ao_off,
-                     const int32_t* d_z, const double* d_xyz, size_t total_atoms, std::vector<double>& grads) {
+                     const int32_t* d_z, const double* d_xyz, size_t total_atoms, std::vector<double>& grads,
+                     const double* dens = nullptr) {
   grads.assign(3 * total_atoms, 0.0);
   if (mols.empty()) return PM3GPU_OK;
   long long npairs = mols.back().pair0 + (long long)mols.back().natom * (mols.back().natom - 1) / 2;
@@ -429,7 +442,7 @@ int launch_gradients(pm3gpu_ctx* c, const std::vector<GradMol>& mols, const std:
     g.mols = c->gmols.as<GradMol>();
     g.nmol = (int)mols.size();
     g.npairs = npairs;
-    g.dens = c->dens.as<double>();
+    g.dens = dens ? dens : c->dens.as<double>();
     g.grad = c->grads.as<double>();
     const long long blocks = std::min<long long>((npairs + 127) / 128, (long long)c->sms * 16);
     gradient_kernel<<<(unsigned)blocks, 128, 0, c->stream>>>(g);
@@ -440,6 +453,146 @@ int launch_gradients(pm3gpu_ctx* c, const std::vector<GradMol>& mols, const std:
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->h2d += (long long)(sizeof(GradMol) * mols.size() + 4 * ao_off.size());
   c->d2h += (long long)(24 * total_atoms);
+  return PM3GPU_OK;
+}
+
+#include "large_driver.cuh"
+
+// run_pm3 (scf.rs:450-848) for one molecule on the whole-GPU path: the first pass, the
+// stability rungs in the reference's order when the search triggers, the same selection, then
+// the epilogue and (optionally) the gradient at the selected state.
+int run_large(pm3gpu_ctx* c, const MolPlan& p, const int32_t* hz, const int32_t* dz, const double* dxyz,
+              const pm3gpu_options* o, const Want& want, pm3gpu_result& Rm, double* charges, double* density,
+              double* mo_energies, double* gradient) {
+  if (!c->blas) BLAS_TRY(c, cublasCreate(&c->blas));
+  BLAS_TRY(c, cublasSetStream(c->blas, c->stream));
+  if (!c->lbuf) c->lbuf = new LargeBufs();
+  LargeSolver S(c, *c->lbuf);
+  double ecc = 0.0;
+  int rc = S.setup(hz, dz, dxyz, p.natom, p.nao, &ecc);
+  if (rc != PM3GPU_OK) return rc;
+  const size_t nn = (size_t)p.nao * p.nao;
+  const bool keep_dens = want.density || want.grad;
+  auto save = [&](const LargeRun& run) -> int {  // densities of the state that is currently selected
+    if (!keep_dens) return PM3GPU_OK;
+    CUDA_TRY(c, c->lsel.ensure(8 * nn * (run.uhf ? 3 : 1)));
+    CUDA_TRY(c, cudaMemcpyAsync(c->lsel.p, S.final_pt(), 8 * nn, cudaMemcpyDeviceToDevice, c->stream));
+    if (run.uhf) {
+      CUDA_TRY(c, cudaMemcpyAsync(c->lsel.as<double>() + nn, S.final_pa(), 8 * nn, cudaMemcpyDeviceToDevice, c->stream));
+      CUDA_TRY(c, cudaMemcpyAsync(c->lsel.as<double>() + 2 * nn, S.final_pb(), 8 * nn, cudaMemcpyDeviceToDevice,
+                                  c->stream));
+    }
+    return PM3GPU_OK;
+  };
+  const JobDesc fj = p.steered ? make_job(p, o->guess, o->accelerator, o->level_shift_ev, o->damping, false, 0)
+                               : make_job(p, o->guess, o->accelerator, 0.0, 0.0, false, 0);
+  LargeRun st;
+  rc = S.scf(fj, st);
+  if (rc != PM3GPU_OK) return rc;
+  if ((rc = save(st)) != PM3GPU_OK) return rc;
+  bool st_unres = (fj.flags & kJobUhf) != 0;
+  const double first_ev = st.o.electronic;
+  int paths = 1;
+  const bool search = o->stability == PM3GPU_STABILITY_OFF
+                          ? false
+                          : (o->stability == PM3GPU_STABILITY_ALWAYS ? !p.steered : (!p.steered && st.o.gap < 6.0));
+  if (search) {  // scf.rs:610-715
+    const int primary = o->guess == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_CORE : PM3GPU_GUESS_SAD;
+    const int other = primary == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_SAD : PM3GPU_GUESS_CORE;
+    const bool closed = !p.use_uhf;
+    const Rung all[7] = {{primary, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                         {other, o->accelerator, 0.0, 0.0, false},
+                         {other, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                         {PM3GPU_GUESS_SYMMETRY_BROKEN, o->accelerator, 0.0, 0.0, false},
+                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, -2.0, 0.0, closed},
+                         {primary, PM3GPU_ACCEL_CDIIS, 0.0, 0.85, closed}};
+    for (const Rung& r : all) {
+      if (r.unrestricted != closed) continue;
+      ++paths;
+      const JobDesc rj = make_job(p, r.guess, r.accel, r.shift, r.damp, r.unrestricted, 0);
+      LargeRun cand;
+      if (S.scf(rj, cand) != PM3GPU_OK) continue;
+      if (!cand.o.converged) continue;
+      bool cand_unres = (rj.flags & kJobUhf) != 0;
+      if (r.unrestricted) {  // a spin-pure unrestricted closed shell is a restricted state
+        if (!(cand.o.spin_max < 1.0e-8)) continue;
+        cand_unres = false;
+        cand.o.homo = cand.o.homo_a;
+        cand.o.lumo = cand.o.lumo_a;
+        cand.o.has_homo = cand.o.has_homo_a;
+        cand.o.has_lumo = cand.o.has_lumo_a;
+      }
+      if (!st.o.converged || cand.o.electronic < st.o.electronic - 1.0e-6) {
+        st = std::move(cand);
+        st_unres = cand_unres;
+        if ((rc = save(st)) != PM3GPU_OK) return rc;
+      }
+    }
+  }
+  double e_isol = 0.0, eheat = 0.0;
+  for (int a = 0; a < p.natom; ++a) {
+    e_isol += c->h_elem[hz[a]].e_isol;
+    eheat += c->h_elem[hz[a]].eheat_ev;
+  }
+  const JobOut& so = st.o;
+  Rm.status = PM3GPU_OK;
+  Rm.nao = p.nao;
+  Rm.n_occ = p.n_alpha;
+  Rm.n_beta = st_unres ? p.n_beta : p.n_alpha;
+  Rm.electronic_ev = so.electronic;
+  Rm.core_ev = ecc;
+  Rm.total_ev = so.electronic + ecc;
+  Rm.heat_of_formation_kcal = (Rm.total_ev - e_isol + eheat) * kEvToKcal;
+  Rm.iterations = so.iterations;
+  Rm.converged = so.converged;
+  Rm.unrestricted = st_unres ? 1 : 0;
+  Rm.scf_paths_tried = paths;
+  Rm.scf_improvement_ev = std::max(first_ev - so.electronic, 0.0);
+  Rm.last_change = so.last_change;
+  Rm.homo_ev = so.homo;
+  Rm.lumo_ev = so.lumo;
+  Rm.has_homo = so.has_homo;
+  Rm.has_lumo = so.has_lumo;
+  for (int k = 0; k < 3; ++k) Rm.dipole_debye[k] = so.dipole[k];
+  Rm.dipole_magnitude = std::sqrt(Rm.dipole_debye[0] * Rm.dipole_debye[0] + Rm.dipole_debye[1] * Rm.dipole_debye[1] +
+                                  Rm.dipole_debye[2] * Rm.dipole_debye[2]);
+  if (!so.converged) {
+    Rm.status = PM3GPU_SCF_NOT_CONVERGED;
+    char msg[160];
+    std::snprintf(msg, sizeof msg, "PM3 SCF did not converge after %d iterations (error=%.3e)", so.iterations,
+                  so.last_change);
+    c->err = msg;
+  }
+  if (charges) std::memcpy(charges, st.charges.data(), 8 * (size_t)p.natom);
+  if (density && want.density) {
+    CUDA_TRY(c, cudaMemcpyAsync(density, c->lsel.p, 8 * nn, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  if (mo_energies && want.eps) {
+    std::vector<double> all;
+    if ((rc = S.all_eigenvalues(st.tri_a, all)) != PM3GPU_OK) return rc;
+    std::memcpy(mo_energies, all.data(), 8 * (size_t)p.nao);
+  }
+  if (want.grad && gradient && so.converged) {
+    std::vector<int32_t> ao_off(p.natom);
+    for (int a = 0, off = 0; a < p.natom; ++a) {
+      ao_off[a] = off;
+      off += c->h_elem[hz[a]].norb;
+    }
+    GradMol g{};
+    g.atom0 = 0;
+    g.natom = p.natom;
+    g.nao = p.nao;
+    g.uhf = st_unres ? 1 : 0;
+    if (!st.uhf) g.uhf = 0;
+    g.pair0 = 0;
+    g.dens_off = 0;
+    std::vector<double> gr;
+    rc = launch_gradients(c, {g}, ao_off, dz, dxyz, (size_t)p.natom, gr, c->lsel.as<double>());
+    if (rc != PM3GPU_OK) return rc;
+    std::memcpy(gradient, gr.data(), 24 * (size_t)p.natom);
+  }
   return PM3GPU_OK;
 }
 
@@ -484,7 +637,7 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
     if (na < 0) return fail(c, PM3GPU_INVALID_INPUT, "atom_offsets must be non-decreasing");
     const pm3gpu_options* o = per_mol ? opts + m : opts;
     plan_molecule(c, h_z + p.atom0, h_xyz ? h_xyz + 3 * (size_t)p.atom0 : nullptr, na, o, p);
-    if (p.status != PM3GPU_OK) continue;
+    if (p.status != PM3GPU_OK || p.large) continue;  // large molecules: whole-GPU path below
     JobDesc j = p.steered ? make_job(p, o->guess, o->accelerator, o->level_shift_ev, o->damping, false, 0)
                           : make_job(p, o->guess, o->accelerator, 0.0, 0.0, false, 0);
     j.mol = m;
@@ -545,6 +698,17 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
     Rm.nao = p.nao;
     if (p.status != PM3GPU_OK) {
       if (c->err.empty() || n_mol == 1) c->err = p.msg;
+      continue;
+    }
+    if (p.large) {
+      const pm3gpu_options* o = per_mol ? opts + m : opts;
+      const int rl = run_large(c, p, h_z + p.atom0, dz + p.atom0, dxyz + 3 * (size_t)p.atom0, o, want, Rm,
+                               charges ? charges + p.atom0 : nullptr, density, mo_energies,
+                               (want.grad && gradients) ? gradients + 3 * (size_t)p.atom0 : nullptr);
+      if (rl != PM3GPU_OK) {
+        Rm.status = rl;
+        if (n_mol == 1) return rl;
+      }
       continue;
     }
     const JobDesc& fj = jobs[p.first_job];
@@ -616,7 +780,7 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
     long long pair0 = 0;
     for (int m = 0; m < n_mol; ++m) {
       const MolPlan& p = plans[m];
-      if (p.status != PM3GPU_OK || !chosen[m].o.converged) continue;
+      if (p.status != PM3GPU_OK || p.large || !chosen[m].o.converged) continue;
       int off = 0;
       for (int a = 0; a < p.natom; ++a) {
         ao_off[p.atom0 + a] = off;
@@ -639,7 +803,7 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
     if (rc != PM3GPU_OK) return rc;
     for (int m = 0; m < n_mol; ++m) {
       const MolPlan& p = plans[m];
-      if (p.status != PM3GPU_OK || !chosen[m].o.converged) continue;
+      if (p.status != PM3GPU_OK || p.large || !chosen[m].o.converged) continue;
       std::memcpy(gradients + 3 * (size_t)p.atom0, gr.data() + 3 * (size_t)p.atom0, 24 * (size_t)p.natom);
     }
   }
@@ -745,6 +909,12 @@ void pm3gpu_context_destroy(pm3gpu_ctx* c) {
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   for (int k = 0; k < 2; ++k)
     if (c->kev[k]) cudaEventDestroy(c->kev[k]);
+  if (c->lbuf) {
+    c->lbuf->release();
+    delete c->lbuf;
+  }
+  c->lsel.release();
+  if (c->blas) cublasDestroy(c->blas);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
 }
@@ -912,6 +1082,14 @@ int pm3gpu_last_timings(pm3gpu_ctx* c, double* ms, int max_entries) {
 }
 
 int pm3gpu_last_kernel_launches(pm3gpu_ctx* c) { return c ? c->launches : 0; }
+
+int pm3gpu_set_large_threshold(pm3gpu_ctx* c, int nao) {
+  if (!c) return PM3GPU_INVALID_INPUT;
+  if (nao < 1 || nao > kMaxN + 1) return fail(c, PM3GPU_INVALID_INPUT, "large-path threshold outside 1..257");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->large_min = nao;
+  return PM3GPU_OK;
+}
 
 int pm3gpu_last_phase_cycles(pm3gpu_ctx* c, double* cycles, int max_entries) {
   if (!c || !cycles) return 0;

@@ -193,6 +193,58 @@ __device__ void setup_job(Ctx& c) {
   __syncthreads();
 }
 
+// One atom pair of H_core (hamiltonian.rs:191-344): both atoms' electron-core attraction blocks
+// (added to their packed diagonal accumulators), the pair table block W in (a, b) orientation (a
+// the atom with more orbitals), and the resonance block H_ab = (beta_i + beta_j)/2 S_ij written to
+// both triangles of H (row stride n). Returns the pair's core-core energy (repulsion.rs:57-120),
+// evaluated with the atoms in the caller's (u, v) order.
+__device__ __forceinline__ double core_pair(const ElemDev& ea, const ElemDev& eb, const ElemDev& eu, const ElemDev& ev,
+                                            const PairDev& pp, const double* xa, const double* xb, int oa, int ob,
+                                            size_t n, double* hacc_a, double* hacc_b, double* w, double* H) {
+  const double d[3] = {xb[0] - xa[0], xb[1] - xa[1], xb[2] - xa[2]};
+  const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  const double dv[3] = {d[0] / r * r, d[1] / r * r, d[2] / r * r};
+  const double mdv[3] = {-dv[0], -dv[1], -dv[2]};
+  double blk[10];
+  core_attraction(ea, eb, dv, blk);
+  for (int k = 0; k < (ea.norb == 4 ? 10 : 1); ++k) atomicAdd(&hacc_a[k], blk[k]);
+  core_attraction(eb, ea, mdv, blk);
+  for (int k = 0; k < (eb.norb == 4 ? 10 : 1); ++k) atomicAdd(&hacc_b[k], blk[k]);
+  const double ir = 1.0 / r;
+  double R[9];
+  frame(-(dv[0] * ir), -(dv[1] * ir), -(dv[2] * ir), R);
+  const double rv = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+  if (ea.norb == 1) {
+    const double s = ea.rho0 + eb.rho0;
+    w[0] = rsq(rv * rv + s * s) * kEv;
+  } else if (eb.norb == 1) {
+    double ri[4];
+    local4(ee_pole(ea), eb.rho0, rv, ri);
+    for (int kk = 0; kk < 4; ++kk)
+      for (int ll = 0; ll <= kk; ++ll) w[pk(kk, ll)] = w4(ri, R, kk, ll);
+  } else {
+    double ri[22];
+    local22(ee_pole(ea), ee_pole(eb), rv, ri);
+    for (int kk = 0; kk < 4; ++kk)
+      for (int ll = 0; ll <= kk; ++ll)
+        for (int mm = 0; mm < 4; ++mm)
+          for (int nn = 0; nn <= mm; ++nn) w[pk(kk, ll) * 10 + pk(mm, nn)] = w22(ri, R, kk, ll, mm, nn);
+  }
+  double s[16];
+  overlap_block(ea, eb, d, s);
+  for (int i = 0; i < ea.norb; ++i) {
+    const double bi = i == 0 ? ea.bs : ea.bp;
+    for (int j = 0; j < eb.norb; ++j) {
+      const double bj = j == 0 ? eb.bs : eb.bp;
+      const double h = 0.5 * (bi + bj) * s[i * 4 + j];
+      H[(size_t)(oa + i) * n + ob + j] = h;
+      H[(size_t)(ob + j) * n + oa + i] = h;
+    }
+  }
+  const double dd = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  return core_core(eu, ev, pp, dd);
+}
+
 // H_core (hamiltonian.rs:191-344) and the pair table W; returns the core-core energy
 // (repulsion.rs:13-27) to every thread.
 __device__ double build_core(Ctx& c) {
@@ -208,53 +260,9 @@ __device__ double build_core(Ctx& c) {
     pair_uv(N, t, u, v);
     const bool hu = heavy(c, u), hv = heavy(c, v);
     const int a = (hu || !hv) ? u : v, b = a == u ? v : u;
-    const ElemDev& ea = A.elem[c.sz[a]];
-    const ElemDev& eb = A.elem[c.sz[b]];
-    const double d[3] = {c.sxyz[3 * b] - c.sxyz[3 * a], c.sxyz[3 * b + 1] - c.sxyz[3 * a + 1], c.sxyz[3 * b + 2] - c.sxyz[3 * a + 2]};
-    const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-    const double dv[3] = {d[0] / r * r, d[1] / r * r, d[2] / r * r};
-    const double mdv[3] = {-dv[0], -dv[1], -dv[2]};
-    double blk[10];
-    core_attraction(ea, eb, dv, blk);
-    for (int k = 0; k < (ea.norb == 4 ? 10 : 1); ++k) atomicAdd(&hacc[a * 10 + k], blk[k]);
-    core_attraction(eb, ea, mdv, blk);
-    for (int k = 0; k < (eb.norb == 4 ? 10 : 1); ++k) atomicAdd(&hacc[b * 10 + k], blk[k]);
-    // pair table in (a, b) orientation
-    double* w = c.W + woff(c, u, v);
-    const double ir = 1.0 / r;
-    double R[9];
-    frame(-(dv[0] * ir), -(dv[1] * ir), -(dv[2] * ir), R);
-    const double rv = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
-    if (ea.norb == 1) {
-      const double s = ea.rho0 + eb.rho0;
-      w[0] = rsq(rv * rv + s * s) * kEv;
-    } else if (eb.norb == 1) {
-      double ri[4];
-      local4(ee_pole(ea), eb.rho0, rv, ri);
-      for (int kk = 0; kk < 4; ++kk)
-        for (int ll = 0; ll <= kk; ++ll) w[pk(kk, ll)] = w4(ri, R, kk, ll);
-    } else {
-      double ri[22];
-      local22(ee_pole(ea), ee_pole(eb), rv, ri);
-      for (int kk = 0; kk < 4; ++kk)
-        for (int ll = 0; ll <= kk; ++ll)
-          for (int mm = 0; mm < 4; ++mm)
-            for (int nn = 0; nn <= mm; ++nn) w[pk(kk, ll) * 10 + pk(mm, nn)] = w22(ri, R, kk, ll, mm, nn);
-    }
-    double s[16];
-    overlap_block(ea, eb, d, s);
-    const int oa = c.soff[a], ob = c.soff[b];
-    for (int i = 0; i < ea.norb; ++i) {
-      const double bi = i == 0 ? ea.bs : ea.bp;
-      for (int j = 0; j < eb.norb; ++j) {
-        const double bj = j == 0 ? eb.bs : eb.bp;
-        const double h = 0.5 * (bi + bj) * s[i * 4 + j];
-        c.H[(size_t)(oa + i) * n + ob + j] = h;
-        c.H[(size_t)(ob + j) * n + oa + i] = h;
-      }
-    }
-    const double dd = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-    ecc += (u < v) ? core_core(A.elem[c.sz[u]], A.elem[c.sz[v]], *A.pairs, dd) : 0.0;
+    ecc += core_pair(A.elem[c.sz[a]], A.elem[c.sz[b]], A.elem[c.sz[u]], A.elem[c.sz[v]], *A.pairs, c.sxyz + 3 * a,
+                     c.sxyz + 3 * b, c.soff[a], c.soff[b], (size_t)n, hacc + a * 10, hacc + b * 10, c.W + woff(c, u, v),
+                     c.H);
   }
   __syncthreads();
   // diagonal blocks: U + sum of electron-core attractions
@@ -437,7 +445,7 @@ __device__ void commutator(Ctx& c, const double* Fm, const double* Pm, double* E
 
 // ------------------------------------------------------------ small dense solves (thread 0)
 // Pulay coefficients from the Gram matrix (scf.rs:1544-1630); false = singular / unusable.
-__device__ bool cdiis_coeffs(int m, const double* gram, double* x) {
+__host__ __device__ bool cdiis_coeffs(int m, const double* gram, double* x) {
   if (m < 2) return false;
   double scale = 0.0;
   for (int i = 0; i < m * m; ++i) scale = fmax(scale, fabs(gram[(i / m) * kMaxDepth + i % m]));
