@@ -207,6 +207,11 @@ int pm3gpu_last_kernel_launches(pm3gpu_ctx* ctx);
  * reference has one CPU path). */
 int pm3gpu_set_large_threshold(pm3gpu_ctx* ctx, int nao);
 
+/* Wall-clock ms per phase of the last whole-GPU solve (core, Fock, DIIS, tridiagonalise,
+ * eigenvalues, eigenvectors, back-transform, orthonormalise, density), when the context was
+ * created with PM3GPU_PROFILE=1 (each phase then waits for the stream); returns the count. */
+int pm3gpu_last_large_phase_ms(pm3gpu_ctx* ctx, double* ms, int max_entries);
+
 #ifdef __cplusplus
 }
 #endif

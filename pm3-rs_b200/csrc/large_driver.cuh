@@ -19,12 +19,12 @@ struct LargeBufs {
   DevBuf H, W, hacc, dpk, jacc, part, scal;
   DevBuf P[2], Q[2], Pt, F, G, hist, A;
   DevBuf d, e, e2, tau, lam, dlam, blk;
-  DevBuf V, Wp, y, wtmp, ps, s64;
+  DevBuf V, Wp, y, wtmp, ps, s64, vcol;
   DevBuf X, Xt, Dp, Lp, Um;
   DevBuf Gm, Mm, Tm, Z1, Z2, blocks, Gk;
   void release() {
     for (DevBuf* b : {&ao, &sprow, &sroff, &H, &W, &hacc, &dpk, &jacc, &part, &scal, &P[0], &P[1], &Q[0], &Q[1], &Pt,
-                      &F, &G, &hist, &A, &d, &e, &e2, &tau, &lam, &dlam, &blk, &V, &Wp, &y, &wtmp, &ps, &s64, &X, &Xt,
+                      &F, &G, &hist, &A, &d, &e, &e2, &tau, &lam, &dlam, &blk, &V, &Wp, &y, &wtmp, &ps, &s64, &vcol, &X, &Xt,
                       &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk})
       b->release();
   }
@@ -37,6 +37,11 @@ struct LargeRun {
   std::vector<double> eps_a, eps_b;      // eigenvalues of the last iteration (n_occ + 1 each)
   std::vector<double> tri_a, tri_b;      // saved tridiagonals (d | e) of the last iteration
   std::vector<double> charges;
+};
+
+// Phases of the whole-GPU path (wall-clock ms when profiling).
+enum LargePhase : int {
+  kLgCore = 0, kLgFock, kLgDiis, kLgTridiag, kLgEigval, kLgEigvec, kLgBack, kLgOrth, kLgDensity, kLgPhases
 };
 
 #define BLAS_TRY(ctx, call)                                                                        \
@@ -162,6 +167,7 @@ class LargeSolver {
     CUDA_TRY(c_, cudaGetLastError());
     CUDA_TRY(c_, cudaMemcpyAsync(ecc, B_.scal.p, 8, cudaMemcpyDeviceToHost, c_->stream));
     CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+    tick(kLgCore);
     return PM3GPU_OK;
   }
 
@@ -276,6 +282,7 @@ class LargeSolver {
         if ((rc = dot(Pt, B_.H.as<double>(), nullptr, nullptr, &h1)) || (rc = dot(Pc, Fa, Qc, Fb, &h2))) return rc;
         e_elec = 0.5 * (h1 + h2);
       }
+      tick(kLgFock);
       // ---- accelerator (scf.rs:1240-1259 RHF; 1398-1413 UHF)
       bool use_hist = false;
       if (J.accel != 0) {
@@ -314,6 +321,7 @@ class LargeSolver {
         }
         ++len;
         use_hist = ok;
+        tick(kLgDiis);
       }
       // ---- diagonalise (level shift for UHF only, scf.rs:1416-1418) and rebuild densities
       double sq_a = 0.0, sq_b = 0.0;
@@ -344,6 +352,7 @@ class LargeSolver {
         double* Pnew = spin == 0 ? Pn : Qn;
         rc = density_from_x(occ, occ, uhf ? 1.0 : 2.0, Pnew);
         if (rc) return rc;
+        tick(kLgDensity);
         double sq;
         if ((rc = sqdiff(Pnew, Pold, &sq))) return rc;
         (spin == 0 ? sq_a : sq_b) = sq;
@@ -600,7 +609,7 @@ class LargeSolver {
                  std::vector<double>* tri) {
     const int n = n_;
     const size_t K = (size_t)std::max(kvec, 1);
-    for (DevBuf* b : {&B_.d, &B_.e, &B_.tau, &B_.y, &B_.wtmp}) CUDA_TRY(c_, b->ensure(8 * (size_t)n));
+    for (DevBuf* b : {&B_.d, &B_.e, &B_.tau, &B_.y, &B_.wtmp, &B_.vcol}) CUDA_TRY(c_, b->ensure(8 * (size_t)n));
     CUDA_TRY(c_, B_.V.ensure(8 * (size_t)n * large::kPanel));
     CUDA_TRY(c_, B_.Wp.ensure(8 * (size_t)n * large::kPanel));
     CUDA_TRY(c_, B_.ps.ensure(8 * 64 * (size_t)large::kRedBlocks));
@@ -612,25 +621,23 @@ class LargeSolver {
     double* W = B_.Wp.as<double>();
     const double one = 1.0, mone = -1.0, zero = 0.0;
     // ---- 1. Householder tridiagonalisation (sytrd/latrd, lower)
-    const int smem_max = 8 * n;
-    CUDA_TRY(c_, cudaFuncSetAttribute(large::panel_symv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      std::max(smem_max, 1024)));
+    double* vcol = B_.vcol.as<double>();
     for (int p = 0; p < n - 2; p += large::kPanel) {
       const int b = std::min(large::kPanel, n - 2 - p);
       for (int j = 0; j < b; ++j) {
         const int i = p + j;
         const int m = n - i - 1;
-        large::panel_column_kernel<<<1, large::kColThreads, 0, c_->stream>>>(A, n, i, j, V, W, d, e, tau);
-        const int gs = std::max(1, std::min((m + 7) / 8, 4 * c_->sms));
-        large::panel_symv_kernel<<<gs, large::kBlock, 8 * (size_t)m, c_->stream>>>(A, n, i, j, V, W, B_.y.as<double>(),
-                                                                                    B_.ps.as<double>());
-        large::panel_reduce_kernel<<<1, 64, 0, c_->stream>>>(B_.ps.as<double>(), gs, B_.s64.as<double>());
+        large::panel_column_kernel<<<1, large::kColThreads, 0, c_->stream>>>(A, n, i, j, V, W, vcol, d, e, tau);
+        const int gs = std::max(1, std::min(std::min((m + 7) / 8, 8 * c_->sms), large::kRedBlocks));
+        large::panel_symv_kernel<<<gs, large::kBlock, 0, c_->stream>>>(A, n, i, j, vcol, V, W, B_.y.as<double>(),
+                                                                       B_.ps.as<double>());
+        large::panel_reduce_kernel<<<64, large::kBlock, 0, c_->stream>>>(B_.ps.as<double>(), gs, B_.s64.as<double>());
         const int gw = grid_for((size_t)m, large::kBlock, 4 * c_->sms);
-        large::panel_wfix_kernel<<<gw, large::kBlock, 0, c_->stream>>>(n, i, j, V, W, B_.y.as<double>(),
+        large::panel_wfix_kernel<<<gw, large::kBlock, 0, c_->stream>>>(n, i, j, V, W, vcol, B_.y.as<double>(),
                                                                         B_.s64.as<double>(), tau + i,
                                                                         B_.wtmp.as<double>(), B_.part.as<double>());
         large::panel_wfinal_kernel<<<grid_for((size_t)n, large::kBlock, 4 * c_->sms), large::kBlock, 0, c_->stream>>>(
-            n, i, j, V, W, B_.wtmp.as<double>(), B_.part.as<double>(), gw, tau + i);
+            n, i, j, vcol, W, B_.wtmp.as<double>(), B_.part.as<double>(), gw, tau + i);
         c_->launches += 5;
       }
       const int q = p + b, m = n - q;
@@ -647,6 +654,7 @@ class LargeSolver {
     large::tail_kernel<<<1, 1, 0, c_->stream>>>(A, n, d, e, tau);
     ++c_->launches;
     CUDA_TRY(c_, cudaGetLastError());
+    tick(kLgTridiag);
     // ---- 2. eigenvalues (host split bookkeeping, device multisection)
     {
       std::vector<double> hd(n), he(n);
@@ -661,6 +669,7 @@ class LargeSolver {
       int rc = eigenvalues_host(hd, he, kval, lam, dl, warm);
       if (rc) return rc;
     }
+    tick(kLgEigval);
     if (kvec <= 0) return PM3GPU_OK;
     // ---- 3. eigenvectors of the tridiagonal
     CUDA_TRY(c_, B_.X.ensure(8 * (size_t)n * K));
@@ -672,6 +681,7 @@ class LargeSolver {
         X, B_.Dp.as<double>(), B_.Lp.as<double>(), B_.Um.as<double>());
     ++c_->launches;
     CUDA_TRY(c_, cudaGetLastError());
+    tick(kLgEigvec);
     // ---- 4. back-transformation X <- Q X, panels from the last to the first
     CUDA_TRY(c_, B_.Gm.ensure(8 * (size_t)large::kPanel * large::kPanel));
     CUDA_TRY(c_, B_.Tm.ensure(8 * (size_t)large::kPanel * large::kPanel));
@@ -700,6 +710,7 @@ class LargeSolver {
       BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, (int)K, m, b, &mone, B_.Z2.as<double>(), (int)K, Vr,
                                large::kPanel, &one, Xr, (int)K));
     }
+    tick(kLgBack);
     // ---- 5. orthonormalise: X <- X (3I - X^T X) / 2 until max |X^T X - I| < 1e-13
     CUDA_TRY(c_, B_.Mm.ensure(8 * K * K));
     CUDA_TRY(c_, B_.Gk.ensure(8 * K * K));
@@ -724,6 +735,7 @@ class LargeSolver {
       std::swap(B_.X, B_.Xt);
       X = B_.X.as<double>();
     }
+    tick(kLgOrth);
     return PM3GPU_OK;
   }
 
@@ -765,4 +777,15 @@ class LargeSolver {
   }
 
   double pivmin_ = 0.0, tnorm_ = 0.0;
+  std::chrono::steady_clock::time_point t0_ = std::chrono::steady_clock::now();
+
+ public:
+  // Phase clock (profiling only: each tick waits for the stream).
+  void tick(int phase) {
+    if (!c_->profile) return;
+    cudaStreamSynchronize(c_->stream);
+    const auto t = std::chrono::steady_clock::now();
+    c_->large_ms[phase] += std::chrono::duration<double, std::milli>(t - t0_).count();
+    t0_ = t;
+  }
 };

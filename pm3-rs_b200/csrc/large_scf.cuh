@@ -278,21 +278,23 @@ __global__ void __launch_bounds__(kBlock) orth_defect_kernel(const double* G, in
 // vectors w_j such that the trailing matrix becomes A - V W^T - W V^T after the panel.
 //
 // Column i = p + j: bring it up to date with the panel's earlier columns, form the reflector
-// (norm over rows > i+1), store v in V[:, j] and below the subdiagonal of column i, and write
-// d_i, e_i, tau_i. One block.
+// (norm over rows > i+1), and write d_i, e_i, tau_i. The trailing matrix is kept symmetric, so
+// column i below the diagonal is read from row i (contiguous). The reflector v (1 at i+1) goes
+// to V[:, j], to the contiguous vector vcol, and to row i right of the subdiagonal (A[i][r],
+// r >= i+2; row i is not read again), where the back-transformation finds it. One block.
 constexpr int kColThreads = 1024;
 __global__ void __launch_bounds__(kColThreads) panel_column_kernel(double* A, int n, int i, int j, double* V,
-                                                                   const double* W, double* d, double* e,
+                                                                   const double* W, double* vcol, double* d, double* e,
                                                                    double* tau) {
   __shared__ double red[kColThreads / 32];
   __shared__ double bc[2];
-  // updated column into place, partial norm
+  double* rowi = A + (size_t)i * n;
   double part = 0.0;
   for (int r = i + threadIdx.x; r < n; r += kColThreads) {
-    double a = A[(size_t)r * n + i];
+    double a = rowi[r];
     for (int k = 0; k < j; ++k) a -= V[(size_t)r * kPanel + k] * W[(size_t)i * kPanel + k] +
                                      W[(size_t)r * kPanel + k] * V[(size_t)i * kPanel + k];
-    A[(size_t)r * n + i] = a;
+    rowi[r] = a;
     if (r >= i + 2) part = fma(a, a, part);
   }
   part = warp_sum(part);
@@ -301,14 +303,14 @@ __global__ void __launch_bounds__(kColThreads) panel_column_kernel(double* A, in
   if (threadIdx.x == 0) {
     double xn2 = 0.0;
     for (int w = 0; w < kColThreads / 32; ++w) xn2 += red[w];
-    const double alpha = A[(size_t)(i + 1) * n + i];
+    const double alpha = rowi[i + 1];
     double beta = alpha, t = 0.0, sc = 0.0;
     if (xn2 > 0.0) {
       beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
       t = (beta - alpha) / beta;
       sc = 1.0 / (alpha - beta);
     }
-    d[i] = A[(size_t)i * n + i];
+    d[i] = rowi[i];
     e[i] = beta;
     tau[i] = t;
     bc[0] = sc;
@@ -321,34 +323,39 @@ __global__ void __launch_bounds__(kColThreads) panel_column_kernel(double* A, in
     double v = 0.0;
     if (r == i + 1) v = apply ? 1.0 : 0.0;
     else if (r > i + 1) {
-      v = apply ? A[(size_t)r * n + i] * sc : 0.0;
-      A[(size_t)r * n + i] = v;
+      v = apply ? rowi[r] * sc : 0.0;
+      rowi[r] = v;
     }
     V[(size_t)r * kPanel + j] = v;
+    vcol[r] = v;
   }
 }
-// y = A22 v over rows/cols > i (A22 as of the panel start), one warp per row with v staged in
-// shared memory; also the block partials of s1 = W[:, :j]^T v and s2 = V[:, :j]^T v.
-__global__ void __launch_bounds__(kBlock) panel_symv_kernel(const double* A, int n, int i, int j, const double* V,
-                                                            const double* W, double* y, double* partial_s) {
-  extern __shared__ double vs[];  // n - i - 1 values
+// y = A22 v over rows/cols > i (A22 as of the panel start): one warp per row, four independent
+// loads in flight per lane, v read from the contiguous copy (L1/L2 resident). Also the block
+// partials of s1 = W[:, :j]^T v and s2 = V[:, :j]^T v.
+__global__ void __launch_bounds__(kBlock) panel_symv_kernel(const double* __restrict__ A, int n, int i, int j,
+                                                            const double* __restrict__ vcol,
+                                                            const double* __restrict__ V,
+                                                            const double* __restrict__ W, double* y,
+                                                            double* partial_s) {
   const int m = n - i - 1;
-  for (int c = threadIdx.x; c < m; c += kBlock) vs[c] = V[(size_t)(i + 1 + c) * kPanel + j];
-  __syncthreads();
+  const double* vv = vcol + i + 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double s1 = 0.0, s2 = 0.0;  // lane k < j accumulates component k
   for (int rr = blockIdx.x * (kBlock / 32) + warp; rr < m; rr += gridDim.x * (kBlock / 32)) {
     const double* row = A + (size_t)(i + 1 + rr) * n + i + 1;
-    double acc0 = 0.0, acc1 = 0.0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     int c = lane;
-    for (; c + 32 < m; c += 64) {
-      acc0 = fma(row[c], vs[c], acc0);
-      acc1 = fma(row[c + 32], vs[c + 32], acc1);
+    for (; c + 96 < m; c += 128) {
+      a0 = fma(row[c], vv[c], a0);
+      a1 = fma(row[c + 32], vv[c + 32], a1);
+      a2 = fma(row[c + 64], vv[c + 64], a2);
+      a3 = fma(row[c + 96], vv[c + 96], a3);
     }
-    if (c < m) acc0 = fma(row[c], vs[c], acc0);
-    const double yr = warp_sum(acc0 + acc1);
+    for (; c < m; c += 32) a0 = fma(row[c], vv[c], a0);
+    const double yr = warp_sum((a0 + a1) + (a2 + a3));
     if (lane == 0) y[rr] = yr;
-    const double vr = vs[rr];
+    const double vr = vv[rr];
     if (lane < j) {
       const size_t ix = (size_t)(i + 1 + rr) * kPanel + lane;
       s1 = fma(W[ix], vr, s1);
@@ -366,16 +373,25 @@ __global__ void __launch_bounds__(kBlock) panel_symv_kernel(const double* A, int
     partial_s[(size_t)blockIdx.x * 64 + threadIdx.x] = t;
   }
 }
-// s[0..63] = sum over blocks of the symv partials (s1 in 0..31, s2 in 32..63)
-__global__ void __launch_bounds__(64) panel_reduce_kernel(const double* partial_s, int nblocks, double* s) {
+// s[0..63] = sum over blocks of the symv partials (s1 in 0..31, s2 in 32..63): one block per
+// component, its threads striding over the partials.
+__global__ void __launch_bounds__(kBlock) panel_reduce_kernel(const double* partial_s, int nblocks, double* s) {
   double t = 0.0;
-  for (int b = 0; b < nblocks; ++b) t += partial_s[(size_t)b * 64 + threadIdx.x];
-  s[threadIdx.x] = t;
+  for (int b = threadIdx.x; b < nblocks; b += kBlock) t += partial_s[(size_t)b * 64 + blockIdx.x];
+  __shared__ double red[kBlock / 32];
+  t = warp_sum(t);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double u = 0.0;
+    for (int w = 0; w < kBlock / 32; ++w) u += red[w];
+    s[blockIdx.x] = u;
+  }
 }
 // w = tau (y - V s1 - W s2) over rows > i; block partials of w . v
 __global__ void __launch_bounds__(kBlock) panel_wfix_kernel(int n, int i, int j, const double* V, const double* W,
-                                                            const double* y, const double* s, const double* tau_i,
-                                                            double* wtmp, double* partial) {
+                                                            const double* vcol, const double* y, const double* s,
+                                                            const double* tau_i, double* wtmp, double* partial) {
   const int m = n - i - 1;
   const double t = *tau_i;
   double dp = 0.0;
@@ -385,25 +401,26 @@ __global__ void __launch_bounds__(kBlock) panel_wfix_kernel(int n, int i, int j,
     for (int k = 0; k < j; ++k) w -= V[r * kPanel + k] * s[k] + W[r * kPanel + k] * s[32 + k];
     w *= t;
     wtmp[rr] = w;
-    dp = fma(w, V[r * kPanel + j], dp);
+    dp = fma(w, vcol[r], dp);
   }
   block_partial(dp, partial);
 }
 // W[:, j] = w - (tau/2)(w . v) v over rows > i (zero above)
-__global__ void __launch_bounds__(kBlock) panel_wfinal_kernel(int n, int i, int j, const double* V, double* W,
+__global__ void __launch_bounds__(kBlock) panel_wfinal_kernel(int n, int i, int j, const double* vcol, double* W,
                                                               const double* wtmp, const double* partial, int np,
                                                               const double* tau_i) {
-  __shared__ double a2s;
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int b = 0; b < np; ++b) t += partial[b];
-    a2s = -0.5 * (*tau_i) * t;
-  }
+  __shared__ double red[kBlock / 32];
+  double t = 0.0;
+  for (int b = threadIdx.x; b < np; b += kBlock) t += partial[b];
+  t = warp_sum(t);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
   __syncthreads();
-  const double a2 = a2s;
+  double dotwv = 0.0;
+  for (int w = 0; w < kBlock / 32; ++w) dotwv += red[w];
+  const double a2 = -0.5 * (*tau_i) * dotwv;
   for (int r = blockIdx.x * kBlock + threadIdx.x; r < n; r += gridDim.x * kBlock) {
     double w = 0.0;
-    if (r > i) w = wtmp[r - i - 1] + a2 * V[(size_t)r * kPanel + j];
+    if (r > i) w = wtmp[r - i - 1] + a2 * vcol[r];
     W[(size_t)r * kPanel + j] = w;
   }
 }
@@ -417,13 +434,13 @@ __global__ void tail_kernel(const double* A, int n, double* d, double* e, double
   d[n - 1] = A[(size_t)(n - 1) * n + n - 1];
   e[n - 1] = 0.0;
 }
-// V of the panel [p, p+b) rebuilt from the stored reflectors (for the back-transformation)
+// V of the panel [p, p+b) rebuilt from the reflectors stored in rows p .. p+b-1
 __global__ void __launch_bounds__(kBlock) panel_v_kernel(const double* A, int n, int p, int b, double* V) {
   for (size_t q = blockIdx.x * (size_t)kBlock + threadIdx.x; q < (size_t)n * kPanel; q += (size_t)gridDim.x * kBlock) {
     const int r = (int)(q / kPanel), k = (int)(q % kPanel);
     const int i = p + k;
     double v = 0.0;
-    if (k < b) v = r <= i ? 0.0 : (r == i + 1 ? 1.0 : A[(size_t)r * n + i]);
+    if (k < b) v = r <= i ? 0.0 : (r == i + 1 ? 1.0 : A[(size_t)i * n + r]);
     V[q] = v;
   }
 }

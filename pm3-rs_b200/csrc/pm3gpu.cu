@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -100,6 +101,7 @@ struct pm3gpu_ctx {
   int large_min = kMaxN + 1;  // molecules with at least this many basis functions
   LargeBufs* lbuf = nullptr;
   DevBuf lsel;                // densities of the selected state (P_tot | P_alpha | P_beta)
+  double large_ms[16] = {};   // phase times of the last whole-GPU solve (profiling only)
 };
 
 namespace {
@@ -464,6 +466,7 @@ int launch_gradients(pm3gpu_ctx* c, const std::vector<GradMol>& mols, const std:
 int run_large(pm3gpu_ctx* c, const MolPlan& p, const int32_t* hz, const int32_t* dz, const double* dxyz,
               const pm3gpu_options* o, const Want& want, pm3gpu_result& Rm, double* charges, double* density,
               double* mo_energies, double* gradient) {
+  for (double& t : c->large_ms) t = 0.0;
   if (!c->blas) BLAS_TRY(c, cublasCreate(&c->blas));
   BLAS_TRY(c, cublasSetStream(c->blas, c->stream));
   if (!c->lbuf) c->lbuf = new LargeBufs();
@@ -1082,6 +1085,13 @@ int pm3gpu_last_timings(pm3gpu_ctx* c, double* ms, int max_entries) {
 }
 
 int pm3gpu_last_kernel_launches(pm3gpu_ctx* c) { return c ? c->launches : 0; }
+
+int pm3gpu_last_large_phase_ms(pm3gpu_ctx* c, double* ms, int max_entries) {
+  if (!c || !ms) return 0;
+  const int k = std::min(max_entries, (int)kLgPhases);
+  for (int i = 0; i < k; ++i) ms[i] = c->large_ms[i];
+  return c->profile ? k : 0;
+}
 
 int pm3gpu_set_large_threshold(pm3gpu_ctx* c, int nao) {
   if (!c) return PM3GPU_INVALID_INPUT;

@@ -68,7 +68,7 @@ EXPORTS = [
     "pm3gpu_set_stream", "pm3gpu_single_point", "pm3gpu_gradient", "pm3gpu_batch",
     "pm3gpu_batch_device_inputs", "pm3gpu_core_hamiltonian", "pm3gpu_fock", "pm3gpu_last_timings",
     "pm3gpu_last_kernel_launches", "pm3gpu_last_transfer_bytes", "pm3gpu_last_phase_cycles",
-    "pm3gpu_single_point_noalloc", "pm3gpu_set_large_threshold",
+    "pm3gpu_single_point_noalloc", "pm3gpu_set_large_threshold", "pm3gpu_last_large_phase_ms",
 ]
 
 _lib = None
@@ -112,6 +112,7 @@ def load() -> ctypes.CDLL:
     L.pm3gpu_last_timings.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     L.pm3gpu_last_kernel_launches.argtypes = [ctypes.c_void_p]
     L.pm3gpu_set_large_threshold.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.pm3gpu_last_large_phase_ms.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     L.pm3gpu_last_phase_cycles.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     L.pm3gpu_last_transfer_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
                                              ctypes.POINTER(ctypes.c_longlong)]
