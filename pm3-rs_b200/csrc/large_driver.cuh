@@ -14,19 +14,37 @@
 // rotation within the cluster, and the polar step fixes their orthogonality without leaving the
 // cluster's invariant subspace, which is all the density P = w C_occ C_occ^T depends on.
 
+constexpr size_t kBlasWorkspace = 64u << 20;  // cuBLAS workspace, set before graph capture
+
+struct TriGraph {
+  static constexpr int kKeys = 14;
+  cudaGraphExec_t exec = nullptr;
+  int n = 0, launches = 0;
+  const void* key[kKeys] = {};
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    n = 0;
+  }
+};
+
 struct LargeBufs {
+  TriGraph tg;
+  DevBuf blas_ws;
   DevBuf ao, sprow, sroff;
-  DevBuf H, W, hacc, dpk, jacc, part, scal;
+  DevBuf H, W, hacc, dpk, jacc, part, part2, scal;
   DevBuf P[2], Q[2], Pt, F, G, hist, A;
   DevBuf d, e, e2, tau, lam, dlam, blk;
   DevBuf V, Wp, y, wtmp, ps, s64, vcol;
   DevBuf X, Xt, Dp, Lp, Um;
   DevBuf Gm, Mm, Tm, Z1, Z2, blocks, Gk;
   void release() {
-    for (DevBuf* b : {&ao, &sprow, &sroff, &H, &W, &hacc, &dpk, &jacc, &part, &scal, &P[0], &P[1], &Q[0], &Q[1], &Pt,
+    for (DevBuf* b : {&ao, &sprow, &sroff, &H, &W, &hacc, &dpk, &jacc, &part, &part2, &scal, &P[0], &P[1], &Q[0], &Q[1], &Pt,
                       &F, &G, &hist, &A, &d, &e, &e2, &tau, &lam, &dlam, &blk, &V, &Wp, &y, &wtmp, &ps, &s64, &vcol, &X, &Xt,
                       &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk})
       b->release();
+    blas_ws.release();
+    tg.reset();
   }
 };
 
@@ -153,6 +171,7 @@ class LargeSolver {
     CUDA_TRY(c_, B_.dpk.ensure(80 * (size_t)N_));
     CUDA_TRY(c_, B_.jacc.ensure(80 * (size_t)N_));
     CUDA_TRY(c_, B_.part.ensure(8 * (size_t)large::kRedBlocks));
+    CUDA_TRY(c_, B_.part2.ensure(8 * (size_t)large::kRedBlocks));
     CUDA_TRY(c_, B_.scal.ensure(8 * 128));
     CUDA_TRY(c_, cudaMemsetAsync(B_.hacc.p, 0, 80 * (size_t)N_, c_->stream));
     const long long np = (long long)N_ * (N_ - 1) / 2;
@@ -533,6 +552,97 @@ class LargeSolver {
     return PM3GPU_OK;
   }
 
+  // The whole reduction is one fixed sequence of kernels and DGEMMs for a given matrix size and
+  // set of buffers, so it is captured once into a CUDA graph and replayed in later SCF
+  // iterations (it is ~5 launches per column). Streams that cannot be captured run it directly.
+  int run_tridiag(double* A) {
+    TriGraph& g = B_.tg;
+    const void* key[TriGraph::kKeys] = {A,        B_.V.p,  B_.Wp.p,    B_.vcol.p, B_.y.p,   B_.wtmp.p,
+                                        B_.ps.p,  B_.s64.p, B_.part.p, B_.part2.p, B_.d.p,   B_.e.p,
+                                        B_.tau.p, (const void*)c_->stream};
+    bool hit = g.exec != nullptr && g.n == n_;
+    for (int k = 0; hit && k < TriGraph::kKeys; ++k) hit = g.key[k] == key[k];
+    if (!hit) {
+      g.reset();
+      CUDA_TRY(c_, B_.blas_ws.ensure(kBlasWorkspace));
+      BLAS_TRY(c_, cublasSetWorkspace(blas(), B_.blas_ws.p, kBlasWorkspace));
+      if (cudaStreamBeginCapture(c_->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        (void)cudaGetLastError();
+        int launches = 0;
+        const int rc = enqueue_tridiag(A, launches);
+        c_->launches += launches;
+        return rc;
+      }
+      int launches = 0;
+      const int rc = enqueue_tridiag(A, launches);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(c_->stream, &graph);
+      if (rc != PM3GPU_OK || ec != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc != PM3GPU_OK ? rc : fail(c_, PM3GPU_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(ec));
+      }
+      const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ei != cudaSuccess) {
+        g.exec = nullptr;
+        return fail(c_, PM3GPU_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+      }
+      g.n = n_;
+      g.launches = launches;
+      for (int k = 0; k < TriGraph::kKeys; ++k) g.key[k] = key[k];
+    }
+    CUDA_TRY(c_, cudaGraphLaunch(g.exec, c_->stream));
+    c_->launches += g.launches;
+    return PM3GPU_OK;
+  }
+
+  // Enqueues the blocked reduction of A (no host synchronisation inside).
+  int enqueue_tridiag(double* A, int& launches) {
+    const int n = n_;
+    double* d = B_.d.as<double>();
+    double* e = B_.e.as<double>();
+    double* tau = B_.tau.as<double>();
+    double* V = B_.V.as<double>();
+    double* W = B_.Wp.as<double>();
+    double* vcol = B_.vcol.as<double>();
+    const double one = 1.0, mone = -1.0;
+    for (int p = 0; p < n - 2; p += large::kPanel) {
+      const int b = std::min(large::kPanel, n - 2 - p);
+      for (int j = 0; j < b; ++j) {
+        const int i = p + j;
+        const int m = n - i - 1;
+        const int gu = grid_for((size_t)(n - i), large::kBlock, large::kRedBlocks);
+        large::panel_update_kernel<<<gu, large::kBlock, 0, c_->stream>>>(A, n, i, j, V, W, B_.part2.as<double>());
+        const int gs = std::max(1, std::min(std::min((m + 7) / 8, 8 * c_->sms), large::kRedBlocks));
+        large::panel_symv_kernel<<<gs, large::kBlock, 0, c_->stream>>>(A, n, i, j, V, W, B_.part2.as<double>(), gu, d,
+                                                                       e, tau, B_.y.as<double>(), B_.ps.as<double>());
+        large::panel_reduce_kernel<<<64, large::kBlock, 0, c_->stream>>>(B_.ps.as<double>(), gs, B_.s64.as<double>());
+        const int gw = grid_for((size_t)m, large::kBlock, large::kRedBlocks);
+        large::panel_wfix_kernel<<<gw, large::kBlock, 0, c_->stream>>>(A, n, i, j, V, W, vcol, B_.y.as<double>(),
+                                                                        B_.s64.as<double>(), B_.part2.as<double>(), gu,
+                                                                        B_.wtmp.as<double>(), B_.part.as<double>());
+        large::panel_wfinal_kernel<<<grid_for((size_t)n, large::kBlock, large::kRedBlocks), large::kBlock, 0,
+                                     c_->stream>>>(n, i, j, vcol, V, W, B_.wtmp.as<double>(), B_.part.as<double>(), gw,
+                                                   tau + i);
+        launches += 5;
+      }
+      const int q = p + b, m = n - q;
+      if (m > 0) {  // A[q:, q:] -= V W^T + W V^T (row-major); column-major: C -= Wc^T Vc + Vc^T Wc
+        double* C = A + (size_t)q * n + q;
+        const double* Vq = V + (size_t)q * large::kPanel;
+        const double* Wq = W + (size_t)q * large::kPanel;
+        BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Wq, large::kPanel, Vq, large::kPanel,
+                                 &one, C, n));
+        BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Vq, large::kPanel, Wq, large::kPanel,
+                                 &one, C, n));
+      }
+    }
+    large::tail_kernel<<<1, 1, 0, c_->stream>>>(A, n, d, e, tau);
+    ++launches;
+    CUDA_TRY(c_, cudaGetLastError());
+    return PM3GPU_OK;
+  }
+
   // Lowest kval eigenvalues of the tridiagonal in B_.d / B_.e (host bookkeeping of splits).
   int eigenvalues(int kval, std::vector<double>& lam, std::vector<double>& dl, bool warm) {
     const int n = n_;
@@ -620,40 +730,11 @@ class LargeSolver {
     double* V = B_.V.as<double>();
     double* W = B_.Wp.as<double>();
     const double one = 1.0, mone = -1.0, zero = 0.0;
-    // ---- 1. Householder tridiagonalisation (sytrd/latrd, lower)
-    double* vcol = B_.vcol.as<double>();
-    for (int p = 0; p < n - 2; p += large::kPanel) {
-      const int b = std::min(large::kPanel, n - 2 - p);
-      for (int j = 0; j < b; ++j) {
-        const int i = p + j;
-        const int m = n - i - 1;
-        large::panel_column_kernel<<<1, large::kColThreads, 0, c_->stream>>>(A, n, i, j, V, W, vcol, d, e, tau);
-        const int gs = std::max(1, std::min(std::min((m + 7) / 8, 8 * c_->sms), large::kRedBlocks));
-        large::panel_symv_kernel<<<gs, large::kBlock, 0, c_->stream>>>(A, n, i, j, vcol, V, W, B_.y.as<double>(),
-                                                                       B_.ps.as<double>());
-        large::panel_reduce_kernel<<<64, large::kBlock, 0, c_->stream>>>(B_.ps.as<double>(), gs, B_.s64.as<double>());
-        const int gw = grid_for((size_t)m, large::kBlock, 4 * c_->sms);
-        large::panel_wfix_kernel<<<gw, large::kBlock, 0, c_->stream>>>(n, i, j, V, W, vcol, B_.y.as<double>(),
-                                                                        B_.s64.as<double>(), tau + i,
-                                                                        B_.wtmp.as<double>(), B_.part.as<double>());
-        large::panel_wfinal_kernel<<<grid_for((size_t)n, large::kBlock, 4 * c_->sms), large::kBlock, 0, c_->stream>>>(
-            n, i, j, vcol, W, B_.wtmp.as<double>(), B_.part.as<double>(), gw, tau + i);
-        c_->launches += 5;
-      }
-      const int q = p + b, m = n - q;
-      if (m > 0) {  // A[q:, q:] -= V W^T + W V^T (row-major); column-major: C -= Wc^T Vc + Vc^T Wc
-        double* C = A + (size_t)q * n + q;
-        const double* Vq = V + (size_t)q * large::kPanel;
-        const double* Wq = W + (size_t)q * large::kPanel;
-        BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Wq, large::kPanel, Vq, large::kPanel,
-                                 &one, C, n));
-        BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Vq, large::kPanel, Wq, large::kPanel,
-                                 &one, C, n));
-      }
+    // ---- 1. Householder tridiagonalisation (sytrd/latrd, lower), replayed from a CUDA graph
+    {
+      const int rc = run_tridiag(A);
+      if (rc) return rc;
     }
-    large::tail_kernel<<<1, 1, 0, c_->stream>>>(A, n, d, e, tau);
-    ++c_->launches;
-    CUDA_TRY(c_, cudaGetLastError());
     tick(kLgTridiag);
     // ---- 2. eigenvalues (host split bookkeeping, device multisection)
     {

@@ -277,89 +277,96 @@ __global__ void __launch_bounds__(kBlock) orth_defect_kernel(const double* G, in
 // the panel starting at p, V and W (n x kPanel, row-major) hold the panel's reflectors and the
 // vectors w_j such that the trailing matrix becomes A - V W^T - W V^T after the panel.
 //
-// Column i = p + j: bring it up to date with the panel's earlier columns, form the reflector
-// (norm over rows > i+1), and write d_i, e_i, tau_i. The trailing matrix is kept symmetric, so
-// column i below the diagonal is read from row i (contiguous). The reflector v (1 at i+1) goes
-// to V[:, j], to the contiguous vector vcol, and to row i right of the subdiagonal (A[i][r],
-// r >= i+2; row i is not read again), where the back-transformation finds it. One block.
-constexpr int kColThreads = 1024;
-__global__ void __launch_bounds__(kColThreads) panel_column_kernel(double* A, int n, int i, int j, double* V,
-                                                                   const double* W, double* vcol, double* d, double* e,
-                                                                   double* tau) {
-  __shared__ double red[kColThreads / 32];
-  __shared__ double bc[2];
+// Column i = p + j, step 1 (grid): bring row i (= column i below the diagonal: the trailing
+// matrix is kept symmetric) up to date with the panel's earlier columns,
+// a_r = A[i][r] - sum_{k<j} (V[r][k] W[i][k] + W[r][k] V[i][k]) for r >= i, in place, and the
+// block partials of the reflector norm sum_{r >= i+2} a_r^2.
+__global__ void __launch_bounds__(kBlock) panel_update_kernel(double* A, int n, int i, int j, const double* V,
+                                                              const double* W, double* partial) {
   double* rowi = A + (size_t)i * n;
+  const double* wi = W + (size_t)i * kPanel;
+  const double* vi = V + (size_t)i * kPanel;
   double part = 0.0;
-  for (int r = i + threadIdx.x; r < n; r += kColThreads) {
+  for (int r = i + blockIdx.x * kBlock + threadIdx.x; r < n; r += gridDim.x * kBlock) {
     double a = rowi[r];
-    for (int k = 0; k < j; ++k) a -= V[(size_t)r * kPanel + k] * W[(size_t)i * kPanel + k] +
-                                     W[(size_t)r * kPanel + k] * V[(size_t)i * kPanel + k];
+    const double* vr = V + (size_t)r * kPanel;
+    const double* wr = W + (size_t)r * kPanel;
+    for (int k = 0; k < j; ++k) a -= vr[k] * wi[k] + wr[k] * vi[k];
     rowi[r] = a;
     if (r >= i + 2) part = fma(a, a, part);
   }
-  part = warp_sum(part);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+  block_partial(part, partial);
+}
+// The reflector of column i from the norm partials (every block computes the same scalars):
+// returns scal (v_r = a_r scal below the subdiagonal) and tau; block 0 writes d_i, e_i, tau_i.
+__device__ __forceinline__ void panel_reflector(const double* rowi, int i, const double* partial, int np, double* d,
+                                                double* e, double* tau, double& scal, double& t) {
+  __shared__ double red[kBlock / 32];
+  __shared__ double bc[2];
+  double x = 0.0;
+  for (int b = threadIdx.x; b < np; b += kBlock) x += partial[b];
+  x = warp_sum(x);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
   __syncthreads();
   if (threadIdx.x == 0) {
     double xn2 = 0.0;
-    for (int w = 0; w < kColThreads / 32; ++w) xn2 += red[w];
+    for (int w = 0; w < kBlock / 32; ++w) xn2 += red[w];
     const double alpha = rowi[i + 1];
-    double beta = alpha, t = 0.0, sc = 0.0;
+    double beta = alpha, tt = 0.0, sc = 0.0;
     if (xn2 > 0.0) {
       beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
-      t = (beta - alpha) / beta;
+      tt = (beta - alpha) / beta;
       sc = 1.0 / (alpha - beta);
     }
-    d[i] = rowi[i];
-    e[i] = beta;
-    tau[i] = t;
+    if (blockIdx.x == 0) {
+      d[i] = rowi[i];
+      e[i] = beta;
+      tau[i] = tt;
+    }
     bc[0] = sc;
-    bc[1] = xn2 > 0.0 ? 1.0 : 0.0;
+    bc[1] = tt;
   }
   __syncthreads();
-  const double sc = bc[0];
-  const bool apply = bc[1] != 0.0;
-  for (int r = threadIdx.x; r < n; r += kColThreads) {
-    double v = 0.0;
-    if (r == i + 1) v = apply ? 1.0 : 0.0;
-    else if (r > i + 1) {
-      v = apply ? rowi[r] * sc : 0.0;
-      rowi[r] = v;
-    }
-    V[(size_t)r * kPanel + j] = v;
-    vcol[r] = v;
-  }
+  scal = bc[0];
+  t = bc[1];
 }
-// y = A22 v over rows/cols > i (A22 as of the panel start): one warp per row, four independent
-// loads in flight per lane, v read from the contiguous copy (L1/L2 resident). Also the block
-// partials of s1 = W[:, :j]^T v and s2 = V[:, :j]^T v.
+// Step 2 (grid): y = A22 v over rows/cols > i (A22 as of the panel start), one warp per row with
+// four independent loads in flight per lane; v_{i+1} = 1 and v_r = a_r scal are formed on the fly
+// from row i. Also the block partials of s1 = W[:, :j]^T v and s2 = V[:, :j]^T v.
 __global__ void __launch_bounds__(kBlock) panel_symv_kernel(const double* __restrict__ A, int n, int i, int j,
-                                                            const double* __restrict__ vcol,
                                                             const double* __restrict__ V,
-                                                            const double* __restrict__ W, double* y,
+                                                            const double* __restrict__ W, const double* norm_partial,
+                                                            int np, double* d, double* e, double* tau, double* y,
                                                             double* partial_s) {
+  const double* rowi = A + (size_t)i * n;
+  double scal, t;
+  panel_reflector(rowi, i, norm_partial, np, d, e, tau, scal, t);
   const int m = n - i - 1;
-  const double* vv = vcol + i + 1;
+  const double* aa = rowi + i + 1;  // a_{i+1} ...
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double s1 = 0.0, s2 = 0.0;  // lane k < j accumulates component k
-  for (int rr = blockIdx.x * (kBlock / 32) + warp; rr < m; rr += gridDim.x * (kBlock / 32)) {
-    const double* row = A + (size_t)(i + 1 + rr) * n + i + 1;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    int c = lane;
-    for (; c + 96 < m; c += 128) {
-      a0 = fma(row[c], vv[c], a0);
-      a1 = fma(row[c + 32], vv[c + 32], a1);
-      a2 = fma(row[c + 64], vv[c + 64], a2);
-      a3 = fma(row[c + 96], vv[c + 96], a3);
-    }
-    for (; c < m; c += 32) a0 = fma(row[c], vv[c], a0);
-    const double yr = warp_sum((a0 + a1) + (a2 + a3));
-    if (lane == 0) y[rr] = yr;
-    const double vr = vv[rr];
-    if (lane < j) {
-      const size_t ix = (size_t)(i + 1 + rr) * kPanel + lane;
-      s1 = fma(W[ix], vr, s1);
-      s2 = fma(V[ix], vr, s2);
+  if (t != 0.0) {
+    for (int rr = blockIdx.x * (kBlock / 32) + warp; rr < m; rr += gridDim.x * (kBlock / 32)) {
+      const double* row = A + (size_t)(i + 1 + rr) * n + i + 1;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      int c = lane;
+      for (; c + 96 < m; c += 128) {
+        a0 = fma(row[c], aa[c], a0);
+        a1 = fma(row[c + 32], aa[c + 32], a1);
+        a2 = fma(row[c + 64], aa[c + 64], a2);
+        a3 = fma(row[c + 96], aa[c + 96], a3);
+      }
+      for (; c < m; c += 32) a0 = fma(row[c], aa[c], a0);
+      double yr = warp_sum((a0 + a1) + (a2 + a3));
+      // A22 v with v_0 = 1, v_c = a_c scal (c >= 1): scal * (row . a) + row[0] (1 - scal a_0)
+      yr = scal * yr + row[0] * (1.0 - scal * aa[0]);
+      if (lane == 0) y[rr] = yr;
+      const double vr = rr == 0 ? 1.0 : aa[rr] * scal;
+      if (lane < j) {
+        const size_t ix = (size_t)(i + 1 + rr) * kPanel + lane;
+        s1 = fma(W[ix], vr, s1);
+        s2 = fma(V[ix], vr, s2);
+      }
     }
   }
   __shared__ double red[2][kBlock / 32][32];
@@ -368,12 +375,12 @@ __global__ void __launch_bounds__(kBlock) panel_symv_kernel(const double* __rest
   __syncthreads();
   if (threadIdx.x < 64) {
     const int which = threadIdx.x >> 5, k = threadIdx.x & 31;
-    double t = 0.0;
-    for (int w = 0; w < kBlock / 32; ++w) t += red[which][w][k];
-    partial_s[(size_t)blockIdx.x * 64 + threadIdx.x] = t;
+    double u = 0.0;
+    for (int w = 0; w < kBlock / 32; ++w) u += red[which][w][k];
+    partial_s[(size_t)blockIdx.x * 64 + threadIdx.x] = u;
   }
 }
-// s[0..63] = sum over blocks of the symv partials (s1 in 0..31, s2 in 32..63): one block per
+// Step 3: s[0..63] = sum over blocks of the symv partials (s1 in 0..31, s2 in 32..63): one block per
 // component, its threads striding over the partials.
 __global__ void __launch_bounds__(kBlock) panel_reduce_kernel(const double* partial_s, int nblocks, double* s) {
   double t = 0.0;
@@ -388,27 +395,51 @@ __global__ void __launch_bounds__(kBlock) panel_reduce_kernel(const double* part
     s[blockIdx.x] = u;
   }
 }
-// w = tau (y - V s1 - W s2) over rows > i; block partials of w . v
-__global__ void __launch_bounds__(kBlock) panel_wfix_kernel(int n, int i, int j, const double* V, const double* W,
-                                                            const double* vcol, const double* y, const double* s,
-                                                            const double* tau_i, double* wtmp, double* partial) {
+// Step 4 (grid): v into V[:, j], vcol and row i (the stored reflector, A[i][r] for r >= i+2);
+// w = tau (y - V s1 - W s2) over rows > i; block partials of w . v.
+__global__ void __launch_bounds__(kBlock) panel_wfix_kernel(double* A, int n, int i, int j, double* V, const double* W,
+                                                            double* vcol, const double* y, const double* s,
+                                                            const double* norm_partial, int np_norm, double* wtmp,
+                                                            double* partial) {
+  double* rowi = A + (size_t)i * n;
+  __shared__ double red[kBlock / 32];
+  double x = 0.0;
+  for (int b = threadIdx.x; b < np_norm; b += kBlock) x += norm_partial[b];
+  x = warp_sum(x);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+  __syncthreads();
+  double xn2 = 0.0;
+  for (int w = 0; w < kBlock / 32; ++w) xn2 += red[w];
+  const double alpha = rowi[i + 1];
+  double tt = 0.0, sc = 0.0;
+  if (xn2 > 0.0) {
+    const double beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+    tt = (beta - alpha) / beta;
+    sc = 1.0 / (alpha - beta);
+  }
   const int m = n - i - 1;
-  const double t = *tau_i;
   double dp = 0.0;
   for (int rr = blockIdx.x * kBlock + threadIdx.x; rr < m; rr += gridDim.x * kBlock) {
     const size_t r = (size_t)(i + 1 + rr);
-    double w = y[rr];
-    for (int k = 0; k < j; ++k) w -= V[r * kPanel + k] * s[k] + W[r * kPanel + k] * s[32 + k];
-    w *= t;
+    const double v = tt == 0.0 ? 0.0 : (rr == 0 ? 1.0 : rowi[r] * sc);
+    double w = 0.0;
+    if (tt != 0.0) {
+      w = y[rr];
+      for (int k = 0; k < j; ++k) w -= V[r * kPanel + k] * s[k] + W[r * kPanel + k] * s[32 + k];
+      w *= tt;
+    }
     wtmp[rr] = w;
-    dp = fma(w, vcol[r], dp);
+    dp = fma(w, v, dp);
+    V[r * kPanel + j] = v;
+    vcol[r] = v;
+    if (rr > 0) rowi[r] = v;
   }
   block_partial(dp, partial);
 }
-// W[:, j] = w - (tau/2)(w . v) v over rows > i (zero above)
-__global__ void __launch_bounds__(kBlock) panel_wfinal_kernel(int n, int i, int j, const double* vcol, double* W,
-                                                              const double* wtmp, const double* partial, int np,
-                                                              const double* tau_i) {
+// Step 5 (grid): W[:, j] = w - (tau/2)(w . v) v over rows > i (zero above, as V[:, j])
+__global__ void __launch_bounds__(kBlock) panel_wfinal_kernel(int n, int i, int j, const double* vcol, double* V,
+                                                              double* W, const double* wtmp, const double* partial,
+                                                              int np, const double* tau_i) {
   __shared__ double red[kBlock / 32];
   double t = 0.0;
   for (int b = threadIdx.x; b < np; b += kBlock) t += partial[b];
@@ -421,6 +452,7 @@ __global__ void __launch_bounds__(kBlock) panel_wfinal_kernel(int n, int i, int 
   for (int r = blockIdx.x * kBlock + threadIdx.x; r < n; r += gridDim.x * kBlock) {
     double w = 0.0;
     if (r > i) w = wtmp[r - i - 1] + a2 * vcol[r];
+    else V[(size_t)r * kPanel + j] = 0.0;
     W[(size_t)r * kPanel + j] = w;
   }
 }
