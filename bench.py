@@ -222,7 +222,7 @@ def water_cpu_baseline(nw, iters):
 
 def water_main(args, rank):
     """One 6000-atom water cluster (the large single-system workload): seconds per converged SCF."""
-    nw = 2000
+    nw = args.waters
     if args.impl == "reference":
         if rank != 0:
             return
@@ -331,7 +331,7 @@ def water_main(args, rank):
         "metric": METRIC, "value": value, "unit": "s/SCF", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": statistics.median(ms), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "water-2000: 2000 H2O (6000 atoms, 12000 basis functions), RHF PM3 FP64, "
+        "config": {"workload": f"water-{nw}: {nw} H2O ({3 * nw} atoms, {6 * nw} basis functions), RHF PM3 FP64, "
                                "reference default options", "iterations": iters, "heat_of_formation_kcal": hof,
                    "l2": "inputs and matrices (1.15 GB each) far exceed L2", "parallelism": "replicas only"},
         "e2e": {"value": e_ms[0] * 1e-3, "unit": "s/SCF", "h2d_bytes_per_step": hb.value, "d2h_bytes_per_step": db.value},
@@ -364,6 +364,8 @@ def main():
     ap.add_argument("--workload", default="organics-4096", choices=["organics-4096", "water-2000"],
                     help="organics-4096: the batched headline (default); water-2000: one 6000-atom water "
                          "cluster (12000 basis functions) on the whole-GPU path, seconds per SCF")
+    ap.add_argument("--waters", type=int, default=2000,
+                    help="water-2000 workload: number of waters (the cluster uses the first sites of a 13 x 13 x 12 grid)")
     ap.add_argument("--phases", action="store_true",
                     help="after the timed steps, run one more (untimed) batch with per-phase SM-cycle counters "
                          "and print the phase shares to stderr")

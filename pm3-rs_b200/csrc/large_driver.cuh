@@ -17,7 +17,7 @@
 constexpr size_t kBlasWorkspace = 64u << 20;  // cuBLAS workspace, set before graph capture
 
 struct TriGraph {
-  static constexpr int kKeys = 14;
+  static constexpr int kKeys = 17;
   cudaGraphExec_t exec = nullptr;
   int n = 0, launches = 0;
   const void* key[kKeys] = {};
@@ -35,12 +35,12 @@ struct LargeBufs {
   DevBuf H, W, hacc, dpk, jacc, part, part2, scal;
   DevBuf P[2], Q[2], Pt, F, G, hist, A;
   DevBuf d, e, e2, tau, lam, dlam, blk;
-  DevBuf V, Wp, y, wtmp, ps, s64, vcol;
+  DevBuf V, Wp, y, wtmp, ps, s64, vcol, tp, ctr, refl;
   DevBuf X, Xt, Dp, Lp, Um;
   DevBuf Gm, Mm, Tm, Z1, Z2, blocks, Gk;
   void release() {
     for (DevBuf* b : {&ao, &sprow, &sroff, &H, &W, &hacc, &dpk, &jacc, &part, &part2, &scal, &P[0], &P[1], &Q[0], &Q[1], &Pt,
-                      &F, &G, &hist, &A, &d, &e, &e2, &tau, &lam, &dlam, &blk, &V, &Wp, &y, &wtmp, &ps, &s64, &vcol, &X, &Xt,
+                      &F, &G, &hist, &A, &d, &e, &e2, &tau, &lam, &dlam, &blk, &V, &Wp, &y, &wtmp, &ps, &s64, &vcol, &tp, &ctr, &refl, &X, &Xt,
                       &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk})
       b->release();
     blas_ws.release();
@@ -559,7 +559,7 @@ class LargeSolver {
     TriGraph& g = B_.tg;
     const void* key[TriGraph::kKeys] = {A,        B_.V.p,  B_.Wp.p,    B_.vcol.p, B_.y.p,   B_.wtmp.p,
                                         B_.ps.p,  B_.s64.p, B_.part.p, B_.part2.p, B_.d.p,   B_.e.p,
-                                        B_.tau.p, (const void*)c_->stream};
+                                        B_.tau.p, B_.tp.p, B_.ctr.p, B_.refl.p, (const void*)c_->stream};
     bool hit = g.exec != nullptr && g.n == n_;
     for (int k = 0; hit && k < TriGraph::kKeys; ++k) hit = g.key[k] == key[k];
     if (!hit) {
@@ -612,19 +612,25 @@ class LargeSolver {
         const int i = p + j;
         const int m = n - i - 1;
         const int gu = grid_for((size_t)(n - i), large::kBlock, large::kRedBlocks);
-        large::panel_update_kernel<<<gu, large::kBlock, 0, c_->stream>>>(A, n, i, j, V, W, B_.part2.as<double>());
-        const int gs = std::max(1, std::min(std::min((m + 7) / 8, 8 * c_->sms), large::kRedBlocks));
-        large::panel_symv_kernel<<<gs, large::kBlock, 0, c_->stream>>>(A, n, i, j, V, W, B_.part2.as<double>(), gu, d,
-                                                                       e, tau, B_.y.as<double>(), B_.ps.as<double>());
-        large::panel_reduce_kernel<<<64, large::kBlock, 0, c_->stream>>>(B_.ps.as<double>(), gs, B_.s64.as<double>());
+        double* refl = B_.refl.as<double>();
+        unsigned int* ctr = B_.ctr.as<unsigned int>();
+        large::panel_update_kernel<<<gu, large::kBlock, 0, c_->stream>>>(A, n, i, j, V, W, B_.part2.as<double>(), ctr,
+                                                                         d, e, tau, refl);
+        const int nt = (m + large::kTile - 1) / large::kTile;
+        const long long ntiles = (long long)nt * (nt + 1) / 2;
+        large::symv_tiles_kernel<<<(unsigned)ntiles, large::kBlock, 0, c_->stream>>>(A, n, i, refl, B_.tp.as<double>());
+        const int gg = std::max(1, std::min((m + 31) / 32, large::kRedBlocks));
+        large::symv_gather_kernel<<<gg, large::kBlock, 0, c_->stream>>>(A, n, i, j, V, W, refl, B_.tp.as<double>(),
+                                                                        B_.y.as<double>(), B_.ps.as<double>(), ctr + 1,
+                                                                        B_.s64.as<double>());
         const int gw = grid_for((size_t)m, large::kBlock, large::kRedBlocks);
         large::panel_wfix_kernel<<<gw, large::kBlock, 0, c_->stream>>>(A, n, i, j, V, W, vcol, B_.y.as<double>(),
-                                                                        B_.s64.as<double>(), B_.part2.as<double>(), gu,
+                                                                        B_.s64.as<double>(), refl,
                                                                         B_.wtmp.as<double>(), B_.part.as<double>());
         large::panel_wfinal_kernel<<<grid_for((size_t)n, large::kBlock, large::kRedBlocks), large::kBlock, 0,
                                      c_->stream>>>(n, i, j, vcol, V, W, B_.wtmp.as<double>(), B_.part.as<double>(), gw,
                                                    tau + i);
-        launches += 5;
+        launches += 5;  // update, tiles, gather, wfix, wfinal
       }
       const int q = p + b, m = n - q;
       if (m > 0) {  // A[q:, q:] -= V W^T + W V^T (row-major); column-major: C -= Wc^T Vc + Vc^T Wc
@@ -724,6 +730,15 @@ class LargeSolver {
     CUDA_TRY(c_, B_.Wp.ensure(8 * (size_t)n * large::kPanel));
     CUDA_TRY(c_, B_.ps.ensure(8 * 64 * (size_t)large::kRedBlocks));
     CUDA_TRY(c_, B_.s64.ensure(8 * 64));
+    {
+      const long long nt = (n - 1 + large::kTile - 1) / large::kTile;
+      CUDA_TRY(c_, B_.tp.ensure(8 * (size_t)(2 * large::kTile) * (size_t)std::max<long long>(nt * (nt + 1) / 2, 1)));
+      if (!B_.ctr.p) {
+        CUDA_TRY(c_, B_.ctr.ensure(256));
+        CUDA_TRY(c_, cudaMemsetAsync(B_.ctr.p, 0, 256, c_->stream));
+      }
+      CUDA_TRY(c_, B_.refl.ensure(256));
+    }
     double* d = B_.d.as<double>();
     double* e = B_.e.as<double>();
     double* tau = B_.tau.as<double>();

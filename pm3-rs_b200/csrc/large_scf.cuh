@@ -282,141 +282,193 @@ __global__ void __launch_bounds__(kBlock) orth_defect_kernel(const double* G, in
 // a_r = A[i][r] - sum_{k<j} (V[r][k] W[i][k] + W[r][k] V[i][k]) for r >= i, in place, and the
 // block partials of the reflector norm sum_{r >= i+2} a_r^2.
 __global__ void __launch_bounds__(kBlock) panel_update_kernel(double* A, int n, int i, int j, const double* V,
-                                                              const double* W, double* partial) {
+                                                              const double* W, double* partial, unsigned int* counter,
+                                                              double* d, double* e, double* tau, double* refl) {
   double* rowi = A + (size_t)i * n;
   const double* wi = W + (size_t)i * kPanel;
   const double* vi = V + (size_t)i * kPanel;
   double part = 0.0;
   for (int r = i + blockIdx.x * kBlock + threadIdx.x; r < n; r += gridDim.x * kBlock) {
-    double a = rowi[r];
     const double* vr = V + (size_t)r * kPanel;
     const double* wr = W + (size_t)r * kPanel;
-    for (int k = 0; k < j; ++k) a -= vr[k] * wi[k] + wr[k] * vi[k];
+    double a0 = rowi[r], a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int k = 0;
+    for (; k + 3 < j; k += 4) {
+      a0 -= vr[k] * wi[k] + wr[k] * vi[k];
+      a1 -= vr[k + 1] * wi[k + 1] + wr[k + 1] * vi[k + 1];
+      a2 -= vr[k + 2] * wi[k + 2] + wr[k + 2] * vi[k + 2];
+      a3 -= vr[k + 3] * wi[k + 3] + wr[k + 3] * vi[k + 3];
+    }
+    for (; k < j; ++k) a0 -= vr[k] * wi[k] + wr[k] * vi[k];
+    const double a = (a0 + a1) + (a2 + a3);
     rowi[r] = a;
     if (r >= i + 2) part = fma(a, a, part);
   }
   block_partial(part, partial);
-}
-// The reflector of column i from the norm partials (every block computes the same scalars):
-// returns scal (v_r = a_r scal below the subdiagonal) and tau; block 0 writes d_i, e_i, tau_i.
-__device__ __forceinline__ void panel_reflector(const double* rowi, int i, const double* partial, int np, double* d,
-                                                double* e, double* tau, double& scal, double& t) {
+  // the last block to finish forms the reflector scalars (no block waits for another)
+  __threadfence();
+  __shared__ bool last;
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
   __shared__ double red[kBlock / 32];
-  __shared__ double bc[2];
   double x = 0.0;
-  for (int b = threadIdx.x; b < np; b += kBlock) x += partial[b];
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += kBlock) x += ((volatile double*)partial)[b];
   x = warp_sum(x);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
   __syncthreads();
   if (threadIdx.x == 0) {
     double xn2 = 0.0;
     for (int w = 0; w < kBlock / 32; ++w) xn2 += red[w];
-    const double alpha = rowi[i + 1];
+    const double alpha = ((volatile double*)rowi)[i + 1];
     double beta = alpha, tt = 0.0, sc = 0.0;
     if (xn2 > 0.0) {
       beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
       tt = (beta - alpha) / beta;
       sc = 1.0 / (alpha - beta);
     }
-    if (blockIdx.x == 0) {
-      d[i] = rowi[i];
-      e[i] = beta;
-      tau[i] = tt;
-    }
-    bc[0] = sc;
-    bc[1] = tt;
+    d[i] = ((volatile double*)rowi)[i];
+    e[i] = beta;
+    tau[i] = tt;
+    refl[0] = sc;
+    refl[1] = tt;
+    *counter = 0u;
   }
-  __syncthreads();
-  scal = bc[0];
-  t = bc[1];
 }
-// Step 2 (grid): y = A22 v over rows/cols > i (A22 as of the panel start), one warp per row with
-// four independent loads in flight per lane; v_{i+1} = 1 and v_r = a_r scal are formed on the fly
-// from row i. Also the block partials of s1 = W[:, :j]^T v and s2 = V[:, :j]^T v.
-__global__ void __launch_bounds__(kBlock) panel_symv_kernel(const double* __restrict__ A, int n, int i, int j,
-                                                            const double* __restrict__ V,
-                                                            const double* __restrict__ W, const double* norm_partial,
-                                                            int np, double* d, double* e, double* tau, double* y,
-                                                            double* partial_s) {
+// Symmetric GEMV over the lower triangle only (half the HBM traffic of a full GEMV): y = A22 v in
+// 64 x 64 tiles (I >= J) of A22 = A[i+1.., i+1..]. A tile contributes the row sums A_IJ v_J to
+// y_I and, off the diagonal, the column sums A_IJ^T v_I to y_J; both go to per-tile slots
+// (64 + 64 values) that symv_gather adds up in a fixed order.
+constexpr int kTile = 64;
+__global__ void __launch_bounds__(kBlock) symv_tiles_kernel(const double* __restrict__ A, int n, int i,
+                                                            const double* __restrict__ refl, double* tp) {
   const double* rowi = A + (size_t)i * n;
-  double scal, t;
-  panel_reflector(rowi, i, norm_partial, np, d, e, tau, scal, t);
+  const double scal = refl[0], t = refl[1];
   const int m = n - i - 1;
-  const double* aa = rowi + i + 1;  // a_{i+1} ...
+  const long long tidx = blockIdx.x;
+  int I = (int)((sqrt(8.0 * (double)tidx + 1.0) - 1.0) * 0.5);
+  while ((long long)(I + 1) * (I + 2) / 2 <= tidx) ++I;
+  while ((long long)I * (I + 1) / 2 > tidx) --I;
+  const int J = (int)(tidx - (long long)I * (I + 1) / 2);
+  const double* aa = rowi + i + 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double s1 = 0.0, s2 = 0.0;  // lane k < j accumulates component k
-  if (t != 0.0) {
-    for (int rr = blockIdx.x * (kBlock / 32) + warp; rr < m; rr += gridDim.x * (kBlock / 32)) {
-      const double* row = A + (size_t)(i + 1 + rr) * n + i + 1;
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      int c = lane;
-      for (; c + 96 < m; c += 128) {
-        a0 = fma(row[c], aa[c], a0);
-        a1 = fma(row[c + 32], aa[c + 32], a1);
-        a2 = fma(row[c + 64], aa[c + 64], a2);
-        a3 = fma(row[c + 96], aa[c + 96], a3);
-      }
-      for (; c < m; c += 32) a0 = fma(row[c], aa[c], a0);
-      double yr = warp_sum((a0 + a1) + (a2 + a3));
-      // A22 v with v_0 = 1, v_c = a_c scal (c >= 1): scal * (row . a) + row[0] (1 - scal a_0)
-      yr = scal * yr + row[0] * (1.0 - scal * aa[0]);
-      if (lane == 0) y[rr] = yr;
-      const double vr = rr == 0 ? 1.0 : aa[rr] * scal;
-      if (lane < j) {
-        const size_t ix = (size_t)(i + 1 + rr) * kPanel + lane;
-        s1 = fma(W[ix], vr, s1);
-        s2 = fma(V[ix], vr, s2);
+  const int c0 = J * kTile + lane, c1 = c0 + 32;
+  auto vval = [&](int c) { return c == 0 ? 1.0 : aa[c] * scal; };
+  const double vc0 = (t != 0.0 && c0 < m) ? vval(c0) : 0.0, vc1 = (t != 0.0 && c1 < m) ? vval(c1) : 0.0;
+  double rs[kTile / 8];
+  double col0 = 0.0, col1 = 0.0;
+#pragma unroll
+  for (int q = 0; q < kTile / 8; ++q) {
+    const int rl = warp + 8 * q, r = I * kTile + rl;
+    rs[q] = 0.0;
+    if (r < m && t != 0.0) {
+      const double* row = A + (size_t)(i + 1 + r) * n + i + 1;
+      const double a0 = c0 < m ? row[c0] : 0.0, a1 = c1 < m ? row[c1] : 0.0;
+      rs[q] = fma(a0, vc0, a1 * vc1);
+      if (I != J) {
+        const double vr = vval(r);
+        col0 = fma(a0, vr, col0);
+        col1 = fma(a1, vr, col1);
       }
     }
   }
-  __shared__ double red[2][kBlock / 32][32];
-  red[0][warp][lane] = s1;
-  red[1][warp][lane] = s2;
+  double* slot = tp + (size_t)tidx * (2 * kTile);
+#pragma unroll
+  for (int q = 0; q < kTile / 8; ++q) {
+    const double v = warp_sum(rs[q]);
+    if (lane == 0) slot[warp + 8 * q] = v;
+  }
+  __shared__ double cs[8][kTile];
+  cs[warp][lane] = col0;
+  cs[warp][lane + 32] = col1;
+  __syncthreads();
+  if (threadIdx.x < kTile) {
+    double u = 0.0;
+    for (int w = 0; w < 8; ++w) u += cs[w][threadIdx.x];
+    slot[kTile + threadIdx.x] = u;
+  }
+}
+// y_r = (row sums of stripe I over J <= I) + (column sums of the tiles below in column stripe I),
+// one thread per r; then s1 = W[:, :j]^T v and s2 = V[:, :j]^T v (one warp per row, lane k
+// accumulating component k) into block partials, which the last block to finish adds into s.
+__global__ void __launch_bounds__(kBlock) symv_gather_kernel(const double* __restrict__ A, int n, int i, int j,
+                                                             const double* __restrict__ V,
+                                                             const double* __restrict__ W,
+                                                             const double* __restrict__ refl, const double* tp,
+                                                             double* y, double* partial_s, unsigned int* counter,
+                                                             double* s) {
+  const double* rowi = A + (size_t)i * n;
+  const double scal = refl[0];
+  const double xn2 = refl[1] != 0.0 ? 1.0 : 0.0;  // a reflection exists
+  const int m = n - i - 1;
+  const int nt = (m + kTile - 1) / kTile;
+  const double* aa = rowi + i + 1;
+  {  // y over one 64-row stripe per block iteration: the 8 warps split its nt tile slots
+    __shared__ double ys[8][kTile];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int I = blockIdx.x; I < nt; I += gridDim.x) {
+      const long long base = (long long)I * (I + 1) / 2;
+      double y0 = 0.0, y1 = 0.0;
+      for (int J = warp; J < nt; J += 8) {
+        const size_t sl = J <= I ? (size_t)(base + J) * (2 * kTile) : (size_t)((long long)J * (J + 1) / 2 + I) * (2 * kTile) + kTile;
+        y0 += tp[sl + lane];
+        y1 += tp[sl + lane + 32];
+      }
+      ys[warp][lane] = y0;
+      ys[warp][lane + 32] = y1;
+      __syncthreads();
+      if (threadIdx.x < kTile) {
+        double u = 0.0;
+        for (int w = 0; w < 8; ++w) u += ys[w][threadIdx.x];
+        const int r = I * kTile + threadIdx.x;
+        if (r < m) y[r] = u;
+      }
+      __syncthreads();
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double s1 = 0.0, s2 = 0.0;
+  if (xn2 > 0.0 && lane < j)
+    for (int rr = blockIdx.x * (kBlock / 32) + warp; rr < m; rr += gridDim.x * (kBlock / 32)) {
+      const double vr = rr == 0 ? 1.0 : aa[rr] * scal;
+      const size_t ix = (size_t)(i + 1 + rr) * kPanel + lane;
+      s1 = fma(W[ix], vr, s1);
+      s2 = fma(V[ix], vr, s2);
+    }
+  __shared__ double rs2[2][kBlock / 32][32];
+  rs2[0][warp][lane] = s1;
+  rs2[1][warp][lane] = s2;
   __syncthreads();
   if (threadIdx.x < 64) {
     const int which = threadIdx.x >> 5, k = threadIdx.x & 31;
     double u = 0.0;
-    for (int w = 0; w < kBlock / 32; ++w) u += red[which][w][k];
+    for (int w = 0; w < kBlock / 32; ++w) u += rs2[which][w][k];
     partial_s[(size_t)blockIdx.x * 64 + threadIdx.x] = u;
   }
-}
-// Step 3: s[0..63] = sum over blocks of the symv partials (s1 in 0..31, s2 in 32..63): one block per
-// component, its threads striding over the partials.
-__global__ void __launch_bounds__(kBlock) panel_reduce_kernel(const double* partial_s, int nblocks, double* s) {
-  double t = 0.0;
-  for (int b = threadIdx.x; b < nblocks; b += kBlock) t += partial_s[(size_t)b * 64 + blockIdx.x];
-  __shared__ double red[kBlock / 32];
-  t = warp_sum(t);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  // the last block to finish adds the block partials (no block waits for another)
+  __threadfence();
+  __shared__ bool last;
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double u = 0.0;
-    for (int w = 0; w < kBlock / 32; ++w) u += red[w];
-    s[blockIdx.x] = u;
+  if (last) {
+    __threadfence();
+    if (threadIdx.x < 64) {
+      double u = 0.0;
+      for (unsigned b = 0; b < gridDim.x; ++b) u += ((volatile double*)partial_s)[(size_t)b * 64 + threadIdx.x];
+      s[threadIdx.x] = u;
+    }
+    if (threadIdx.x == 0) *counter = 0u;
   }
 }
 // Step 4 (grid): v into V[:, j], vcol and row i (the stored reflector, A[i][r] for r >= i+2);
 // w = tau (y - V s1 - W s2) over rows > i; block partials of w . v.
 __global__ void __launch_bounds__(kBlock) panel_wfix_kernel(double* A, int n, int i, int j, double* V, const double* W,
                                                             double* vcol, const double* y, const double* s,
-                                                            const double* norm_partial, int np_norm, double* wtmp,
+                                                            const double* __restrict__ refl, double* wtmp,
                                                             double* partial) {
   double* rowi = A + (size_t)i * n;
-  __shared__ double red[kBlock / 32];
-  double x = 0.0;
-  for (int b = threadIdx.x; b < np_norm; b += kBlock) x += norm_partial[b];
-  x = warp_sum(x);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
-  __syncthreads();
-  double xn2 = 0.0;
-  for (int w = 0; w < kBlock / 32; ++w) xn2 += red[w];
-  const double alpha = rowi[i + 1];
-  double tt = 0.0, sc = 0.0;
-  if (xn2 > 0.0) {
-    const double beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
-    tt = (beta - alpha) / beta;
-    sc = 1.0 / (alpha - beta);
-  }
+  const double sc = refl[0], tt = refl[1];
   const int m = n - i - 1;
   double dp = 0.0;
   for (int rr = blockIdx.x * kBlock + threadIdx.x; rr < m; rr += gridDim.x * kBlock) {
@@ -424,9 +476,18 @@ __global__ void __launch_bounds__(kBlock) panel_wfix_kernel(double* A, int n, in
     const double v = tt == 0.0 ? 0.0 : (rr == 0 ? 1.0 : rowi[r] * sc);
     double w = 0.0;
     if (tt != 0.0) {
-      w = y[rr];
-      for (int k = 0; k < j; ++k) w -= V[r * kPanel + k] * s[k] + W[r * kPanel + k] * s[32 + k];
-      w *= tt;
+      const double* vr = V + r * kPanel;
+      const double* wr = W + r * kPanel;
+      double w0 = y[rr], w1 = 0.0, w2 = 0.0, w3 = 0.0;
+      int k = 0;
+      for (; k + 3 < j; k += 4) {
+        w0 -= vr[k] * s[k] + wr[k] * s[32 + k];
+        w1 -= vr[k + 1] * s[k + 1] + wr[k + 1] * s[33 + k];
+        w2 -= vr[k + 2] * s[k + 2] + wr[k + 2] * s[34 + k];
+        w3 -= vr[k + 3] * s[k + 3] + wr[k + 3] * s[35 + k];
+      }
+      for (; k < j; ++k) w0 -= vr[k] * s[k] + wr[k] * s[32 + k];
+      w = tt * ((w0 + w1) + (w2 + w3));
     }
     wtmp[rr] = w;
     dp = fma(w, v, dp);
