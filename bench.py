@@ -315,9 +315,9 @@ def water_main(args, rank):
     k = pctx.lib.pm3gpu_last_large_phase_ms(pctx.ptr, ph, 16)
     phases = {LARGE_PHASES[i]: round(ph[i], 1) for i in range(min(k, len(LARGE_PHASES)))}
     n = 6 * nw
-    # dominant phase: the Householder reduction, HBM-bound on its panel GEMVs, which read the
-    # trailing matrix once per column: sum_i (n-i)^2 * 8 bytes = 8 n^3 / 3 per tridiagonalisation
-    tri_bytes = 8.0 * n ** 3 / 3.0
+    # dominant phase: the Householder reduction, HBM-bound on its panel GEMVs, which must read the
+    # lower triangle of the trailing matrix once per column: sum_i (n-i)^2 / 2 * 8 bytes = 4 n^3 / 3
+    tri_bytes = 4.0 * n ** 3 / 3.0
     tri_ms = phases.get("tridiagonalise", 0.0) / max(res[0].iterations, 1)
     peak = None
     try:
@@ -338,7 +338,7 @@ def water_main(args, rank):
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved and peak else None, "traffic": None,
-                     "kernel": "Householder reduction (panel_symv_kernel + panel kernels + DGEMM updates)",
+                     "kernel": "Householder reduction (symv_tiles_kernel + panel kernels + DGEMM trailing updates)",
                      "peak_source": peak_src, "bytes_per_tridiagonalisation": tri_bytes,
                      "ms_per_tridiagonalisation": tri_ms},
         "phases_ms": phases,
