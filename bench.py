@@ -53,7 +53,7 @@ def _oracle_worker(args):
     return n_conv
 
 
-def cpu_throughput(mols, cores, steps=1, warmup=0):
+def cpu_throughput(mols, cores, steps=1, warmup=0, opts=None):
     """Converged molecules/s of the oracle over `mols` on `cores` spawn workers (one thread each)."""
     import multiprocessing as mp
 
@@ -62,22 +62,36 @@ def cpu_throughput(mols, cores, steps=1, warmup=0):
     ctx = mp.get_context("spawn")
     chunks = [mols[i::cores] for i in range(cores)]
     with ctx.Pool(cores) as pool:
-        pool.map(_oracle_worker, [(c[:1], {}) for c in chunks])  # start-up outside the timing
+        o = opts or {}
+        pool.map(_oracle_worker, [(c[:1], o) for c in chunks])  # start-up outside the timing
         for _ in range(warmup):
-            pool.map(_oracle_worker, [(c, {}) for c in chunks])
+            pool.map(_oracle_worker, [(c, o) for c in chunks])
         rates = []
         for _ in range(max(steps, 1)):
             t0 = time.perf_counter()
-            n = sum(pool.map(_oracle_worker, [(c, {}) for c in chunks]))
+            n = sum(pool.map(_oracle_worker, [(c, o) for c in chunks]))
             rates.append((n, time.perf_counter() - t0))
     return rates
 
 
-def molecules(n_mol, seed):
+def molecules(n_mol, seed, workload="organics-4096"):
     from pm3_rs import workloads
 
-    mols = workloads.organic_batch(n_mol, 5, 60, seed=seed)
+    if workload == "radicals-2048":
+        mols = workloads.radical_batch(n_mol, 10, 80, seed=seed)
+    else:
+        mols = workloads.organic_batch(n_mol, 5, 60, seed=seed)
     return [(z, xyz * A2B) for z, xyz in mols]
+
+
+RADICALS = "radicals-2048: seeded C/H/N/O/S organics of 10-80 atoms minus one H (doublets), UHF PM3 FP64 + analytic gradients, reference default options"
+
+
+def workload_spec(args):
+    """(description, oracle options, GPU option overrides, gradients?, default batch size)."""
+    if args.workload == "radicals-2048":
+        return RADICALS, {"multiplicity": 2, "want_gradient": True}, {"multiplicity": 2}, True, 2048
+    return WORKLOAD, {}, {}, False, 4096
 
 
 # --------------------------------------------------------------------------- GPU helpers
@@ -175,9 +189,10 @@ DRAM_BYTES_PER_MOLECULE = 7.43e9 / 256
 
 
 def scf_flops(nao, n_occ, iters):
-    """Algorithmic FP64 flops of the dense SCF algebra per molecule: per iteration
+    """Algorithmic FP64 flops of the dense SCF algebra per molecule: per iteration and spin
     tridiagonalisation 4/3 n^3 + back-transformation 2 n^3 + commutator 2 n^3 + density
-    2 n^2 n_occ (the per-iteration formula of the hot-path measurement plan)."""
+    2 n^2 n_occ (the per-iteration formula of the hot-path measurement plan); `iters` counts
+    iterations times spins."""
     n = nao.astype(np.float64)
     return float(np.sum(iters * ((4.0 / 3.0) * n ** 3 + 2.0 * n ** 3 + 2.0 * n ** 3 + 2.0 * n * n * n_occ)))
 
@@ -358,12 +373,13 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pm3gpu", choices=["pm3gpu", "reference"])
-    ap.add_argument("--n-mol", type=int, default=4096)
+    ap.add_argument("--n-mol", type=int, default=None, help="molecules per step (default: 4096 organics, 2048 radicals)")
     ap.add_argument("--cpu-sample", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="organics-4096", choices=["organics-4096", "water-2000"],
-                    help="organics-4096: the batched headline (default); water-2000: one 6000-atom water "
-                         "cluster (12000 basis functions) on the whole-GPU path, seconds per SCF")
+    ap.add_argument("--workload", default="organics-4096", choices=["organics-4096", "radicals-2048", "water-2000"],
+                    help="organics-4096: the batched headline (default); radicals-2048: 2048 doublet radicals "
+                         "of 10-80 atoms, UHF + analytic gradients; water-2000: one 6000-atom water cluster "
+                         "(12000 basis functions) on the whole-GPU path, seconds per SCF")
     ap.add_argument("--waters", type=int, default=2000,
                     help="water-2000 workload: number of waters (the cluster uses the first sites of a 13 x 13 x 12 grid)")
     ap.add_argument("--phases", action="store_true",
@@ -379,11 +395,14 @@ def main():
 
     if args.workload == "water-2000":
         return water_main(args, rank)
+    desc, oracle_opts, gpu_opts, want_grad, default_n = workload_spec(args)
+    if args.n_mol is None:
+        args.n_mol = default_n
     if args.impl == "reference":
         if rank != 0:
             return
-        mols = molecules(args.n_mol, seed=1234)[: args.cpu_sample]
-        rates = cpu_throughput(mols, cores, steps=args.steps, warmup=0)
+        mols = molecules(args.n_mol, seed=1234, workload=args.workload)[: args.cpu_sample]
+        rates = cpu_throughput(mols, cores, steps=args.steps, warmup=0, opts=oracle_opts)
         n = sum(r[0] for r in rates)
         t = sum(r[1] for r in rates)
         value = n / t
@@ -391,7 +410,7 @@ def main():
             "impl": "reference", "metric": METRIC, "value": value, "unit": "SCF/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / len(rates),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "molecules_per_step": len(mols), "note": "CPU sample of the workload"},
+            "config": {"workload": desc, "molecules_per_step": len(mols), "note": "CPU sample of the workload"},
             "cpu_baseline": {"value": value, "unit": "SCF/s", "cores": cores, "kind": "port",
                              "sample": f"first {len(mols)} of the {args.n_mol} molecules per step, one process per core"},
             "e2e": {"value": value, "unit": "SCF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -415,7 +434,7 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
 
-    mols = molecules(args.n_mol, seed=1234 + 7919 * rank)
+    mols = molecules(args.n_mol, seed=1234 + 7919 * rank, workload=args.workload)
     from pm3_rs import workloads
 
     offs, z, xyz = workloads.pack(mols)
@@ -424,9 +443,11 @@ def main():
     lib = ctx.lib
     stream = torch.cuda.current_stream(dev)
     lib.pm3gpu_set_stream(ctx.ptr, ctypes.c_void_p(stream.cuda_stream))
-    opts = native.options()
+    opts = native.options(**gpu_opts)
     results = (_lib.Result * n_mol)()
     charges = np.zeros(n_atoms)
+    grads = np.zeros((n_atoms, 3)) if want_grad else None
+    pgr = torch.zeros(3 * n_atoms, dtype=torch.float64).pin_memory() if want_grad else None
     d_z = torch.from_numpy(z).to(dev)
     d_xyz = torch.from_numpy(np.ascontiguousarray(xyz)).to(dev)
     d_off = torch.from_numpy(offs).to(dev)
@@ -442,14 +463,15 @@ def main():
         rc = lib.pm3gpu_batch_device_inputs(ctx.ptr, n_mol, ctypes.c_void_p(d_off.data_ptr()),
                                             ctypes.c_void_p(d_z.data_ptr()), ctypes.c_void_p(d_xyz.data_ptr()),
                                             h_off.ctypes.data_as(I32), h_z.ctypes.data_as(I32), ctypes.byref(opts),
-                                            results, charges.ctypes.data_as(D), None)
+                                            results, charges.ctypes.data_as(D),
+                                            grads.ctypes.data_as(D) if want_grad else None)
         if rc != 0:
             raise RuntimeError(ctx.last_error())
 
     def run_host():
         rc = lib.pm3gpu_batch(ctx.ptr, n_mol, h_off.ctypes.data_as(I32), ctypes.cast(pz.data_ptr(), I32),
                               ctypes.cast(pxyz.data_ptr(), D), ctypes.byref(opts), 0, results,
-                              ctypes.cast(pq.data_ptr(), D), None)
+                              ctypes.cast(pq.data_ptr(), D), ctypes.cast(pgr.data_ptr(), D) if want_grad else None)
         if rc != 0:
             raise RuntimeError(ctx.last_error())
 
@@ -481,7 +503,8 @@ def main():
             nao = np.array([r.nao for r in results])
             nocc = np.array([r.n_occ for r in results])
             its = np.array([r.iterations for r in results])
-            flops += scf_flops(nao[st == 0], nocc[st == 0], its[st == 0])
+            spins = 1.0 + np.array([r.unrestricted for r in results], dtype=np.float64)
+            flops += scf_flops(nao[st == 0], nocc[st == 0], its[st == 0] * spins[st == 0])
         return ms, conv, launches, kern_ms, flops
 
     for _ in range(args.warmup):
@@ -519,7 +542,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "SCF/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "molecules_per_step_per_gpu": n_mol, "parallelism": f"dp{world}",
+        "config": {"workload": desc, "molecules_per_step_per_gpu": n_mol, "parallelism": f"dp{world}",
                    "l2": "flushed between steps (512 MiB write)", "converged_fraction": conv / (n_mol * args.steps * world)},
         "e2e": {"value": e2e, "unit": "SCF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
@@ -539,7 +562,7 @@ def main():
                           "cta_cycles": tot_c}), file=sys.stderr)
     if world == 1 and not args.no_cpu_baseline:
         sample = mols[: args.cpu_sample]
-        r = cpu_throughput(sample, os.cpu_count() or 1, steps=1)
+        r = cpu_throughput(sample, os.cpu_count() or 1, steps=1, opts=oracle_opts)
         line["cpu_baseline"] = {"value": r[0][0] / r[0][1], "unit": "SCF/s", "cores": os.cpu_count(),
                                 "kind": "port",
                                 "sample": f"first {len(sample)} of the {n_mol} molecules, one oracle process per core"}
