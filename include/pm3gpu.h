@@ -50,6 +50,7 @@ extern "C" {
 #define PM3GPU_GUESS_SAD 1
 #define PM3GPU_GUESS_CORE 2
 #define PM3GPU_GUESS_SYMMETRY_BROKEN 3
+#define PM3GPU_GUESS_LEARNED 4  /* no reference counterpart: see pm3gpu_guess_train */
 #define PM3GPU_STABILITY_OFF 0
 #define PM3GPU_STABILITY_AUTO 1
 #define PM3GPU_STABILITY_ALWAYS 2
@@ -206,6 +207,28 @@ int pm3gpu_last_kernel_launches(pm3gpu_ctx* ctx);
  * time, all SMs on it). Same run_pm3 semantics either way (no reference counterpart: the
  * reference has one CPU path). */
 int pm3gpu_set_large_threshold(pm3gpu_ctx* ctx, int nao);
+
+/* Learned initial density (no counterpart in the reference). A 3 x 256 BF16 MLP predicts every
+ * atom block and atom-pair block of the initial density from element one-hots, 32 Gaussian
+ * distance functions (6 A cutoff) and coordination counts; the SCF then starts from it (guess =
+ * PM3GPU_GUESS_LEARNED in the options). The plain SCF stays the judge: a molecule that does not
+ * converge from the learned start is solved again from the standard guess.
+ *
+ * pm3gpu_guess_train solves the given molecules with the plain SCF (their options), takes the
+ * converged densities as targets and trains the network on the GPU (Adam, minibatches of `batch`
+ * rows, `epochs` passes, learning rate `lr`, seeded shuffling and initialisation; continues from
+ * the context's current parameters when it has some). losses[epochs] receives the mean masked
+ * squared error of each epoch. Parameters: PM3GPU_GUESS_PARAMS floats (W1 b1 W2 b2 W3 b3 W4 b4). */
+#define PM3GPU_GUESS_PARAMS 150280
+int pm3gpu_guess_train(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
+                       const double* xyz_bohr, const pm3gpu_options* opts, int epochs, int batch, float lr,
+                       unsigned seed, float* losses);
+int pm3gpu_guess_set_params(pm3gpu_ctx* ctx, const float* params, int n_params);
+/* The network's feature rows (64 floats each, optional) and outputs (8 floats each) for a batch:
+ * per molecule its atoms, then its pairs a < b (the atom with more orbitals first in a pair). */
+int pm3gpu_guess_predict(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
+                         const double* xyz_bohr, float* features, float* outputs);
+int pm3gpu_guess_get_params(pm3gpu_ctx* ctx, float* params, int n_params);
 
 /* Wall-clock ms per phase of the last whole-GPU solve (core, Fock, DIIS, tridiagonalise,
  * eigenvalues, eigenvectors, back-transform, orthonormalise, density), when the context was

@@ -10,12 +10,14 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <random>
 #include <string>
 #include <vector>
 
 #include "../../include/pm3gpu.h"
 #include "gradient_kernel.cuh"
 #include "large_scf.cuh"
+#include "guess_mlp.cuh"
 #include "scf_job.cuh"
 
 using namespace pm3gpu;
@@ -102,6 +104,11 @@ struct pm3gpu_ctx {
   LargeBufs* lbuf = nullptr;
   DevBuf lsel;                // densities of the selected state (P_tot | P_alpha | P_beta)
   double large_ms[16] = {};   // phase times of the last whole-GPU solve (profiling only)
+  // learned initial density: FP32 master parameters, BF16 copy, Adam moments, gradients
+  bool has_guess_model = false;
+  long long adam_steps = 0;
+  DevBuf gp, gpb, gm, gv, gg;
+  DevBuf gqmols, gatom, gao, gcoord, gX, gY, gZ[3], gH[3], gdH, gdZ, gT, gM, gidx, gXb, gTb, gMb, gdY, gpart, gguess, gdens;
 };
 
 namespace {
@@ -205,7 +212,8 @@ JobDesc make_job(const MolPlan& m, int guess, int accel, double shift, double da
   j.n_beta = m.n_beta;
   const bool uhf = m.use_uhf || force_uhf;
   j.flags = (uhf ? kJobUhf : 0) | extra_flags;
-  j.guess = (guess == PM3GPU_GUESS_CORE) ? 2 : (guess == PM3GPU_GUESS_SYMMETRY_BROKEN ? 3 : 1);
+  j.guess = (guess == PM3GPU_GUESS_CORE) ? 2
+            : (guess == PM3GPU_GUESS_SYMMETRY_BROKEN ? 3 : (guess == PM3GPU_GUESS_LEARNED ? 4 : 1));
   const bool use_diis = o.use_diis && accel != PM3GPU_ACCEL_NONE;
   if (!uhf) {  // scf.rs:1201-1228
     int a = use_diis ? accel : PM3GPU_ACCEL_NONE;
@@ -218,6 +226,8 @@ JobDesc make_job(const MolPlan& m, int guess, int accel, double shift, double da
     j.accel = (use_diis && accel == PM3GPU_ACCEL_CDIIS) ? PM3GPU_ACCEL_CDIIS : PM3GPU_ACCEL_NONE;
     j.depth = diis_depth(m.nao, 4, o.scf_memory_mb);
   }
+  j.backup = -1;
+  j.guess_off = 0;
   j.max_scf = o.max_scf;
   j.e_tol = o.e_tol;
   j.p_tol = o.p_tol;
@@ -369,6 +379,7 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   a.rready = c->rq.as<int>() + std::max(nr, 1);
   a.charges = c->charges.as<double>();
   a.densities = c->dens.as<double>();
+  a.guess_dens = c->gguess.as<double>();
   a.grads = nullptr;
   a.eps = c->eps.as<double>();
   a.work = c->work.as<double>();
@@ -599,6 +610,124 @@ int run_large(pm3gpu_ctx* c, const MolPlan& p, const int32_t* hz, const int32_t*
   return PM3GPU_OK;
 }
 
+// ------------------------------------------------------------------ learned initial density
+// Feature rows of a set of molecules: per molecule its atoms (self rows) then its pairs a < b.
+struct GuessRows {
+  std::vector<guess::Mol> mols;
+  std::vector<int> atom_mol, ao;  // per atom of the packed batch: molecule, first AO
+  long long rows = 0;
+  size_t dens_total = 0;
+};
+
+void guess_rows(const pm3gpu_ctx* c, const std::vector<int>& atom0, const std::vector<int>& natom,
+                const int32_t* h_z_all, int total_atoms, GuessRows& G) {
+  G.mols.clear();
+  G.atom_mol.assign(total_atoms, 0);
+  G.ao.assign(total_atoms, 0);
+  G.rows = 0;
+  G.dens_total = 0;
+  for (size_t m = 0; m < atom0.size(); ++m) {
+    guess::Mol M{};
+    M.atom0 = atom0[m];
+    M.natom = natom[m];
+    int off = 0;
+    for (int a = 0; a < M.natom; ++a) {
+      G.atom_mol[M.atom0 + a] = (int)m;
+      G.ao[M.atom0 + a] = off;
+      off += c->h_elem[h_z_all[M.atom0 + a]].norb;
+    }
+    M.nao = off;
+    M.row0 = G.rows;
+    M.dens_off = (long long)G.dens_total;
+    G.rows += M.natom + (long long)M.natom * (M.natom - 1) / 2;
+    G.dens_total += (size_t)off * off;
+    G.mols.push_back(M);
+  }
+}
+
+inline int gblocks(long long work, int threads = 256) {
+  return (int)std::max<long long>(1, std::min<long long>((work + threads - 1) / threads, 4096));
+}
+
+// coordination counts and BF16 feature rows into c->gX
+int guess_features(pm3gpu_ctx* c, const GuessRows& G, const int32_t* dz, const double* dxyz, int total_atoms) {
+  CUDA_TRY(c, c->gqmols.ensure(sizeof(guess::Mol) * std::max<size_t>(G.mols.size(), 1)));
+  CUDA_TRY(c, c->gatom.ensure(4 * (size_t)std::max(total_atoms, 1)));
+  CUDA_TRY(c, c->gao.ensure(4 * (size_t)std::max(total_atoms, 1)));
+  CUDA_TRY(c, c->gcoord.ensure(4 * (size_t)std::max(total_atoms, 1)));
+  CUDA_TRY(c, c->gX.ensure(2 * (size_t)guess::kIn * std::max<long long>(G.rows, 1)));
+  CUDA_TRY(c, cudaMemcpyAsync(c->gqmols.p, G.mols.data(), sizeof(guess::Mol) * G.mols.size(), cudaMemcpyHostToDevice,
+                              c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->gatom.p, G.atom_mol.data(), 4 * (size_t)total_atoms, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->gao.p, G.ao.data(), 4 * (size_t)total_atoms, cudaMemcpyHostToDevice, c->stream));
+  guess::coord_kernel<<<gblocks(total_atoms), 256, 0, c->stream>>>(c->gqmols.as<guess::Mol>(), (int)G.mols.size(),
+                                                                 c->gatom.as<int>(), dxyz, total_atoms,
+                                                                 c->gcoord.as<float>());
+  guess::features_kernel<<<gblocks(G.rows), 256, 0, c->stream>>>(c->gqmols.as<guess::Mol>(), (int)G.mols.size(),
+                                                                c->elem.as<ElemDev>(), dz, dxyz, c->gcoord.as<float>(),
+                                                                G.rows, c->gX.as<__nv_bfloat16>());
+  c->launches += 2;
+  CUDA_TRY(c, cudaGetLastError());
+  return PM3GPU_OK;
+}
+
+template <bool TA, bool TB>
+void gemm_bf16(pm3gpu_ctx* c, int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb,
+               float* C, int ldc, bool acc = false) {
+  const dim3 grid((N + guess::kGT - 1) / guess::kGT, (M + guess::kGT - 1) / guess::kGT);
+  guess::gemm_bf16_kernel<TA, TB><<<grid, 128, 0, c->stream>>>(M, N, K, A, lda, B, ldb, C, ldc, acc ? 1 : 0);
+  ++c->launches;
+}
+
+// MLP forward over `rows` feature rows of X (BF16) into Y (rows x kOut, FP32). With `keep`, the
+// pre-activations Z and activations H of each hidden layer stay in c->gZ / c->gH (training).
+int mlp_forward(pm3gpu_ctx* c, const __nv_bfloat16* X, long long rows, float* Y) {
+  using namespace guess;
+  const __nv_bfloat16* P = c->gpb.as<__nv_bfloat16>();
+  for (int l = 0; l < 3; ++l) {
+    CUDA_TRY(c, c->gZ[l].ensure(4 * (size_t)kHid * std::max<long long>(rows, 1)));
+    CUDA_TRY(c, c->gH[l].ensure(2 * (size_t)kHid * std::max<long long>(rows, 1)));
+  }
+  const int woff[3] = {kW1, kW2, kW3}, boff[3] = {kB1, kB2, kB3};
+  const __nv_bfloat16* in = X;
+  int kin = kIn;
+  for (int l = 0; l < 3; ++l) {
+    gemm_bf16<false, false>(c, (int)rows, kHid, kin, in, kin, P + woff[l], kHid, c->gZ[l].as<float>(), kHid);
+    bias_act_kernel<<<gblocks(rows * kHid), 256, 0, c->stream>>>(c->gZ[l].as<float>(), c->gp.as<float>() + boff[l], kHid,
+                                                                 rows, c->gH[l].as<__nv_bfloat16>(), 1);
+    ++c->launches;
+    in = c->gH[l].as<__nv_bfloat16>();
+    kin = kHid;
+  }
+  gemm_bf16<false, false>(c, (int)rows, kOut, kHid, in, kHid, P + kW4, kOut, Y, kOut);
+  bias_act_kernel<<<gblocks(rows * kOut), 256, 0, c->stream>>>(Y, c->gp.as<float>() + kB4, kOut, rows, nullptr, 0);
+  ++c->launches;
+  CUDA_TRY(c, cudaGetLastError());
+  return PM3GPU_OK;
+}
+
+// Initial densities of the molecules in G (device buffer c->gguess, G.dens_total doubles).
+int guess_infer(pm3gpu_ctx* c, const GuessRows& G, const int32_t* dz, const double* dxyz, int total_atoms) {
+  if (!c->has_guess_model) return fail(c, PM3GPU_INVALID_INPUT, "learned guess requested but no model is set");
+  int rc = guess_features(c, G, dz, dxyz, total_atoms);
+  if (rc != PM3GPU_OK) return rc;
+  CUDA_TRY(c, c->gY.ensure(4 * (size_t)guess::kOut * std::max<long long>(G.rows, 1)));
+  CUDA_TRY(c, c->gguess.ensure(8 * std::max<size_t>(G.dens_total, 1)));
+  const long long chunk = 1 << 20;
+  for (long long r0 = 0; r0 < G.rows; r0 += chunk) {
+    const long long nr = std::min(chunk, G.rows - r0);
+    rc = mlp_forward(c, c->gX.as<__nv_bfloat16>() + r0 * guess::kIn, nr, c->gY.as<float>() + r0 * guess::kOut);
+    if (rc != PM3GPU_OK) return rc;
+  }
+  CUDA_TRY(c, cudaMemsetAsync(c->gguess.p, 0, 8 * G.dens_total, c->stream));
+  guess::assemble_kernel<<<gblocks(G.rows), 256, 0, c->stream>>>(c->gqmols.as<guess::Mol>(), (int)G.mols.size(),
+                                                                c->elem.as<ElemDev>(), dz, dxyz, c->gao.as<int>(),
+                                                                c->gY.as<float>(), G.rows, c->gguess.as<double>());
+  ++c->launches;
+  CUDA_TRY(c, cudaGetLastError());
+  return PM3GPU_OK;
+}
+
 struct HostJobResult {
   JobOut o;
   const JobDesc* job = nullptr;
@@ -610,7 +739,8 @@ struct HostJobResult {
 // each molecule's state exactly as run_pm3 does and forms the epilogue.
 int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_z, const double* h_xyz,
               const int32_t* d_z, const double* d_xyz, const pm3gpu_options* opts, int per_mol, const Want& want,
-              pm3gpu_result* results, double* charges, double* gradients, double* density, double* mo_energies) {
+              pm3gpu_result* results, double* charges, double* gradients, double* density, double* mo_energies,
+              double* all_dens = nullptr, const size_t* all_dens_off = nullptr) {
   c->launches = 0;
   c->timings[5] = 0.0;
   c->h2d = c->d2h = 0;
@@ -674,8 +804,38 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
         ++j.nrung;
       }
     }
+    if (j.guess == 4) {  // the same pass from the standard guess, run only if the learned start fails
+      JobDesc bj = p.steered ? make_job(p, PM3GPU_GUESS_SAD, o->accelerator, o->level_shift_ev, o->damping, false, 0)
+                             : make_job(p, PM3GPU_GUESS_SAD, o->accelerator, 0.0, 0.0, false, 0);
+      bj.mol = m;
+      bj.stab = j.stab;
+      bj.rung0 = j.rung0;
+      bj.nrung = j.nrung;
+      assign_offsets(bj, want, tot);
+      j.backup = (int)rjobs.size();
+      rjobs.push_back(bj);
+    }
     p.first_job = (int)jobs.size();
     jobs.push_back(j);
+  }
+  // learned initial densities for the molecules that asked for them
+  {
+    std::vector<int> la0, lna, lmol;
+    for (int m = 0; m < n_mol; ++m) {
+      const MolPlan& p = plans[m];
+      if (p.status == PM3GPU_OK && !p.large && jobs[p.first_job].guess == 4) {
+        la0.push_back(p.atom0);
+        lna.push_back(p.natom);
+        lmol.push_back(m);
+      }
+    }
+    if (!lmol.empty()) {
+      GuessRows G;
+      guess_rows(c, la0, lna, h_z, total_atoms, G);
+      const int rg = guess_infer(c, G, dz, dxyz, total_atoms);
+      if (rg != PM3GPU_OK) return rg;
+      for (size_t k = 0; k < lmol.size(); ++k) jobs[plans[lmol[k]].first_job].guess_off = G.mols[k].dens_off;
+    }
   }
   // largest first (longest-processing-time order) for the work queue
   std::vector<int> order(jobs.size()), pos(jobs.size());
@@ -719,6 +879,11 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
     st.o = R.out[pos[p.first_job]];
     st.job = &fj;
     st.unrestricted = (fj.flags & kJobUhf) != 0;
+    if (fj.backup >= 0 && !st.o.converged && R.rout[fj.backup].status != -1) {  // learned start failed
+      st.o = R.rout[fj.backup];
+      st.job = &rjobs[fj.backup];
+      st.unrestricted = (st.job->flags & kJobUhf) != 0;
+    }
     const double first_ev = st.o.electronic;
     int paths = 1;
     const bool searched = fj.nrung > 0 && R.rout[fj.rung0].status != -1;
@@ -774,6 +939,8 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
     }
     if (charges) std::memcpy(charges + p.atom0, R.charges.data() + st.job->charge_off, 8 * (size_t)p.natom);
     if (density && want.density) std::memcpy(density, R.dens.data() + st.job->dens_off, 8 * (size_t)p.nao * p.nao);
+    if (all_dens && want.density && st.o.converged)
+      std::memcpy(all_dens + all_dens_off[m], R.dens.data() + st.job->dens_off, 8 * (size_t)p.nao * p.nao);
     if (mo_energies && want.eps) std::memcpy(mo_energies, R.eps.data() + st.job->eps_off, 8 * (size_t)p.nao);
   }
   // ---------------------------------------------------------------- analytic gradients
@@ -917,6 +1084,10 @@ void pm3gpu_context_destroy(pm3gpu_ctx* c) {
     delete c->lbuf;
   }
   c->lsel.release();
+  for (DevBuf* b : {&c->gp, &c->gpb, &c->gm, &c->gv, &c->gg, &c->gqmols, &c->gatom, &c->gao, &c->gcoord, &c->gX, &c->gY,
+                    &c->gZ[0], &c->gZ[1], &c->gZ[2], &c->gH[0], &c->gH[1], &c->gH[2], &c->gdH, &c->gdZ, &c->gT, &c->gM,
+                    &c->gidx, &c->gXb, &c->gTb, &c->gMb, &c->gdY, &c->gpart, &c->gguess, &c->gdens})
+    b->release();
   if (c->blas) cublasDestroy(c->blas);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
@@ -1093,6 +1264,229 @@ int pm3gpu_last_large_phase_ms(pm3gpu_ctx* c, double* ms, int max_entries) {
   return c->profile ? k : 0;
 }
 
+int pm3gpu_guess_set_params(pm3gpu_ctx* c, const float* params, int n_params) {
+  if (!c || !params || n_params != guess::kParams) return fail(c, PM3GPU_INVALID_INPUT, "expected PM3GPU_GUESS_PARAMS floats");
+  std::lock_guard<std::mutex> lk(c->mu);
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  const size_t np = guess::kParams;
+  CUDA_TRY(c, c->gp.ensure(4 * np));
+  CUDA_TRY(c, c->gpb.ensure(2 * np));
+  CUDA_TRY(c, c->gm.ensure(4 * np));
+  CUDA_TRY(c, c->gv.ensure(4 * np));
+  CUDA_TRY(c, cudaMemcpyAsync(c->gp.p, params, 4 * np, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->gm.p, 0, 4 * np, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->gv.p, 0, 4 * np, c->stream));
+  guess::to_bf16_kernel<<<gblocks(np), 256, 0, c->stream>>>(c->gp.as<float>(), (int)np, c->gpb.as<__nv_bfloat16>());
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->adam_steps = 0;
+  c->has_guess_model = true;
+  return PM3GPU_OK;
+}
+
+int pm3gpu_guess_get_params(pm3gpu_ctx* c, float* params, int n_params) {
+  if (!c || !params || n_params != guess::kParams) return fail(c, PM3GPU_INVALID_INPUT, "expected PM3GPU_GUESS_PARAMS floats");
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (!c->has_guess_model) return fail(c, PM3GPU_INVALID_INPUT, "no learned guess model");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  CUDA_TRY(c, cudaMemcpyAsync(params, c->gp.p, 4 * (size_t)guess::kParams, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return PM3GPU_OK;
+}
+
+int pm3gpu_guess_predict(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t* z, const double* xyz,
+                         float* features, float* outputs) {
+  using namespace guess;
+  if (!c || n_mol < 1 || !offs || !z || !xyz) return fail(c, PM3GPU_INVALID_INPUT, "bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  if (!c->has_guess_model) return fail(c, PM3GPU_INVALID_INPUT, "no learned guess model");
+  const int total_atoms = offs[n_mol];
+  for (int a = 0; a < total_atoms; ++a)
+    if (!supported(z[a])) return fail(c, PM3GPU_UNSUPPORTED, "unsupported element");
+  std::vector<int> a0(n_mol), na(n_mol);
+  for (int m = 0; m < n_mol; ++m) {
+    a0[m] = offs[m];
+    na[m] = offs[m + 1] - offs[m];
+  }
+  GuessRows G;
+  guess_rows(c, a0, na, z, total_atoms, G);
+  CUDA_TRY(c, c->z.ensure(4 * (size_t)total_atoms));
+  CUDA_TRY(c, c->xyz.ensure(24 * (size_t)total_atoms));
+  CUDA_TRY(c, cudaMemcpyAsync(c->z.p, z, 4 * (size_t)total_atoms, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->xyz.p, xyz, 24 * (size_t)total_atoms, cudaMemcpyHostToDevice, c->stream));
+  int rc = guess_features(c, G, c->z.as<int32_t>(), c->xyz.as<double>(), total_atoms);
+  if (rc != PM3GPU_OK) return rc;
+  CUDA_TRY(c, c->gY.ensure(4 * (size_t)kOut * std::max<long long>(G.rows, 1)));
+  rc = mlp_forward(c, c->gX.as<__nv_bfloat16>(), G.rows, c->gY.as<float>());
+  if (rc != PM3GPU_OK) return rc;
+  if (outputs)
+    CUDA_TRY(c, cudaMemcpyAsync(outputs, c->gY.p, 4 * (size_t)kOut * G.rows, cudaMemcpyDeviceToHost, c->stream));
+  std::vector<__nv_bfloat16> xb;
+  if (features) {
+    xb.resize((size_t)kIn * G.rows);
+    CUDA_TRY(c, cudaMemcpyAsync(xb.data(), c->gX.p, 2 * xb.size(), cudaMemcpyDeviceToHost, c->stream));
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  for (size_t k = 0; k < xb.size(); ++k) features[k] = __bfloat162float(xb[k]);
+  return PM3GPU_OK;
+}
+
+int pm3gpu_guess_train(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t* z, const double* xyz,
+                       const pm3gpu_options* opts, int epochs, int batch, float lr, unsigned seed, float* losses) {
+  using namespace guess;
+  if (!c || n_mol < 1 || !offs || !z || !xyz || epochs < 0 || batch < 64) return fail(c, PM3GPU_INVALID_INPUT, "bad argument");
+  std::unique_lock<std::mutex> lk(c->mu);
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  c->err.clear();
+  pm3gpu_options o;
+  if (opts) o = *opts;
+  else pm3gpu_default_options(&o);
+  if (o.guess == PM3GPU_GUESS_LEARNED) o.guess = PM3GPU_GUESS_AUTO;  // targets come from the plain SCF
+  const int total_atoms = offs[n_mol];
+  // 1. plain SCF of every molecule, converged densities kept
+  std::vector<size_t> doff(n_mol);
+  size_t dtot = 0;
+  std::vector<int> nao(n_mol);
+  for (int m = 0; m < n_mol; ++m) {
+    int k = 0;
+    for (int a = offs[m]; a < offs[m + 1]; ++a) k += supported(z[a]) ? c->h_elem[z[a]].norb : 0;
+    nao[m] = k;
+    doff[m] = dtot;
+    dtot += (size_t)k * k;
+  }
+  std::vector<double> dens(std::max<size_t>(dtot, 1), 0.0);
+  std::vector<pm3gpu_result> res(n_mol);
+  std::vector<double> q(std::max(total_atoms, 1));
+  Want w;
+  w.density = true;
+  int rc = run_batch(c, n_mol, offs, z, xyz, nullptr, nullptr, &o, 0, w, res.data(), q.data(), nullptr, nullptr, nullptr,
+                     dens.data(), doff.data());
+  if (rc != PM3GPU_OK) return rc;
+  // 2. training rows: the converged molecules below one CTA's size
+  std::vector<int> a0, na, keep;
+  for (int m = 0; m < n_mol; ++m)
+    if (res[m].status == PM3GPU_OK && res[m].converged && nao[m] <= kMaxN) {
+      a0.push_back(offs[m]);
+      na.push_back(offs[m + 1] - offs[m]);
+      keep.push_back(m);
+    }
+  if (keep.empty()) return fail(c, PM3GPU_INVALID_INPUT, "no converged training molecule");
+  GuessRows G;
+  guess_rows(c, a0, na, z, total_atoms, G);
+  std::vector<double> packed(std::max<size_t>(G.dens_total, 1));
+  for (size_t k = 0; k < keep.size(); ++k)
+    std::memcpy(packed.data() + G.mols[k].dens_off, dens.data() + doff[keep[k]], 8 * (size_t)G.mols[k].nao * G.mols[k].nao);
+  CUDA_TRY(c, c->z.ensure(4 * (size_t)total_atoms));
+  CUDA_TRY(c, c->xyz.ensure(24 * (size_t)total_atoms));
+  CUDA_TRY(c, cudaMemcpyAsync(c->z.p, z, 4 * (size_t)total_atoms, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->xyz.p, xyz, 24 * (size_t)total_atoms, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, c->gdens.ensure(8 * packed.size()));
+  CUDA_TRY(c, cudaMemcpyAsync(c->gdens.p, packed.data(), 8 * packed.size(), cudaMemcpyHostToDevice, c->stream));
+  rc = guess_features(c, G, c->z.as<int32_t>(), c->xyz.as<double>(), total_atoms);
+  if (rc != PM3GPU_OK) return rc;
+  const long long rows = G.rows;
+  CUDA_TRY(c, c->gT.ensure(4 * (size_t)kOut * rows));
+  CUDA_TRY(c, c->gM.ensure(4 * (size_t)kOut * rows));
+  targets_kernel<<<gblocks(rows), 256, 0, c->stream>>>(c->gqmols.as<Mol>(), (int)G.mols.size(), c->elem.as<ElemDev>(),
+                                                        c->z.as<int32_t>(), c->xyz.as<double>(), c->gao.as<int>(),
+                                                        c->gdens.as<double>(), rows, c->gT.as<float>(), c->gM.as<float>());
+  CUDA_TRY(c, cudaGetLastError());
+  // masked entries per row on average (normalises the loss gradient)
+  double mask_total = 0.0;
+  for (size_t k = 0; k < keep.size(); ++k) {
+    long long h = 0, l = 0;
+    for (int a = 0; a < G.mols[k].natom; ++a) (c->h_elem[z[G.mols[k].atom0 + a]].norb == 4 ? h : l) += 1;
+    mask_total += 3.0 * h + l + 5.0 * h * (h - 1) / 2 + 2.0 * h * l + 1.0 * l * (l - 1) / 2;
+  }
+  const double mask_per_row = mask_total / (double)rows;
+  // 3. parameters (Xavier-uniform, seeded) unless the context already has a model
+  const size_t np = kParams;
+  if (!c->has_guess_model) {
+    std::vector<float> init(np, 0.0f);
+    std::mt19937 gen(seed);
+    auto fill = [&](int off, int fin, int fout) {
+      const float lim = std::sqrt(6.0f / (float)(fin + fout));
+      std::uniform_real_distribution<float> U(-lim, lim);
+      for (int k = 0; k < fin * fout; ++k) init[off + k] = U(gen);
+    };
+    fill(kW1, kIn, kHid);
+    fill(kW2, kHid, kHid);
+    fill(kW3, kHid, kHid);
+    fill(kW4, kHid, kOut);
+    lk.unlock();
+    rc = pm3gpu_guess_set_params(c, init.data(), (int)np);
+    lk.lock();
+    if (rc != PM3GPU_OK) return rc;
+  }
+  CUDA_TRY(c, c->gg.ensure(4 * np));
+  const int B = batch;
+  CUDA_TRY(c, c->gidx.ensure(8 * (size_t)rows));
+  CUDA_TRY(c, c->gXb.ensure(2 * (size_t)kIn * B));
+  CUDA_TRY(c, c->gTb.ensure(4 * (size_t)kOut * B));
+  CUDA_TRY(c, c->gMb.ensure(4 * (size_t)kOut * B));
+  CUDA_TRY(c, c->gY.ensure(4 * (size_t)kOut * B));
+  CUDA_TRY(c, c->gdY.ensure(2 * (size_t)kOut * B));
+  CUDA_TRY(c, c->gdH.ensure(4 * (size_t)kHid * B));
+  CUDA_TRY(c, c->gdZ.ensure(2 * (size_t)kHid * B));
+  CUDA_TRY(c, c->gpart.ensure(4 * 1024));
+  CUDA_TRY(c, cudaMemsetAsync(c->gpart.p, 0, 4 * 1024, c->stream));
+  std::vector<long long> idx(rows);
+  for (long long r = 0; r < rows; ++r) idx[r] = r;
+  std::mt19937_64 shuf(seed ^ 0x9e3779b97f4a7c15ull);
+  float* gp = c->gp.as<float>();
+  float* gg = c->gg.as<float>();
+  const __nv_bfloat16* Pb = c->gpb.as<__nv_bfloat16>();
+  const int woff[3] = {kW1, kW2, kW3}, boff[3] = {kB1, kB2, kB3};
+  const int nbatch = (int)(rows / B);
+  for (int ep = 0; ep < epochs; ++ep) {
+    std::shuffle(idx.begin(), idx.end(), shuf);
+    CUDA_TRY(c, cudaMemcpyAsync(c->gidx.p, idx.data(), 8 * (size_t)rows, cudaMemcpyHostToDevice, c->stream));
+    float* accum = c->gpart.as<float>() + (ep % 1024);
+    for (int bi = 0; bi < nbatch; ++bi) {
+      gather_rows_kernel<<<gblocks((long long)B * kIn), 256, 0, c->stream>>>(
+          c->gidx.as<long long>() + (size_t)bi * B, B, c->gX.as<__nv_bfloat16>(), c->gT.as<float>(), c->gM.as<float>(),
+          c->gXb.as<__nv_bfloat16>(), c->gTb.as<float>(), c->gMb.as<float>());
+      rc = mlp_forward(c, c->gXb.as<__nv_bfloat16>(), B, c->gY.as<float>());
+      if (rc != PM3GPU_OK) return rc;
+      loss_kernel<<<gblocks((long long)B * kOut), 256, 0, c->stream>>>(
+          c->gY.as<float>(), c->gTb.as<float>(), c->gMb.as<float>(), (long long)B * kOut,
+          (float)(1.0 / (mask_per_row * B)), c->gdY.as<__nv_bfloat16>(), accum);
+      // output layer
+      gemm_bf16<true, false>(c, kHid, kOut, B, c->gH[2].as<__nv_bfloat16>(), kHid, c->gdY.as<__nv_bfloat16>(), kOut,
+                             gg + kW4, kOut);
+      colsum_kernel<<<kOut, 256, 0, c->stream>>>(c->gdY.as<__nv_bfloat16>(), kOut, B, gg + kB4);
+      gemm_bf16<false, true>(c, B, kHid, kOut, c->gdY.as<__nv_bfloat16>(), kOut, Pb + kW4, kOut, c->gdH.as<float>(), kHid);
+      // hidden layers, last to first
+      for (int l = 2; l >= 0; --l) {
+        dact_kernel<<<gblocks((long long)B * kHid), 256, 0, c->stream>>>(c->gdH.as<float>(), c->gZ[l].as<float>(),
+                                                                         (long long)B * kHid, c->gdZ.as<__nv_bfloat16>());
+        const __nv_bfloat16* in = l > 0 ? c->gH[l - 1].as<__nv_bfloat16>() : c->gXb.as<__nv_bfloat16>();
+        const int kin = l > 0 ? kHid : kIn;
+        gemm_bf16<true, false>(c, kin, kHid, B, in, kin, c->gdZ.as<__nv_bfloat16>(), kHid, gg + woff[l], kHid);
+        colsum_kernel<<<kHid, 256, 0, c->stream>>>(c->gdZ.as<__nv_bfloat16>(), kHid, B, gg + boff[l]);
+        if (l > 0)
+          gemm_bf16<false, true>(c, B, kHid, kHid, c->gdZ.as<__nv_bfloat16>(), kHid, Pb + woff[l], kHid,
+                                 c->gdH.as<float>(), kHid);
+      }
+      ++c->adam_steps;
+      const float b1 = 0.9f, b2 = 0.999f;
+      const float c1 = 1.0f - std::pow(b1, (float)c->adam_steps), c2 = 1.0f - std::pow(b2, (float)c->adam_steps);
+      adam_kernel<<<gblocks(np), 256, 0, c->stream>>>(gp, gg, c->gm.as<float>(), c->gv.as<float>(), (int)np, lr, b1, b2,
+                                                      c1, c2, c->gpb.as<__nv_bfloat16>());
+      CUDA_TRY(c, cudaGetLastError());
+    }
+    if (losses) {
+      float sum = 0.0f;
+      CUDA_TRY(c, cudaMemcpyAsync(&sum, accum, 4, cudaMemcpyDeviceToHost, c->stream));
+      CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+      losses[ep] = (float)(sum / (mask_per_row * (double)nbatch * B));
+    }
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return PM3GPU_OK;
+}
+
 int pm3gpu_set_large_threshold(pm3gpu_ctx* c, int nao) {
   if (!c) return PM3GPU_INVALID_INPUT;
   if (nao < 1 || nao > kMaxN + 1) return fail(c, PM3GPU_INVALID_INPUT, "large-path threshold outside 1..257");
@@ -1163,6 +1557,8 @@ int noalloc_run(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz,
   std::memset(result, 0, sizeof(*result));
   if (n_atoms < 1 || n_atoms > kMaxN)
     return fail(c, PM3GPU_INVALID_INPUT, "atom count outside 1..256 for the allocation-free path");
+  if (o->guess == PM3GPU_GUESS_LEARNED)
+    return fail(c, PM3GPU_INVALID_INPUT, "the learned guess is not available on the allocation-free path");
   MolPlan p;
   plan_molecule(c, z, xyz, n_atoms, o, p);
   result->nao = p.nao;

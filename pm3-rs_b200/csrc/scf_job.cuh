@@ -52,6 +52,20 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
     eigensolve(c, Ap, n < kv + 1 ? n : kv + 1, kv, c.Vt, c.tri_a + 2 * n, nullptr);
     density(c, c.Vt, na, uhf ? 1.0 : 2.0, Pa, Pa, 0.0);
     if (uhf) density(c, c.Vt, nb, 1.0, Pb, Pb, 0.0);
+  } else if (J.guess == 4) {  // given (learned) density, scaled to the electron count
+    const double* G0 = A.guess_dens + J.guess_off;
+    double tr = 0.0;
+    for (int k = tid; k < n; k += kThreads) tr += G0[(size_t)k * n + k];
+    tr = block_sum(tr, c.red);
+    const double ne = (double)(na + nb);
+    const double sc = tr > 0.0 ? ne / tr : 0.0;
+    const double fa = uhf ? (ne > 0.0 ? na / ne : 0.5) : 1.0, fb = ne > 0.0 ? nb / ne : 0.5;
+    for (size_t k = tid; k < nn; k += kThreads) {
+      const double g = G0[k] * sc;
+      Pa[k] = fa * g;
+      if (uhf) Pb[k] = fb * g;
+    }
+    __syncthreads();
   } else {
     double fa = 1.0, fb = 0.0;
     if (uhf) {
@@ -315,8 +329,13 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
   mark(c, kPhFinal);
   if (tid == 0) {
     *out = o;
-    // stability search (scf.rs:599-715): queue this molecule's rungs for any free CTA
-    if (J.nrung > 0 && (J.stab == 2 || (J.stab == 1 && o.gap < 6.0))) {
+    if (J.backup >= 0 && !o.converged) {  // learned start failed: the standard-guess pass takes over
+      const int base = atomicAdd(&A.queue[1], 1);
+      A.rlist[base] = J.backup;
+      __threadfence();
+      atomicExch(&A.rready[base], 1);
+    } else if (J.nrung > 0 && (J.stab == 2 || (J.stab == 1 && o.gap < 6.0))) {
+      // stability search (scf.rs:599-715): queue this molecule's rungs for any free CTA
       const int base = atomicAdd(&A.queue[1], J.nrung);
       for (int k = 0; k < J.nrung; ++k) A.rlist[base + k] = J.rung0 + k;
       __threadfence();

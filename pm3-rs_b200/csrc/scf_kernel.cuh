@@ -40,14 +40,15 @@ struct JobDesc {
   int mol;     // molecule index (host bookkeeping)
   int rung0, nrung;  // stability-search jobs of this molecule in the rung table (first pass only)
   int stab;    // 0 no search, 1 search when the frontier gap < 6 eV, 2 always (first pass only)
-  int guess;   // 1 SAD, 2 core Hamiltonian, 3 symmetry-broken SAD
+  int backup;  // rung-table job that repeats this pass from the standard guess if it fails (-1: none)
+  int guess;   // 1 SAD, 2 core Hamiltonian, 3 symmetry-broken SAD, 4 given density (learned guess)
   int accel;   // 0 none, 1 CDIIS, 2 A-DIIS -> CDIIS (already combined with use_diis)
   int depth;   // accelerator history length
   int max_scf;
   double e_tol, p_tol, adiis_switch, shift, damping;
   long long charge_off;   // into charges[] (natom values)
   long long dens_off;     // into densities[] (nao^2), when kJobDensity
-  long long grad_off;     // unused (the gradient kernel works from the exported densities)
+  long long guess_off;    // into guess_dens[] (nao^2), when guess == 4 (learned initial density)
   long long eps_off;      // into eps[] (2 nao: alpha then beta), when kJobEps
 };
 
@@ -87,6 +88,7 @@ struct KernelArgs {
   int* rready;           // [nrjobs] 1 once rlist[i] is published
   double* charges;
   double* densities;
+  const double* guess_dens;  // initial densities of guess-4 jobs
   double* grads;
   double* eps;
   double* work;          // per-CTA slots
