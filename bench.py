@@ -367,6 +367,93 @@ def water_main(args, rank):
     print(json.dumps(line))
 
 
+def basis_size(zs):
+    return int(sum(1 if int(v) == 1 else 4 for v in zs))
+
+
+def guess_main(args, rank):
+    """Learned initial density: train on seeded organics (5-60 atoms), then solve held-out organics
+    (20-90 atoms, basis within one CTA) from the learned start and from SAD; SCF iterations, time to
+    converged results, and how far the learned-start heats of formation are from the SAD ones."""
+    import ctypes
+
+    import torch
+
+    from pm3_rs import _lib, native, workloads
+
+    if rank != 0:
+        return
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    ctx = _lib.Context(0)
+    lib = ctx.lib
+    stream = torch.cuda.current_stream(dev)
+    lib.pm3gpu_set_stream(ctx.ptr, ctypes.c_void_p(stream.cuda_stream))
+    I32, D, F = ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float)
+    train = workloads.organic_batch(args.train, 5, 60, seed=90001)
+    offs, z, xyz = workloads.pack(train)
+    offs, z, xyz = np.ascontiguousarray(offs), np.ascontiguousarray(z), np.ascontiguousarray(xyz * A2B)
+    losses = np.zeros(args.epochs, np.float32)
+    opts = native.options()
+    t0 = time.perf_counter()
+    rc = lib.pm3gpu_guess_train(ctx.ptr, len(train), offs.ctypes.data_as(I32), z.ctypes.data_as(I32),
+                                xyz.ctypes.data_as(D), ctypes.byref(opts), args.epochs, 4096, 1e-3, 7,
+                                losses.ctypes.data_as(F))
+    if rc != 0:
+        raise RuntimeError(ctx.last_error())
+    train_s = time.perf_counter() - t0
+    held = [m for m in workloads.organic_batch(args.n_mol or 4096, 20, 90, seed=90002) if basis_size(m[0]) <= 256]
+    hoffs, hz, hxyz = workloads.pack(held)
+    hoffs, hz, hxyz = np.ascontiguousarray(hoffs), np.ascontiguousarray(hz), np.ascontiguousarray(hxyz * A2B)
+    n_mol = len(held)
+    res = (_lib.Result * n_mol)()
+    q = np.zeros(len(hz))
+
+    def solve(guess):
+        o = native.options(guess=guess)
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        rc = lib.pm3gpu_batch(ctx.ptr, n_mol, hoffs.ctypes.data_as(I32), hz.ctypes.data_as(I32),
+                              hxyz.ctypes.data_as(D), ctypes.byref(o), 0, res, q.ctypes.data_as(D), None)
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        if rc != 0:
+            raise RuntimeError(ctx.last_error())
+        return (s.elapsed_time(e), np.array([r.iterations for r in res]), np.array([r.status for r in res]),
+                np.array([r.heat_of_formation_kcal for r in res]))
+
+    for _ in range(max(args.warmup, 1)):
+        solve(1)
+        solve(_lib.GUESS_LEARNED)
+    sad = [solve(1) for _ in range(max(args.steps, 1))]
+    lrn = [solve(_lib.GUESS_LEARNED) for _ in range(max(args.steps, 1))]
+    ms_sad = statistics.median([x[0] for x in sad])
+    ms_lrn = statistics.median([x[0] for x in lrn])
+    it_sad, st_sad, hof_sad = sad[0][1], sad[0][2], sad[0][3]
+    it_lrn, st_lrn, hof_lrn = lrn[0][1], lrn[0][2], lrn[0][3]
+    both = (st_sad == 0) & (st_lrn == 0)
+    dhf = np.abs(hof_lrn[both] - hof_sad[both])
+    line = {
+        "metric": METRIC, "value": int((st_lrn == 0).sum()) / (ms_lrn * 1e-3), "unit": "SCF/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_lrn, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 SCF, bf16 network", "data": "synthetic",
+        "config": {"workload": f"learned-guess: trained on {len(train)} organics (5-60 atoms, seed 90001, "
+                               f"{args.epochs} epochs), evaluated on {n_mol} held-out organics (20-90 atoms, "
+                               "basis <= 256, seed 90002), RHF PM3 FP64",
+                   "train_seconds": train_s, "train_loss_per_epoch": [float(v) for v in losses]},
+        "standard_guess": {"scf_per_s": int((st_sad == 0).sum()) / (ms_sad * 1e-3), "ms_per_batch": ms_sad,
+                           "mean_iterations": float(it_sad[st_sad == 0].mean())},
+        "learned_guess": {"scf_per_s": int((st_lrn == 0).sum()) / (ms_lrn * 1e-3), "ms_per_batch": ms_lrn,
+                          "mean_iterations": float(it_lrn[st_lrn == 0].mean()),
+                          "converged": int((st_lrn == 0).sum()), "of": n_mol},
+        "max_abs_dhf_kcal_vs_standard": float(dhf.max()) if dhf.size else None,
+        "molecules_dhf_above_0.01_kcal": int((dhf > 0.01).sum()),
+        "time_to_converged_ratio": ms_sad / ms_lrn,
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -376,10 +463,13 @@ def main():
     ap.add_argument("--n-mol", type=int, default=None, help="molecules per step (default: 4096 organics, 2048 radicals)")
     ap.add_argument("--cpu-sample", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="organics-4096", choices=["organics-4096", "radicals-2048", "water-2000"],
+    ap.add_argument("--workload", default="organics-4096",
+                    choices=["organics-4096", "radicals-2048", "water-2000", "learned-guess"],
                     help="organics-4096: the batched headline (default); radicals-2048: 2048 doublet radicals "
                          "of 10-80 atoms, UHF + analytic gradients; water-2000: one 6000-atom water cluster "
                          "(12000 basis functions) on the whole-GPU path, seconds per SCF")
+    ap.add_argument("--train", type=int, default=20000, help="learned-guess workload: training molecules")
+    ap.add_argument("--epochs", type=int, default=6, help="learned-guess workload: training epochs")
     ap.add_argument("--waters", type=int, default=2000,
                     help="water-2000 workload: number of waters (the cluster uses the first sites of a 13 x 13 x 12 grid)")
     ap.add_argument("--phases", action="store_true",
@@ -395,6 +485,8 @@ def main():
 
     if args.workload == "water-2000":
         return water_main(args, rank)
+    if args.workload == "learned-guess":
+        return guess_main(args, rank)
     desc, oracle_opts, gpu_opts, want_grad, default_n = workload_spec(args)
     if args.n_mol is None:
         args.n_mol = default_n

@@ -210,7 +210,8 @@ int pm3gpu_set_large_threshold(pm3gpu_ctx* ctx, int nao);
 
 /* Learned initial density (no counterpart in the reference). A 3 x 256 BF16 MLP predicts every
  * atom block and atom-pair block of the initial density from element one-hots, 32 Gaussian
- * distance functions (6 A cutoff) and coordination counts; the SCF then starts from it (guess =
+ * distance functions (6 A cutoff) and coordination counts; the SCF starts from the aufbau density
+ * of that prediction's Fock matrix (guess =
  * PM3GPU_GUESS_LEARNED in the options). The plain SCF stays the judge: a molecule that does not
  * converge from the learned start is solved again from the standard guess.
  *

@@ -5,7 +5,8 @@
 // cutoff) and coordination counts. Pair blocks are described in the bond frame (x along a -> b):
 // P[s_a][s_b] = ss, P[s_a][p_b] = s_sigma u, P[p_a][s_b] = sigma_s u,
 // P[p_a][p_b] = sigma_sigma u u^T + pi_pi (I - u u^T); atom blocks by P_ss and the mean p
-// population. The SCF then starts from the assembled matrix (scaled to the electron count).
+// population. The assembled matrix, scaled to the electron count, gives the first Fock matrix;
+// its aufbau density is where the SCF iteration starts.
 //
 // Everything runs on the device: features, training targets from converged densities, the GEMMs
 // (mma.sync m16n8k16 BF16 -> FP32, hand-written), activations, loss, backward pass, Adam, and the

@@ -66,6 +66,25 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
       if (uhf) Pb[k] = fb * g;
     }
     __syncthreads();
+    // The prediction is not an idempotent density, and A-DIIS would treat it as one. One
+    // Roothaan step turns it into an aufbau density (as the core guess does with H): its Fock
+    // matrix, diagonalised, gives the occupied orbitals the iteration starts from.
+    if (!uhf) {
+      build_fock(c, Pa, nullptr, nullptr, c.F, nullptr);
+    } else {
+      double* Pt = c.Vb + nn;
+      for (size_t k = tid; k < nn; k += kThreads) Pt[k] = Pa[k] + Pb[k];
+      __syncthreads();
+      build_fock(c, Pt, Pa, Pb, c.F, c.G);
+    }
+    double* Ap = pack_input(c, c.F, nullptr, 0.0);
+    eigensolve(c, Ap, n < na + 1 ? n : na + 1, na, c.Vt, c.tri_a + 2 * n, nullptr);
+    density(c, c.Vt, na, uhf ? 1.0 : 2.0, Pa, Pa, 0.0);
+    if (uhf) {
+      Ap = pack_input(c, c.G, nullptr, 0.0);
+      eigensolve(c, Ap, n < nb + 1 ? n : nb + 1, nb, c.Vb, c.tri_b + 2 * n, nullptr);
+      density(c, c.Vb, nb, 1.0, Pb, Pb, 0.0);
+    }
   } else {
     double fa = 1.0, fb = 0.0;
     if (uhf) {
