@@ -275,6 +275,10 @@ def water_main(args, rank):
     stream = torch.cuda.current_stream(dev)
     lib.pm3gpu_set_stream(ctx.ptr, ctypes.c_void_p(stream.cuda_stream))
     opts = native.options()
+    mixed = args.precision == "mixed"
+    mode = _lib.PRECISION_MIXED if mixed else _lib.PRECISION_FP64
+    if lib.pm3gpu_set_precision(ctx.ptr, mode) != 0:
+        raise RuntimeError(ctx.last_error())
     res = (_lib.Result * 1)()
     q = np.zeros(n_atoms)
     d_z, d_xyz = torch.from_numpy(z).to(dev), torch.from_numpy(xyz).to(dev)
@@ -315,6 +319,10 @@ def water_main(args, rank):
     clocks = clk.summary()
     launches = lib.pm3gpu_last_kernel_launches(ctx.ptr)
     iters, hof = res[0].iterations, res[0].heat_of_formation_kcal
+    nrow = lib.pm3gpu_last_large_trace(ctx.ptr, None, 0)
+    trace = np.zeros((max(nrow, 1), 5))
+    lib.pm3gpu_last_large_trace(ctx.ptr, trace.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nrow)
+    trace = trace[:nrow]
     hb, db = ctypes.c_longlong(), ctypes.c_longlong()
     e_ms = timed(run_host, 1)
     lib.pm3gpu_last_transfer_bytes(ctx.ptr, ctypes.byref(hb), ctypes.byref(db))
@@ -322,6 +330,7 @@ def water_main(args, rank):
     os.environ["PM3GPU_PROFILE"] = "1"
     pctx = _lib.Context(0)
     pctx.lib.pm3gpu_set_stream(pctx.ptr, ctypes.c_void_p(stream.cuda_stream))
+    pctx.lib.pm3gpu_set_precision(pctx.ptr, mode)
     rc = pctx.lib.pm3gpu_batch_device_inputs(pctx.ptr, 1, None, ctypes.c_void_p(d_z.data_ptr()),
                                              ctypes.c_void_p(d_xyz.data_ptr()), offs.ctypes.data_as(I32),
                                              z.ctypes.data_as(I32), ctypes.byref(opts), res, q.ctypes.data_as(D),
@@ -342,12 +351,33 @@ def water_main(args, rank):
         peak, peak_src = 6650.0, "fallback 6.65 TB/s"
     achieved = tri_bytes / (tri_ms * 1e-3) / 1e9 if tri_ms > 0 else None
     value = statistics.median(ms) * 1e-3
+    accuracy = None
+    if mixed:  # the mixed result against an FP64 solve of the same cluster, gradients included
+        gctx = _lib.Context(0)
+        gctx.lib.pm3gpu_set_stream(gctx.ptr, ctypes.c_void_p(stream.cuda_stream))
+        out = {}
+        for name, m in (("fp64", _lib.PRECISION_FP64), ("mixed", _lib.PRECISION_MIXED)):
+            gctx.lib.pm3gpu_set_precision(gctx.ptr, m)
+            r, g = _lib.Result(), np.zeros(3 * n_atoms)
+            rc = gctx.lib.pm3gpu_gradient(gctx.ptr, n_atoms, z.ctypes.data_as(I32), xyz.ctypes.data_as(D),
+                                          ctypes.byref(opts), ctypes.byref(r), q.ctypes.data_as(D),
+                                          g.ctypes.data_as(D))
+            if rc != 0:
+                raise RuntimeError(gctx.last_error())
+            out[name] = (r.heat_of_formation_kcal, r.iterations, g * (23.060547830619 * 1.8897261246))  # eV/Bohr -> kcal/mol/A
+        accuracy = {"fp64_heat_of_formation_kcal": out["fp64"][0], "fp64_iterations": out["fp64"][1],
+                    "delta_hof_kcal": out["mixed"][0] - out["fp64"][0],
+                    "max_gradient_error_kcal_per_A": float(np.abs(out["mixed"][2] - out["fp64"][2]).max()),
+                    "split_bf16_iterations": int(trace[:, 4].sum()), "fp64_closing_iterations": int(nrow - trace[:, 4].sum())}
     line = {
         "metric": METRIC, "value": value, "unit": "s/SCF", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": statistics.median(ms), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"water-{nw}: {nw} H2O ({3 * nw} atoms, {6 * nw} basis functions), RHF PM3 FP64, "
-                               "reference default options", "iterations": iters, "heat_of_formation_kcal": hof,
+        "dtype": "bf16x3/f32 + f64" if mixed else "f64", "data": "synthetic",
+        "config": {"workload": f"water-{nw}: {nw} H2O ({3 * nw} atoms, {6 * nw} basis functions), RHF PM3 "
+                               + ("mixed (split-BF16 density and commutator, FP64 closing iterations)" if mixed
+                                  else "FP64") + ", reference default options",
+                   "iterations": iters, "heat_of_formation_kcal": hof,
+                   "rms_density_change": [float(f"{v:.3g}") for v in trace[:, 2]],
                    "l2": "inputs and matrices (1.15 GB each) far exceed L2", "parallelism": "replicas only"},
         "e2e": {"value": e_ms[0] * 1e-3, "unit": "s/SCF", "h2d_bytes_per_step": hb.value, "d2h_bytes_per_step": db.value},
         "gpu_launches": launches,
@@ -359,6 +389,8 @@ def water_main(args, rank):
         "phases_ms": phases,
         "clocks": clocks,
     }
+    if accuracy:
+        line["accuracy_vs_fp64"] = accuracy
     if not args.no_cpu_baseline:
         total, cores, setup, per_iter = water_cpu_baseline(nw, iters)
         line["cpu_baseline"] = {"value": total, "unit": "s/SCF", "cores": cores, "kind": "port",
@@ -472,6 +504,9 @@ def main():
     ap.add_argument("--epochs", type=int, default=6, help="learned-guess workload: training epochs")
     ap.add_argument("--waters", type=int, default=2000,
                     help="water-2000 workload: number of waters (the cluster uses the first sites of a 13 x 13 x 12 grid)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="water-2000 workload: FP64 throughout, or split-BF16 density and commutator products "
+                         "with FP64 closing iterations (reports the heat-of-formation and gradient error against FP64)")
     ap.add_argument("--phases", action="store_true",
                     help="after the timed steps, run one more (untimed) batch with per-phase SM-cycle counters "
                          "and print the phase shares to stderr")

@@ -208,6 +208,23 @@ int pm3gpu_last_kernel_launches(pm3gpu_ctx* ctx);
  * reference has one CPU path). */
 int pm3gpu_set_large_threshold(pm3gpu_ctx* ctx, int nao);
 
+/* Arithmetic of the whole-GPU path's density and commutator products (no counterpart in the
+ * reference, whose products are FP64). PM3GPU_PRECISION_MIXED takes them from split-BF16
+ * tensor-core GEMMs (x = hi + lo, products hi*hi + hi*lo + lo*hi, FP32 accumulation) while the
+ * density is far from converged, then closes the SCF with FP64 iterations: integrals, Fock build,
+ * eigensolver, DIIS solve, energies and gradients stay FP64, and only an FP64 iteration can pass
+ * the convergence test. The per-CTA path (n <= 256) is FP64 in both modes. Default FP64. */
+#define PM3GPU_PRECISION_FP64 0
+#define PM3GPU_PRECISION_MIXED 1
+int pm3gpu_set_precision(pm3gpu_ctx* ctx, int mode);
+
+/* Per-iteration record of the last whole-GPU solve (the reference's PM3_TIMING trace,
+ * scf.rs:1206-1296, as numbers): rows of 5 doubles (pass: 1 = first SCF, 2.. = stability rungs;
+ * |dE| in eV, infinite on a pass's first iteration; RMS density change; DIIS error norm
+ * ||FP - PF||, 0 without an accelerator; 1 if the iteration ran split-BF16, else 0). Copies at
+ * most max_rows rows and returns the total number of rows. */
+int pm3gpu_last_large_trace(pm3gpu_ctx* ctx, double* rows, int max_rows);
+
 /* Learned initial density (no counterpart in the reference). A 3 x 256 BF16 MLP predicts every
  * atom block and atom-pair block of the initial density from element one-hots, 32 Gaussian
  * distance functions (6 A cutoff) and coordination counts; the SCF starts from the aufbau density

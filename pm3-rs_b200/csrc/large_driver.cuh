@@ -15,6 +15,9 @@
 // cluster's invariant subspace, which is all the density P = w C_occ C_occ^T depends on.
 
 constexpr size_t kBlasWorkspace = 64u << 20;  // cuBLAS workspace, set before graph capture
+// Mixed mode hands over to FP64 once the RMS density change is below this (about ten times the
+// split-BF16 density noise at n = 12000).
+constexpr double kMixedSwitch = 1.0e-5;
 
 struct TriGraph {
   static constexpr int kKeys = 17;
@@ -38,10 +41,11 @@ struct LargeBufs {
   DevBuf V, Wp, y, wtmp, ps, s64, vcol, tp, ctr, refl;
   DevBuf X, Xt, Dp, Lp, Um;
   DevBuf Gm, Mm, Tm, Z1, Z2, blocks, Gk;
+  DevBuf mh[2], ml[2], c32;  // mixed mode: BF16 hi / lo parts of two operands, FP32 product
   void release() {
     for (DevBuf* b : {&ao, &sprow, &sroff, &H, &W, &hacc, &dpk, &jacc, &part, &part2, &scal, &P[0], &P[1], &Q[0], &Q[1], &Pt,
                       &F, &G, &hist, &A, &d, &e, &e2, &tau, &lam, &dlam, &blk, &V, &Wp, &y, &wtmp, &ps, &s64, &vcol, &tp, &ctr, &refl, &X, &Xt,
-                      &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk})
+                      &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk, &mh[0], &mh[1], &ml[0], &ml[1], &c32})
       b->release();
     blas_ws.release();
     tg.reset();
@@ -254,8 +258,15 @@ class LargeSolver {
     double e_old = 0.0, last_change = INFINITY;
     bool converged = false;
     const int kva = std::min(n, na + 1), kvb = std::min(n, nb + 1);
+    // Mixed mode: the commutator and the density come from split-BF16 products until the density
+    // settles (kMixedSwitch) or stops improving, then FP64 iterations close the SCF; only an FP64
+    // iteration can satisfy the convergence test, so the result is the FP64 fixed point.
+    bool lowp = c_->precision == PM3GPU_PRECISION_MIXED;
+    ++passes_;
     for (int iter = 0; iter < J.max_scf; ++iter) {
       iterations = iter + 1;
+      const bool lowp_iter = lowp;
+      double trace_err = 0.0;
       double* Pc = B_.P[cur].as<double>();
       double* Pn = B_.P[1 - cur].as<double>();
       double* Qc = uhf ? B_.Q[cur].as<double>() : nullptr;
@@ -305,9 +316,9 @@ class LargeSolver {
       // ---- accelerator (scf.rs:1240-1259 RHF; 1398-1413 UHF)
       bool use_hist = false;
       if (J.accel != 0) {
-        int rc = commutator(Fa, Pc, Ea);
+        int rc = commutator(Fa, Pc, Ea, lowp_iter);
         if (rc) return rc;
-        if (uhf && (rc = commutator(Fb, Qc, Eb))) return rc;
+        if (uhf && (rc = commutator(Fb, Qc, Eb, lowp_iter))) return rc;
         if (keep && (rc = copy(Pc, Dh))) return rc;
         double ee;
         if ((rc = dot(Ea, Ea, Eb, Eb, &ee))) return rc;
@@ -331,6 +342,7 @@ class LargeSolver {
         mg[len * kMaxDepth + len] = dnf;
         const int m = len + 1;
         const double err = std::sqrt(ee);
+        trace_err = err;
         bool ok;
         if (!uhf && J.accel == 2 && err > J.adiis_switch) {
           ok = keep && m >= 2;
@@ -369,7 +381,7 @@ class LargeSolver {
         if (rc) return rc;
         double* Pold = spin == 0 ? Pc : Qc;
         double* Pnew = spin == 0 ? Pn : Qn;
-        rc = density_from_x(occ, occ, uhf ? 1.0 : 2.0, Pnew);
+        rc = density_from_x(occ, occ, uhf ? 1.0 : 2.0, Pnew, lowp_iter);
         if (rc) return rc;
         tick(kLgDensity);
         double sq;
@@ -385,10 +397,13 @@ class LargeSolver {
       const double dp = uhf ? std::sqrt(sq_a / (double)nn_) + std::sqrt(sq_b / (double)nn_)
                             : std::sqrt(sq_a / (double)nn_);
       const double de = std::fabs(e_elec - e_old);
+      c_->ltrace.insert(c_->ltrace.end(), {(double)passes_, iter > 0 ? de : INFINITY, dp, trace_err, lowp_iter ? 1.0 : 0.0});
+      if (lowp && (dp < kMixedSwitch || (iter >= 2 && dp < 1.0e-3 && dp > 0.7 * last_change) || 2 * iter >= J.max_scf))
+        lowp = false;
       last_change = dp;
       e_old = e_elec;
       cur = 1 - cur;
-      if (iter > 0 && de < J.e_tol && dp < J.p_tol) {
+      if (!lowp_iter && iter > 0 && de < J.e_tol && dp < J.p_tol) {
         converged = true;
         break;
       }
@@ -479,6 +494,7 @@ class LargeSolver {
   large::Mol m_{};
   const int32_t* hz_ = nullptr;
   int N_ = 0, n_ = 0;
+  int passes_ = 0;  // SCF passes of this molecule (first pass, stability rungs)
   size_t nn_ = 0;
   long long wcap_ = 1;
   const double* final_pt_ = nullptr;
@@ -533,7 +549,15 @@ class LargeSolver {
     return PM3GPU_OK;
   }
   // E = F P - P F (scf.rs:1039-1054): row-major F P is cuBLAS's column-major P F.
-  int commutator(const double* F, const double* P, double* E) {
+  // Mixed mode (lowp) takes the product from split-BF16 tensor-core GEMMs with FP32 accumulation.
+  int commutator(const double* F, const double* P, double* E, bool lowp = false) {
+    if (lowp) {
+      int rc;
+      if ((rc = split(P, nn_, 0)) || (rc = split(F, nn_, 1)) ||
+          (rc = gemm_split(CUBLAS_OP_N, CUBLAS_OP_N, n_, n_, n_, n_, 0, 1)))
+        return rc;
+      return combine_transpose(E, 1.0, -1.0);
+    }
     const double one = 1.0, zero = 0.0;
     BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, n_, n_, n_, &one, P, n_, F, n_, &zero, E, n_));
     large::antisym_kernel<<<grid_for(nn_), large::kBlock, 0, c_->stream>>>(E, n_);
@@ -541,14 +565,52 @@ class LargeSolver {
     return PM3GPU_OK;
   }
   // P = w X X^T over the first k eigenvectors of the last eigensolve (X is n x ld, row-major).
-  int density_from_x(int k, int ld, double w, double* P) {
+  int density_from_x(int k, int ld, double w, double* P, bool lowp = false) {
     if (k == 0) {
       CUDA_TRY(c_, cudaMemsetAsync(P, 0, 8 * nn_, c_->stream));
       return PM3GPU_OK;
     }
+    if (lowp) {  // both operands are X: one split; the result is symmetrised
+      const double* X = B_.X.as<double>();
+      int rc;
+      if ((rc = split(X, (size_t)n_ * ld, 0)) || (rc = gemm_split(CUBLAS_OP_T, CUBLAS_OP_N, n_, k, ld, ld, 0, 0)))
+        return rc;
+      return combine_transpose(P, 0.5 * w, 0.5 * w);
+    }
     const double zero = 0.0;
     BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, n_, n_, k, &w, B_.X.as<double>(), ld,
                              B_.X.as<double>(), ld, &zero, P, n_));
+    return PM3GPU_OK;
+  }
+
+  // Split x (cnt doubles) into the BF16 hi / lo pair of operand slot s.
+  int split(const double* x, size_t cnt, int s) {
+    CUDA_TRY(c_, B_.mh[s].ensure(2 * cnt));
+    CUDA_TRY(c_, B_.ml[s].ensure(2 * cnt));
+    large::split_bf16_kernel<<<grid_for(cnt), large::kBlock, 0, c_->stream>>>(x, B_.mh[s].as<__nv_bfloat16>(),
+                                                                             B_.ml[s].as<__nv_bfloat16>(), cnt);
+    ++c_->launches;
+    CUDA_TRY(c_, cudaGetLastError());
+    return PM3GPU_OK;
+  }
+  // c32 = op(A) op(B), column-major m x m with inner dimension k, A and B the split operands of
+  // slots sa and sb: hi lo + lo hi first, then hi hi, all accumulated in FP32 on the tensor cores.
+  int gemm_split(cublasOperation_t ta, cublasOperation_t tb, int m, int k, int lda, int ldb, int sa, int sb) {
+    CUDA_TRY(c_, B_.c32.ensure(4 * (size_t)m * m));
+    const void* term[3][2] = {{B_.mh[sa].p, B_.ml[sb].p}, {B_.ml[sa].p, B_.mh[sb].p}, {B_.mh[sa].p, B_.mh[sb].p}};
+    const float one = 1.0f, zero = 0.0f;
+    for (int t = 0; t < 3; ++t)
+      BLAS_TRY(c_, cublasGemmEx(blas(), ta, tb, m, m, k, &one, term[t][0], CUDA_R_16BF, lda, term[t][1], CUDA_R_16BF, ldb,
+                                t == 0 ? &zero : &one, B_.c32.p, CUDA_R_32F, m, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT));
+    return PM3GPU_OK;
+  }
+  // out = a c32 + b c32^T in FP64 (row-major n x n).
+  int combine_transpose(double* out, double a, double b) {
+    const size_t tiles = (size_t)((n_ + 31) / 32) * ((n_ + 31) / 32);
+    large::transpose_combine_kernel<<<grid_for(tiles, 1), large::kBlock, 0, c_->stream>>>(B_.c32.as<float>(), out, n_, a,
+                                                                                         b);
+    ++c_->launches;
+    CUDA_TRY(c_, cudaGetLastError());
     return PM3GPU_OK;
   }
 

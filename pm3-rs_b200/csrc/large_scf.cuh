@@ -5,6 +5,8 @@
 // cuBLAS DGEMMs issued by the host driver; the Householder panel, the Sturm multisection, the
 // twisted-factorisation eigenvectors, the compact-WY factors and all reductions are here.
 #pragma once
+#include <cuda_bf16.h>
+
 #include "scf_kernel.cuh"
 
 namespace pm3gpu {
@@ -225,6 +227,45 @@ __global__ void __launch_bounds__(kBlock) antisym_kernel(double* E, int n) {
     }
   }
 }
+// ---------------------------------------------------------------- split-BF16 products (mixed mode)
+// x = hi + lo with hi = bf16(x) and lo = bf16(x - hi), both rounded to nearest even: 16
+// significant bits, relative representation error <= 2^-17. A product a b is then taken as
+// hi_a hi_b + hi_a lo_b + lo_a hi_b (each term exact in FP32, accumulated in FP32 on the tensor
+// cores); the dropped lo_a lo_b term is 2^-16 of the product.
+__global__ void __launch_bounds__(kBlock) split_bf16_kernel(const double* __restrict__ x, __nv_bfloat16* __restrict__ hi,
+                                                            __nv_bfloat16* __restrict__ lo, size_t cnt) {
+  for (size_t k = blockIdx.x * (size_t)kBlock + threadIdx.x; k < cnt; k += (size_t)gridDim.x * kBlock) {
+    const double v = x[k];
+    const __nv_bfloat16 h = __double2bfloat16(v);
+    hi[k] = h;
+    lo[k] = __double2bfloat16(v - (double)__bfloat162float(h));
+  }
+}
+// out[i][j] = a C[i][j] + b C[j][i] (row-major n x n, C in FP32, out in FP64): the commutator's
+// antisymmetrisation (a = 1, b = -1) and the density's symmetrisation (a = b = w / 2). One block
+// per 32 x 32 output tile; the mirrored tile is read through shared memory so both reads and the
+// write are coalesced.
+__global__ void __launch_bounds__(kBlock) transpose_combine_kernel(const float* __restrict__ C, double* __restrict__ out,
+                                                                   int n, double a, double b) {
+  __shared__ float t[32][33];
+  const int tiles = (n + 31) / 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+  for (int tile = blockIdx.x; tile < tiles * tiles; tile += gridDim.x) {
+    const int i0 = (tile / tiles) * 32, j0 = (tile % tiles) * 32;
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {  // mirrored tile rows j0 + r, columns i0 + tx
+      const int row = j0 + r, col = i0 + tx;
+      t[r][tx] = (row < n && col < n) ? C[(size_t)row * n + col] : 0.0f;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+      const int row = i0 + r, col = j0 + tx;
+      if (row < n && col < n)
+        out[(size_t)row * n + col] = a * (double)C[(size_t)row * n + col] + b * (double)t[tx][r];
+    }
+  }
+}
+
 struct Comb {
   const double* m[8];
   double c[8];

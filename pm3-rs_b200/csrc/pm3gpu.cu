@@ -104,6 +104,8 @@ struct pm3gpu_ctx {
   LargeBufs* lbuf = nullptr;
   DevBuf lsel;                // densities of the selected state (P_tot | P_alpha | P_beta)
   double large_ms[16] = {};   // phase times of the last whole-GPU solve (profiling only)
+  int precision = PM3GPU_PRECISION_FP64;  // arithmetic of the whole-GPU path's dense products
+  std::vector<double> ltrace;  // per-iteration record of the last whole-GPU solve (5 per row)
   // learned initial density: FP32 master parameters, BF16 copy, Adam moments, gradients
   bool has_guess_model = false;
   long long adam_steps = 0;
@@ -478,6 +480,7 @@ int run_large(pm3gpu_ctx* c, const MolPlan& p, const int32_t* hz, const int32_t*
               const pm3gpu_options* o, const Want& want, pm3gpu_result& Rm, double* charges, double* density,
               double* mo_energies, double* gradient) {
   for (double& t : c->large_ms) t = 0.0;
+  c->ltrace.clear();
   if (!c->blas) BLAS_TRY(c, cublasCreate(&c->blas));
   BLAS_TRY(c, cublasSetStream(c->blas, c->stream));
   if (!c->lbuf) c->lbuf = new LargeBufs();
@@ -1485,6 +1488,23 @@ int pm3gpu_guess_train(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int3
   }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return PM3GPU_OK;
+}
+
+int pm3gpu_set_precision(pm3gpu_ctx* c, int mode) {
+  if (!c) return PM3GPU_INVALID_INPUT;
+  if (mode != PM3GPU_PRECISION_FP64 && mode != PM3GPU_PRECISION_MIXED)
+    return fail(c, PM3GPU_INVALID_INPUT, "precision must be PM3GPU_PRECISION_FP64 or PM3GPU_PRECISION_MIXED");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->precision = mode;
+  return PM3GPU_OK;
+}
+
+int pm3gpu_last_large_trace(pm3gpu_ctx* c, double* rows, int max_rows) {
+  if (!c) return 0;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const int total = (int)(c->ltrace.size() / 5);
+  if (rows && max_rows > 0) std::copy_n(c->ltrace.begin(), 5 * (size_t)std::min(total, max_rows), rows);
+  return total;
 }
 
 int pm3gpu_set_large_threshold(pm3gpu_ctx* c, int nao) {

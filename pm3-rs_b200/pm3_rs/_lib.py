@@ -10,6 +10,8 @@ LIB_PATH = os.path.join(_HERE, "libpm3gpu.so")
 OK = 0
 GUESS_LEARNED = 4
 GUESS_PARAMS = 150280
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
 INVALID_INPUT = 1
 MISSING_ELEMENT = 2
 RESOURCE_LIMIT = 3
@@ -71,6 +73,7 @@ EXPORTS = [
     "pm3gpu_batch_device_inputs", "pm3gpu_core_hamiltonian", "pm3gpu_fock", "pm3gpu_last_timings",
     "pm3gpu_last_kernel_launches", "pm3gpu_last_transfer_bytes", "pm3gpu_last_phase_cycles",
     "pm3gpu_single_point_noalloc", "pm3gpu_set_large_threshold", "pm3gpu_last_large_phase_ms",
+    "pm3gpu_set_precision", "pm3gpu_last_large_trace",
     "pm3gpu_guess_train", "pm3gpu_guess_set_params", "pm3gpu_guess_get_params", "pm3gpu_guess_predict",
 ]
 
@@ -116,6 +119,8 @@ def load() -> ctypes.CDLL:
     L.pm3gpu_last_kernel_launches.argtypes = [ctypes.c_void_p]
     L.pm3gpu_set_large_threshold.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.pm3gpu_last_large_phase_ms.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
+    L.pm3gpu_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.pm3gpu_last_large_trace.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     _F = ctypes.POINTER(ctypes.c_float)
     L.pm3gpu_guess_train.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, ctypes.POINTER(Options), ctypes.c_int,
                                      ctypes.c_int, ctypes.c_float, ctypes.c_uint, _F]
