@@ -218,8 +218,8 @@ int pm3gpu_set_large_threshold(pm3gpu_ctx* ctx, int nao);
 #define PM3GPU_PRECISION_MIXED 1
 int pm3gpu_set_precision(pm3gpu_ctx* ctx, int mode);
 
-/* Per-iteration record of the last whole-GPU solve (the reference's PM3_TIMING trace,
- * scf.rs:1206-1296, as numbers): rows of 5 doubles (pass: 1 = first SCF, 2.. = stability rungs;
+/* Per-iteration convergence record of the last whole-GPU solve (no counterpart in the
+ * reference, whose PM3_TIMING trace, scf.rs:1206-1296, prints phase times only): rows of 5 doubles (pass: 1 = first SCF, 2.. = stability rungs;
  * |dE| in eV, infinite on a pass's first iteration; RMS density change; DIIS error norm
  * ||FP - PF||, 0 without an accelerator; 1 if the iteration ran split-BF16, else 0). Copies at
  * most max_rows rows and returns the total number of rows. */

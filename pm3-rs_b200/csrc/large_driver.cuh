@@ -15,9 +15,10 @@
 // cluster's invariant subspace, which is all the density P = w C_occ C_occ^T depends on.
 
 constexpr size_t kBlasWorkspace = 64u << 20;  // cuBLAS workspace, set before graph capture
-// Mixed mode hands over to FP64 once the RMS density change is below this (about ten times the
-// split-BF16 density noise at n = 12000).
-constexpr double kMixedSwitch = 1.0e-5;
+// Mixed mode hands over to FP64 once the RMS density change is below max(10 p_tol, this floor),
+// or when it stops falling. Measured on water clusters (n = 3000), split-BF16 densities track the
+// FP64 ones to three digits of the RMS change down to 2e-6.
+constexpr double kMixedFloor = 1.0e-6;
 
 struct TriGraph {
   static constexpr int kKeys = 17;
@@ -42,10 +43,11 @@ struct LargeBufs {
   DevBuf X, Xt, Dp, Lp, Um;
   DevBuf Gm, Mm, Tm, Z1, Z2, blocks, Gk;
   DevBuf mh[2], ml[2], c32;  // mixed mode: BF16 hi / lo parts of two operands, FP32 product
+  DevBuf gsync, vw, wv;      // cooperative panels: grid barrier, X = [V | W] and Y = [W | V]
   void release() {
     for (DevBuf* b : {&ao, &sprow, &sroff, &H, &W, &hacc, &dpk, &jacc, &part, &part2, &scal, &P[0], &P[1], &Q[0], &Q[1], &Pt,
                       &F, &G, &hist, &A, &d, &e, &e2, &tau, &lam, &dlam, &blk, &V, &Wp, &y, &wtmp, &ps, &s64, &vcol, &tp, &ctr, &refl, &X, &Xt,
-                      &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk, &mh[0], &mh[1], &ml[0], &ml[1], &c32})
+                      &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk, &mh[0], &mh[1], &ml[0], &ml[1], &c32, &gsync, &vw, &wv})
       b->release();
     blas_ws.release();
     tg.reset();
@@ -398,7 +400,8 @@ class LargeSolver {
                             : std::sqrt(sq_a / (double)nn_);
       const double de = std::fabs(e_elec - e_old);
       c_->ltrace.insert(c_->ltrace.end(), {(double)passes_, iter > 0 ? de : INFINITY, dp, trace_err, lowp_iter ? 1.0 : 0.0});
-      if (lowp && (dp < kMixedSwitch || (iter >= 2 && dp < 1.0e-3 && dp > 0.7 * last_change) || 2 * iter >= J.max_scf))
+      if (lowp && (dp < std::max(10.0 * J.p_tol, kMixedFloor) || (iter >= 2 && dp < 1.0e-3 && dp > 0.7 * last_change) ||
+                   2 * iter >= J.max_scf))
         lowp = false;
       last_change = dp;
       e_old = e_elec;
@@ -494,6 +497,7 @@ class LargeSolver {
   large::Mol m_{};
   const int32_t* hz_ = nullptr;
   int N_ = 0, n_ = 0;
+  int coop_g_ = -1;  // cooperative panel grid for this device (-1: not yet queried)
   int passes_ = 0;  // SCF passes of this molecule (first pass, stability rungs)
   size_t nn_ = 0;
   long long wcap_ = 1;
@@ -618,6 +622,12 @@ class LargeSolver {
   // set of buffers, so it is captured once into a CUDA graph and replayed in later SCF
   // iterations (it is ~5 launches per column). Streams that cannot be captured run it directly.
   int run_tridiag(double* A) {
+    if (coop_grid() > 0) {  // one cooperative launch per panel: few enough launches to issue directly
+      int launches = 0;
+      const int rc = enqueue_tridiag(A, launches);
+      c_->launches += launches;
+      return rc;
+    }
     TriGraph& g = B_.tg;
     const void* key[TriGraph::kKeys] = {A,        B_.V.p,  B_.Wp.p,    B_.vcol.p, B_.y.p,   B_.wtmp.p,
                                         B_.ps.p,  B_.s64.p, B_.part.p, B_.part2.p, B_.d.p,   B_.e.p,
@@ -658,9 +668,32 @@ class LargeSolver {
     return PM3GPU_OK;
   }
 
+  // Grid of the cooperative panel kernel for this matrix size, 0 when the multi-launch path runs
+  // instead (no cooperative launch, PM3GPU_COOP_PANELS=0, or more 64-row stripes than blocks:
+  // each block owns one stripe).
+  int coop_grid() {
+    if (!c_->coop_panels) return 0;
+    if (coop_g_ < 0) {
+      int occ = 0, coop = 0;
+      if (cudaFuncSetAttribute(large::panel_coop_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)large::kCoopSmem) != cudaSuccess ||
+          cudaFuncSetAttribute(large::panel_coop_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)large::kCoopSmem) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, large::panel_coop_kernel<true>, large::kBlock,
+                                                        large::kCoopSmem) != cudaSuccess ||
+          cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c_->device) != cudaSuccess) {
+        (void)cudaGetLastError();
+        occ = coop = 0;
+      }
+      coop_g_ = (coop && occ > 0) ? std::min(occ, 2) * c_->sms : 0;
+    }
+    if ((long long)coop_g_ * large::kTile < n_) return 0;
+    return coop_g_;
+  }
+
   // Enqueues the blocked reduction of A (no host synchronisation inside).
   int enqueue_tridiag(double* A, int& launches) {
-    const int n = n_;
+    int n = n_;
     double* d = B_.d.as<double>();
     double* e = B_.e.as<double>();
     double* tau = B_.tau.as<double>();
@@ -668,8 +701,45 @@ class LargeSolver {
     double* W = B_.Wp.as<double>();
     double* vcol = B_.vcol.as<double>();
     const double one = 1.0, mone = -1.0;
+    const int G = coop_grid();
+    large::GridSync* gs = nullptr;
+    double *X = nullptr, *Y = nullptr;
+    if (G > 0) {
+      CUDA_TRY(c_, B_.gsync.ensure(sizeof(large::GridSync)));
+      CUDA_TRY(c_, B_.vw.ensure(8 * (size_t)n * large::kCoopLd));
+      CUDA_TRY(c_, B_.wv.ensure(8 * (size_t)n * large::kCoopLd));
+      gs = B_.gsync.as<large::GridSync>();
+      X = B_.vw.as<double>();
+      Y = B_.wv.as<double>();
+      CUDA_TRY(c_, cudaMemsetAsync(gs, 0, sizeof(large::GridSync), c_->stream));
+    }
     for (int p = 0; p < n - 2; p += large::kPanel) {
-      const int b = std::min(large::kPanel, n - 2 - p);
+      int b = std::min(large::kPanel, n - 2 - p);
+      if (G > 0) {
+        double *tp = B_.tp.as<double>(), *pn = B_.part.as<double>();
+        double *ps = B_.ps.as<double>(), *st = B_.s64.as<double>(), *pq = B_.part2.as<double>();
+        void* args[] = {&A, &n, &p, &b, &X, &Y, &d, &e, &tau, &tp, &pn, &ps, &st, &pq, &gs};
+        const void* fn = (n & 1) ? (const void*)large::panel_coop_kernel<false> : (const void*)large::panel_coop_kernel<true>;
+        CUDA_TRY(c_, cudaLaunchCooperativeKernel(fn, dim3(G), dim3(large::kBlock), args,
+                                                 large::kCoopSmem, c_->stream));
+        ++launches;
+        const int q = p + b, m = n - q;
+        if (m > 0) {  // A[q:, q:] -= X Y^T (row-major); column-major: C -= Yc^T Xc, inner dimension 2b
+          double* C = A + (size_t)q * n + q;
+          const double* Xq = X + (size_t)q * large::kCoopLd;
+          const double* Yq = Y + (size_t)q * large::kCoopLd;
+          if (b == large::kPanel) {
+            BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, 2 * b, &mone, Yq, large::kCoopLd, Xq,
+                                     large::kCoopLd, &one, C, n));
+          } else {  // last, narrower panel: columns b.. of X and Y are not part of it
+            BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Yq, large::kCoopLd, Xq,
+                                     large::kCoopLd, &one, C, n));
+            BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Yq + large::kPanel, large::kCoopLd,
+                                     Xq + large::kPanel, large::kCoopLd, &one, C, n));
+          }
+        }
+        continue;
+      }
       for (int j = 0; j < b; ++j) {
         const int i = p + j;
         const int m = n - i - 1;
@@ -793,7 +863,7 @@ class LargeSolver {
     CUDA_TRY(c_, B_.ps.ensure(8 * 64 * (size_t)large::kRedBlocks));
     CUDA_TRY(c_, B_.s64.ensure(8 * 64));
     {
-      const long long nt = (n - 1 + large::kTile - 1) / large::kTile;
+      const long long nt = (n + large::kTile - 1) / large::kTile;  // absolute stripes (covers the trailing ones)
       CUDA_TRY(c_, B_.tp.ensure(8 * (size_t)(2 * large::kTile) * (size_t)std::max<long long>(nt * (nt + 1) / 2, 1)));
       if (!B_.ctr.p) {
         CUDA_TRY(c_, B_.ctr.ensure(256));
@@ -818,7 +888,11 @@ class LargeSolver {
       std::vector<double> hd(n), he(n);
       CUDA_TRY(c_, cudaMemcpyAsync(hd.data(), d, 8 * (size_t)n, cudaMemcpyDeviceToHost, c_->stream));
       CUDA_TRY(c_, cudaMemcpyAsync(he.data(), e, 8 * (size_t)n, cudaMemcpyDeviceToHost, c_->stream));
+      large::GridSync gsh{};
+      if (coop_grid() > 0)
+        CUDA_TRY(c_, cudaMemcpyAsync(&gsh, B_.gsync.p, sizeof(gsh), cudaMemcpyDeviceToHost, c_->stream));
       CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+      if (gsh.err) return fail(c_, PM3GPU_CUDA_ERROR, "Householder panel: a grid barrier wait ran out");
       if (tri) {
         tri->assign(2 * (size_t)n, 0.0);
         std::copy(hd.begin(), hd.end(), tri->begin());

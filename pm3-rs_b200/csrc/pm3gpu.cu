@@ -17,6 +17,7 @@
 #include "../../include/pm3gpu.h"
 #include "gradient_kernel.cuh"
 #include "large_scf.cuh"
+#include "panel_coop.cuh"
 #include "guess_mlp.cuh"
 #include "scf_job.cuh"
 
@@ -105,6 +106,7 @@ struct pm3gpu_ctx {
   DevBuf lsel;                // densities of the selected state (P_tot | P_alpha | P_beta)
   double large_ms[16] = {};   // phase times of the last whole-GPU solve (profiling only)
   int precision = PM3GPU_PRECISION_FP64;  // arithmetic of the whole-GPU path's dense products
+  bool coop_panels = true;    // Householder panels as cooperative launches (PM3GPU_COOP_PANELS=0: off)
   std::vector<double> ltrace;  // per-iteration record of the last whole-GPU solve (5 per row)
   // learned initial density: FP32 master parameters, BF16 copy, Adam moments, gradients
   bool has_guess_model = false;
@@ -1062,6 +1064,8 @@ int pm3gpu_context_create(int device, pm3gpu_ctx** out) {
   {
     const char* pe = std::getenv("PM3GPU_PROFILE");
     c->profile = pe && pe[0] && pe[0] != '0';
+    const char* pc = std::getenv("PM3GPU_COOP_PANELS");
+    c->coop_panels = !(pc && pc[0] == '0');
   }
   if ((e = c->elem.ensure(sizeof(c->h_elem))) != cudaSuccess) return bail(e);
   if ((e = c->pairs.ensure(sizeof(PairDev))) != cudaSuccess) return bail(e);

@@ -125,3 +125,39 @@ def test_water60_beyond_one_cta_matches_oracle():
     ref = O.single_point(z, xyz * A2B, p_tol=1e-8, want_density=True)
     _close(got, ref)
     assert np.abs(got["density"] - ref["density"]).max() < 1e-6
+
+
+def _single_point(ctx, z, xyz_bohr, opts):
+    import ctypes
+
+    z = np.ascontiguousarray(z, dtype=np.int32)
+    x = np.ascontiguousarray(xyz_bohr, dtype=np.float64)
+    res, q = _lib.Result(), np.zeros(len(z))
+    mo = np.zeros(O.nao(z))
+    D = ctypes.POINTER(ctypes.c_double)
+    rc = ctx.lib.pm3gpu_single_point(ctx.ptr, len(z), z.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                     x.ctypes.data_as(D), ctypes.byref(opts), ctypes.byref(res), q.ctypes.data_as(D),
+                                     None, mo.ctypes.data_as(D))
+    assert rc == 0, ctx.last_error()
+    return res, q, mo
+
+
+def test_cooperative_and_multi_launch_reductions_agree(monkeypatch):
+    """The Householder panels as one cooperative launch each (default) and as five launches per
+    column (PM3GPU_COOP_PANELS=0) reduce the same matrices: equal results up to summation order."""
+    z, xyz = workloads.water_cluster(34)
+    opts = native.options(p_tol=1e-8)
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("PM3GPU_COOP_PANELS", flag)
+        ctx = _lib.Context(0)
+        try:
+            assert ctx.lib.pm3gpu_set_large_threshold(ctx.ptr, 1) == 0
+            out.append(_single_point(ctx, z, xyz * A2B, opts))
+        finally:
+            ctx.close()
+    (ra, qa, ma), (rb, qb, mb) = out
+    assert ra.converged and rb.converged and ra.iterations == rb.iterations
+    assert abs(ra.heat_of_formation_kcal - rb.heat_of_formation_kcal) < 1e-8
+    assert np.abs(qa - qb).max() < 1e-9
+    assert np.abs(ma - mb).max() < 1e-9

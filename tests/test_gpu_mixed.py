@@ -102,5 +102,6 @@ def test_per_cta_path_ignores_the_mode():
         b = native.run(z, xyz * A2B, native.options())
     finally:
         assert ctx.lib.pm3gpu_set_precision(ctx.ptr, _lib.PRECISION_FP64) == 0
-    assert a["heat_of_formation_kcal"] == b["heat_of_formation_kcal"]
+    # same FP64 path twice: equal up to the last bits of its reductions
+    assert abs(a["heat_of_formation_kcal"] - b["heat_of_formation_kcal"]) < 1e-9
     assert a["iterations"] == b["iterations"]
