@@ -504,6 +504,9 @@ def main():
     ap.add_argument("--epochs", type=int, default=6, help="learned-guess workload: training epochs")
     ap.add_argument("--waters", type=int, default=2000,
                     help="water-2000 workload: number of waters (the cluster uses the first sites of a 13 x 13 x 12 grid)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="batched workloads: skip the calibration that, before timing, measures the launch choices on a "
+                         "1024-molecule sample of the same generator (another seed) and uses the faster")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="water-2000 workload: FP64 throughout, or split-BF16 density and commutator products "
                          "with FP64 closing iterations (reports the heat-of-formation and gradient error against FP64)")
@@ -585,6 +588,18 @@ def main():
     pq = torch.zeros(n_atoms, dtype=torch.float64).pin_memory()
     I32 = ctypes.POINTER(ctypes.c_int32)
     D = ctypes.POINTER(ctypes.c_double)
+    tuning = None
+    if args.autotune:  # calibrate on another sample of the same generator, outside the timed region
+        tmols = molecules(1024, seed=777 + 7919 * rank, workload=args.workload)
+        t_off, t_z, t_xyz = workloads.pack(tmols)
+        t_off, t_z = np.ascontiguousarray(t_off, np.int32), np.ascontiguousarray(t_z, np.int32)
+        t_xyz = np.ascontiguousarray(t_xyz)
+        path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
+                            f"tuning_{args.workload}.json")
+        if lib.pm3gpu_autotune(ctx.ptr, len(tmols), t_off.ctypes.data_as(I32), t_z.ctypes.data_as(I32),
+                               t_xyz.ctypes.data_as(D), ctypes.byref(opts), path.encode()) != 0:
+            raise RuntimeError(ctx.last_error())
+        tuning = json.load(open(path))["batch"]
 
     def run_device():
         rc = lib.pm3gpu_batch_device_inputs(ctx.ptr, n_mol, ctypes.c_void_p(d_off.data_ptr()),
@@ -670,7 +685,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": desc, "molecules_per_step_per_gpu": n_mol, "parallelism": f"dp{world}",
-                   "l2": "flushed between steps (512 MiB write)", "converged_fraction": conv / (n_mol * args.steps * world)},
+                   "l2": "flushed between steps (512 MiB write)", "converged_fraction": conv / (n_mol * args.steps * world),
+                   "tuning": tuning or "built-in launch choice (--no-autotune)"},
         "e2e": {"value": e2e, "unit": "SCF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

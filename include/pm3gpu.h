@@ -208,6 +208,21 @@ int pm3gpu_last_kernel_launches(pm3gpu_ctx* ctx);
  * reference has one CPU path). */
 int pm3gpu_set_large_threshold(pm3gpu_ctx* ctx, int nao);
 
+/* Autotuner (no counterpart in the reference). Measures, on the caller's sample of molecules
+ * (atom_offsets / z / xyz as in pm3gpu_batch), the two launch choices that trade off against each
+ * other, and keeps the faster per size bucket in the context: CTAs per SM of the batched SCF
+ * launch (bucket: the batch's largest basis size) and, for molecules on the whole-GPU path, the
+ * Householder reduction as one cooperative launch per panel or as five launches per column
+ * (bucket: basis size). Both variants of each choice give the same results. When cache_path is
+ * not NULL the table is written there as JSON; pm3gpu_load_tuning reads such a file into another
+ * context. pm3gpu_tuning_choice returns the choice a size would get (kind 0: CTAs per SM for a
+ * batch whose largest basis is `size`; kind 1: 1 = cooperative panels for basis `size`), or -1
+ * when no tuned bucket covers it. */
+int pm3gpu_autotune(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
+                    const double* xyz_bohr, const pm3gpu_options* opts, const char* cache_path);
+int pm3gpu_load_tuning(pm3gpu_ctx* ctx, const char* path);
+int pm3gpu_tuning_choice(pm3gpu_ctx* ctx, int kind, int size);
+
 /* Arithmetic of the whole-GPU path's density and commutator products (no counterpart in the
  * reference, whose products are FP64). PM3GPU_PRECISION_MIXED takes them from split-BF16
  * tensor-core GEMMs (x = hi + lo, products hi*hi + hi*lo + lo*hi, FP32 accumulation) while the

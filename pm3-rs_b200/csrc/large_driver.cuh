@@ -493,6 +493,32 @@ class LargeSolver {
     return eigenvalues(n_, out, none, false);
   }
 
+  // Autotuner: device time of one Householder reduction of H_core with the cooperative panels
+  // (coop = 1) or the multi-launch path (coop = 0); the second of two runs is timed.
+  int time_reduction(int coop, double* ms) {
+    int rc = prepare_reduction();
+    if (rc) return rc;
+    for (DevBuf* b : {&B_.P[0], &B_.P[1], &B_.F, &B_.A}) CUDA_TRY(c_, b->ensure(8 * nn_));
+    c_->force_coop = coop;
+    for (int rep = 0; rep < 2 && rc == PM3GPU_OK; ++rep) {
+      if ((rc = copy(B_.H.as<double>(), work_matrix()))) break;
+      CUDA_TRY(c_, cudaEventRecord(c_->kev[0], c_->stream));
+      rc = run_tridiag(work_matrix());
+      CUDA_TRY(c_, cudaEventRecord(c_->kev[1], c_->stream));
+      CUDA_TRY(c_, cudaEventSynchronize(c_->kev[1]));
+      float t = 0.0f;
+      CUDA_TRY(c_, cudaEventElapsedTime(&t, c_->kev[0], c_->kev[1]));
+      *ms = t;
+      if (rc == PM3GPU_OK && coop_grid() > 0) {
+        large::GridSync gsh{};
+        CUDA_TRY(c_, cudaMemcpy(&gsh, B_.gsync.p, sizeof(gsh), cudaMemcpyDeviceToHost));
+        if (gsh.err) rc = fail(c_, PM3GPU_CUDA_ERROR, "Householder panel: a grid barrier wait ran out");
+      }
+    }
+    c_->force_coop = -1;
+    return rc;
+  }
+
  private:
   pm3gpu_ctx* c_;
   LargeBufs& B_;
@@ -675,6 +701,7 @@ class LargeSolver {
   // each block owns one stripe).
   int coop_grid() {
     if (!c_->coop_panels) return 0;
+    if ((c_->force_coop >= 0 ? c_->force_coop : tune_lookup(c_->tune_large, n_, 1)) == 0) return 0;
     if (coop_g_ < 0) {
       int occ = 0, coop = 0;
       if (cudaFuncSetAttribute(large::panel_coop_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -859,19 +886,9 @@ class LargeSolver {
                  std::vector<double>* tri) {
     const int n = n_;
     const size_t K = (size_t)std::max(kvec, 1);
-    for (DevBuf* b : {&B_.d, &B_.e, &B_.tau, &B_.y, &B_.wtmp, &B_.vcol}) CUDA_TRY(c_, b->ensure(8 * (size_t)n));
-    CUDA_TRY(c_, B_.V.ensure(8 * (size_t)n * large::kPanel));
-    CUDA_TRY(c_, B_.Wp.ensure(8 * (size_t)n * large::kPanel));
-    CUDA_TRY(c_, B_.ps.ensure(8 * 64 * (size_t)large::kRedBlocks));
-    CUDA_TRY(c_, B_.s64.ensure(8 * 64));
     {
-      const long long nt = (n + large::kTile - 1) / large::kTile;  // absolute stripes (covers the trailing ones)
-      CUDA_TRY(c_, B_.tp.ensure(8 * (size_t)(2 * large::kTile) * (size_t)std::max<long long>(nt * (nt + 1) / 2, 1)));
-      if (!B_.ctr.p) {
-        CUDA_TRY(c_, B_.ctr.ensure(256));
-        CUDA_TRY(c_, cudaMemsetAsync(B_.ctr.p, 0, 256, c_->stream));
-      }
-      CUDA_TRY(c_, B_.refl.ensure(256));
+      const int rc = prepare_reduction();
+      if (rc) return rc;
     }
     double* d = B_.d.as<double>();
     double* e = B_.e.as<double>();
@@ -970,6 +987,24 @@ class LargeSolver {
       X = B_.X.as<double>();
     }
     tick(kLgOrth);
+    return PM3GPU_OK;
+  }
+
+  // Work buffers of the Householder reduction for this matrix size.
+  int prepare_reduction() {
+    const int n = n_;
+    for (DevBuf* b : {&B_.d, &B_.e, &B_.tau, &B_.y, &B_.wtmp, &B_.vcol}) CUDA_TRY(c_, b->ensure(8 * (size_t)n));
+    CUDA_TRY(c_, B_.V.ensure(8 * (size_t)n * large::kPanel));
+    CUDA_TRY(c_, B_.Wp.ensure(8 * (size_t)n * large::kPanel));
+    CUDA_TRY(c_, B_.ps.ensure(8 * 64 * (size_t)large::kRedBlocks));
+    CUDA_TRY(c_, B_.s64.ensure(8 * 64));
+    const long long nt = (n + large::kTile - 1) / large::kTile;  // absolute stripes (covers the trailing ones)
+    CUDA_TRY(c_, B_.tp.ensure(8 * (size_t)(2 * large::kTile) * (size_t)std::max<long long>(nt * (nt + 1) / 2, 1)));
+    if (!B_.ctr.p) {
+      CUDA_TRY(c_, B_.ctr.ensure(256));
+      CUDA_TRY(c_, cudaMemsetAsync(B_.ctr.p, 0, 256, c_->stream));
+    }
+    CUDA_TRY(c_, B_.refl.ensure(256));
     return PM3GPU_OK;
   }
 

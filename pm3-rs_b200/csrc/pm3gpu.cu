@@ -105,6 +105,14 @@ struct pm3gpu_ctx {
   LargeBufs* lbuf = nullptr;
   DevBuf lsel;                // densities of the selected state (P_tot | P_alpha | P_beta)
   double large_ms[16] = {};   // phase times of the last whole-GPU solve (profiling only)
+  // autotuner: measured choices per size bucket (autotune.cuh); forced values while it measures
+  struct Tune {
+    int le;      // bucket: largest basis size it covers
+    int choice;  // batch: CTAs per SM (1 or 2); large: 1 cooperative panels, 0 multi-launch
+    double ms_a, ms_b;  // measured times of the two candidates (batch: 1 and 2 CTAs; large: coop, multi)
+  };
+  std::vector<Tune> tune_batch, tune_large;
+  int force_ctas = 0, force_coop = -1;
   int precision = PM3GPU_PRECISION_FP64;  // arithmetic of the whole-GPU path's dense products
   bool coop_panels = true;    // Householder panels as cooperative launches (PM3GPU_COOP_PANELS=0: off)
   std::vector<double> ltrace;  // per-iteration record of the last whole-GPU solve (5 per row)
@@ -116,6 +124,13 @@ struct pm3gpu_ctx {
 };
 
 namespace {
+
+// Choice recorded for the smallest tuned bucket that covers `size`, else `dflt`.
+int tune_lookup(const std::vector<pm3gpu_ctx::Tune>& t, int size, int dflt) {
+  for (const pm3gpu_ctx::Tune& e : t)
+    if (size <= e.le) return e.choice;
+  return dflt;
+}
 
 int fail(pm3gpu_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
@@ -254,7 +269,10 @@ long long pair_table_doubles(const pm3gpu_ctx* c, const int32_t* z, int natom) {
 // Shared-memory carve-up of one launch. The packed eigen input lives in shared memory for
 // bases up to `nsm` (global memory above). When `naos` is given, the layout is shrunk to let
 // two CTAs share an SM as long as at least 90% of the launch's jobs still fit in shared memory.
-SmemLayout make_layout(int amax, int nmax, int optin, int smem_per_sm = 0, const std::vector<int>* naos = nullptr) {
+// ctas: 0 = choose (two CTAs per SM when at least 90% of the batch keeps its packed eigen input
+// in the smaller layout), 1 or 2 = the autotuner's measured choice.
+SmemLayout make_layout(int amax, int nmax, int optin, int smem_per_sm = 0, const std::vector<int>* naos = nullptr,
+                       int ctas = 0) {
   SmemLayout L{};
   L.amax = amax;
   auto align = [](int b) { return (b + 15) & ~15; };
@@ -274,13 +292,17 @@ SmemLayout make_layout(int amax, int nmax, int optin, int smem_per_sm = 0, const
     return nsm;
   };
   int nsm = fit(optin);
-  if (smem_per_sm > 0 && naos && !naos->empty()) {
+  if (smem_per_sm > 0 && ctas != 1 && (ctas == 2 || (naos && !naos->empty()))) {
     const int budget2 = smem_per_sm / 2 - 1024 - 512;  // per-CTA reservation and static shared memory
     const int nsm2 = fit(budget2);
     if (nsm2 < nsm && off + fixed_union * 8 <= budget2) {
-      size_t inside = 0;
-      for (int v : *naos) inside += v <= nsm2;
-      if (inside * 10 >= naos->size() * 9) nsm = nsm2;
+      if (ctas == 2) {
+        nsm = nsm2;
+      } else {
+        size_t inside = 0;
+        for (int v : *naos) inside += v <= nsm2;
+        if (inside * 10 >= naos->size() * 9) nsm = nsm2;
+      }
     }
   }
   L.nsm = nsm;
@@ -339,7 +361,8 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
       wcap = std::max(wcap, pair_table_doubles(c, zs.data() + j.atom0, j.natom));
     }
   for (const JobDesc& j : jobs) naos.push_back(j.nao);
-  const SmemLayout L = make_layout(amax, nmax, c->smem_optin, c->smem_per_sm, &naos);
+  const int ctas = c->force_ctas ? c->force_ctas : tune_lookup(c->tune_batch, nmax, 0);
+  const SmemLayout L = make_layout(amax, nmax, c->smem_optin, c->smem_per_sm, &naos, ctas);
   CUDA_TRY(c, cudaFuncSetAttribute(scf_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes));
   int per_sm = 0;
   CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scf_batch_kernel, kThreads, L.bytes));
@@ -998,6 +1021,8 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
   return PM3GPU_OK;
 }
 
+#include "autotune.cuh"
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -1492,6 +1517,36 @@ int pm3gpu_guess_train(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int3
   }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return PM3GPU_OK;
+}
+
+int pm3gpu_autotune(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t* z, const double* xyz,
+                    const pm3gpu_options* opts, const char* cache_path) {
+  if (!c || n_mol < 1 || !offs || !z || !xyz) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  c->err.clear();
+  for (int m = 0; m < n_mol; ++m)
+    if (offs[m + 1] < offs[m]) return fail(c, PM3GPU_INVALID_INPUT, "atom offsets must not decrease");
+  pm3gpu_options d;
+  pm3gpu_default_options(&d);
+  int rc = tune_batch_part(c, n_mol, offs, z, xyz, opts ? opts : &d);
+  if (rc == PM3GPU_OK) rc = tune_large_part(c, n_mol, offs, z, xyz);
+  if (rc == PM3GPU_OK && cache_path) rc = write_tuning(c, cache_path);
+  return rc;
+}
+
+int pm3gpu_load_tuning(pm3gpu_ctx* c, const char* path) {
+  if (!c || !path) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  return read_tuning(c, path);
+}
+
+int pm3gpu_tuning_choice(pm3gpu_ctx* c, int kind, int size) {
+  if (!c) return -1;
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (kind == 0) return tune_lookup(c->tune_batch, size, -1);
+  if (kind == 1) return tune_lookup(c->tune_large, size, -1);
+  return -1;
 }
 
 int pm3gpu_set_precision(pm3gpu_ctx* c, int mode) {

@@ -73,7 +73,8 @@ EXPORTS = [
     "pm3gpu_batch_device_inputs", "pm3gpu_core_hamiltonian", "pm3gpu_fock", "pm3gpu_last_timings",
     "pm3gpu_last_kernel_launches", "pm3gpu_last_transfer_bytes", "pm3gpu_last_phase_cycles",
     "pm3gpu_single_point_noalloc", "pm3gpu_set_large_threshold", "pm3gpu_last_large_phase_ms",
-    "pm3gpu_set_precision", "pm3gpu_last_large_trace",
+    "pm3gpu_set_precision", "pm3gpu_last_large_trace", "pm3gpu_autotune", "pm3gpu_load_tuning",
+    "pm3gpu_tuning_choice",
     "pm3gpu_guess_train", "pm3gpu_guess_set_params", "pm3gpu_guess_get_params", "pm3gpu_guess_predict",
 ]
 
@@ -120,6 +121,9 @@ def load() -> ctypes.CDLL:
     L.pm3gpu_set_large_threshold.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.pm3gpu_last_large_phase_ms.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     L.pm3gpu_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.pm3gpu_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, ctypes.POINTER(Options), ctypes.c_char_p]
+    L.pm3gpu_load_tuning.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    L.pm3gpu_tuning_choice.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.pm3gpu_last_large_trace.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     _F = ctypes.POINTER(ctypes.c_float)
     L.pm3gpu_guess_train.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, ctypes.POINTER(Options), ctypes.c_int,
