@@ -187,6 +187,9 @@ class LargeSolver {
     large::core_pairs_kernel<<<gp, large::kBlock, 0, c_->stream>>>(m_, B_.H.as<double>(), B_.W.as<double>(),
                                                                   B_.hacc.as<double>(), B_.part.as<double>());
     ++c_->launches;
+    large::core_atoms_kernel<<<(N_ + large::kBlock / 32 - 1) / (large::kBlock / 32), large::kBlock, 0, c_->stream>>>(
+        m_, B_.hacc.as<double>());
+    ++c_->launches;
     large::finish_sum<<<1, large::kBlock, 0, c_->stream>>>(B_.part.as<double>(), gp, B_.scal.as<double>());
     large::core_diag_kernel<<<grid_for((size_t)N_ * 16), large::kBlock, 0, c_->stream>>>(m_, B_.hacc.as<double>(),
                                                                                         B_.H.as<double>());
@@ -568,6 +571,10 @@ class LargeSolver {
     large::pack_density_kernel<<<gN, large::kBlock, 0, c_->stream>>>(m_, Pt, B_.dpk.as<double>(), B_.jacc.as<double>());
     const long long np = (long long)N_ * (N_ - 1) / 2;
     const int gp = grid_for((size_t)std::max<long long>(np, 1));
+    const int ga = (N_ + large::kBlock / 32 - 1) / (large::kBlock / 32);  // one warp per atom
+    large::coulomb_atoms_kernel<<<ga, large::kBlock, 0, c_->stream>>>(m_, B_.W.as<double>(), B_.dpk.as<double>(),
+                                                                      B_.jacc.as<double>());
+    ++c_->launches;
     if (Pb)
       large::fock_pairs_kernel<true><<<gp, large::kBlock, 0, c_->stream>>>(
           m_, B_.W.as<double>(), B_.H.as<double>(), B_.dpk.as<double>(), B_.jacc.as<double>(), Pt, Pa, Pb, F, G);

@@ -113,9 +113,36 @@ __global__ void __launch_bounds__(kBlock) core_pairs_kernel(Mol m, double* H, do
     const int a = (hu || !hv) ? u : v, b = a == u ? v : u;
     double* w = const_cast<double*>(pair_block(m, W, u, v));
     ecc += core_pair(m.elem[m.z[a]], m.elem[m.z[b]], eu, ev, *m.pairs, m.xyz + 3 * (size_t)a, m.xyz + 3 * (size_t)b,
-                     m.ao[a], m.ao[b], (size_t)m.n, hacc + 10 * (size_t)a, hacc + 10 * (size_t)b, w, H);
+                     m.ao[a], m.ao[b], (size_t)m.n, nullptr, nullptr, w, H);
   }
+  (void)hacc;
   block_partial(ecc, partial);
+}
+// Electron-core attraction blocks summed per atom (hamiltonian.rs:191-344): one warp per atom x,
+// lanes over the partners y in a fixed order, so H_core does not depend on timing.
+__global__ void __launch_bounds__(kBlock) core_atoms_kernel(Mol m, double* hacc) {
+  const int lane = threadIdx.x & 31, x = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+  if (x >= m.N) return;  // whole warps
+  const ElemDev& ex = m.elem[m.z[x]];
+  const double* px = m.xyz + 3 * (size_t)x;
+  double acc[10] = {};
+  for (int y = lane; y < m.N; y += 32) {
+    if (y == x) continue;
+    const double* py = m.xyz + 3 * (size_t)y;
+    const double d[3] = {py[0] - px[0], py[1] - px[1], py[2] - px[2]};
+    const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    const double dv[3] = {d[0] / r * r, d[1] / r * r, d[2] / r * r};  // as core_pair forms it
+    double blk[10];
+    core_attraction(ex, m.elem[m.z[y]], dv, blk);
+#pragma unroll
+    for (int k = 0; k < 10; ++k)
+      if (k < (ex.norb == 4 ? 10 : 1)) acc[k] += blk[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 10; ++k) {
+    const double t = warp_sum(acc[k]);
+    if (lane == 0) hacc[10 * (size_t)x + k] = t;
+  }
 }
 // atom-diagonal blocks of H: U + the summed electron-core attractions
 __global__ void __launch_bounds__(kBlock) core_diag_kernel(Mol m, const double* hacc, double* H) {
@@ -164,6 +191,41 @@ __global__ void __launch_bounds__(kBlock) pack_density_kernel(Mol m, const doubl
     dpk[k] = v;
   }
 }
+// Two-centre Coulomb sums of the Fock build, J_x[p] = sum_{y != x} sum_q (x p | y q) Pbar_y[q]
+// (fock.rs:106-159), one warp per atom x, lanes over the partners in a fixed order (the pair
+// kernel leaves them out), so the Fock matrix does not depend on timing. Pair blocks are stored
+// in (a, b) orientation, a the atom with more orbitals (the first one on a tie).
+__global__ void __launch_bounds__(kBlock) coulomb_atoms_kernel(Mol m, const double* W, const double* dpk, double* jacc) {
+  const int lane = threadIdx.x & 31, x = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+  if (x >= m.N) return;  // whole warps
+  const int sx = m.sprow[x + 1] - m.sprow[x];
+  double acc[10] = {};
+  for (int y = lane; y < m.N; y += 32) {
+    if (y == x) continue;
+    const int sy = m.sprow[y + 1] - m.sprow[y];
+    const int u = min(x, y), v = max(x, y);
+    const int su = u == x ? sx : sy, sv = u == x ? sy : sx;
+    const bool x_rows = ((su == 10 || sv != 10) ? u : v) == x;  // x is the block's row atom
+    const double* w = pair_block(m, W, u, v);
+    const double* dy = dpk + 10 * (size_t)y;
+#pragma unroll
+    for (int p = 0; p < 10; ++p) {
+      if (p >= sx) break;
+      double t = 0.0;
+#pragma unroll
+      for (int q = 0; q < 10; ++q) {
+        if (q >= sy) break;
+        t = fma(dy[q], x_rows ? w[p * sy + q] : w[q * sx + p], t);
+      }
+      acc[p] += t;
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 10; ++p) {
+    const double t = warp_sum(acc[p]);
+    if (lane == 0 && p < sx) jacc[10 * (size_t)x + p] = t;
+  }
+}
 template <bool UHF>
 __global__ void __launch_bounds__(kBlock) fock_pairs_kernel(Mol m, const double* W, const double* H, const double* dpk,
                                                             double* jacc, const double* Pt, const double* Pa,
@@ -177,9 +239,9 @@ __global__ void __launch_bounds__(kBlock) fock_pairs_kernel(Mol m, const double*
     const int a = (hu || !hv) ? u : v, b = a == u ? v : u;
     const double* w = pair_block(m, W, u, v);
     const int oa = m.ao[a], ob = m.ao[b];
-    if (hu && hv) fock_pair<4, 4, UHF>(m.n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
-    else if (hu || hv) fock_pair<4, 1, UHF>(m.n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
-    else fock_pair<1, 1, UHF>(m.n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+    if (hu && hv) fock_pair<4, 4, UHF, false>(m.n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+    else if (hu || hv) fock_pair<4, 1, UHF, false>(m.n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+    else fock_pair<1, 1, UHF, false>(m.n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
   }
 }
 // atom-diagonal blocks: H + one-centre J - K + two-centre J

@@ -207,11 +207,13 @@ __device__ __forceinline__ double core_pair(const ElemDev& ea, const ElemDev& eb
   const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
   const double dv[3] = {d[0] / r * r, d[1] / r * r, d[2] / r * r};
   const double mdv[3] = {-dv[0], -dv[1], -dv[2]};
-  double blk[10];
-  core_attraction(ea, eb, dv, blk);
-  for (int k = 0; k < (ea.norb == 4 ? 10 : 1); ++k) atomicAdd(&hacc_a[k], blk[k]);
-  core_attraction(eb, ea, mdv, blk);
-  for (int k = 0; k < (eb.norb == 4 ? 10 : 1); ++k) atomicAdd(&hacc_b[k], blk[k]);
+  if (hacc_a) {  // null: the caller adds the electron-core blocks per atom itself
+    double blk[10];
+    core_attraction(ea, eb, dv, blk);
+    for (int k = 0; k < (ea.norb == 4 ? 10 : 1); ++k) atomicAdd(&hacc_a[k], blk[k]);
+    core_attraction(eb, ea, mdv, blk);
+    for (int k = 0; k < (eb.norb == 4 ? 10 : 1); ++k) atomicAdd(&hacc_b[k], blk[k]);
+  }
   const double ir = 1.0 / r;
   double R[9];
   frame(-(dv[0] * ir), -(dv[1] * ir), -(dv[2] * ir), R);
@@ -285,12 +287,14 @@ __device__ double build_core(Ctx& c) {
 // accumulators and the exchange block F_ab = H_ab - K_ab, written to both triangles. NA / NB are
 // the orbital counts of atom a (the heavier one) and b, so every loop has a fixed trip count and
 // every array stays in registers. W is the pair's (PA x PB) row-major integral block.
-template <int NA, int NB, bool UHF>
+// kJ = false leaves out the two-centre Coulomb sums into jacc (the whole-GPU path adds them per
+// atom in a fixed order instead of with atomics).
+template <int NA, int NB, bool UHF, bool kJ = true>
 __device__ __forceinline__ void fock_pair(int n, int a, int b, int oa, int ob, const double* __restrict__ dpk,
                                           double* jacc, const double* __restrict__ H, const double* __restrict__ w,
                                           const double* Pt, const double* Pa, const double* Pb, double* F, double* G) {
   constexpr int PA = NA == 4 ? 10 : 1, PB = NB == 4 ? 10 : 1;
-  {  // Coulomb: J_a[p] += sum_q W[p][q] Pb_q, J_b[q] += sum_p Pa_p W[p][q]
+  if (kJ) {  // Coulomb: J_a[p] += sum_q W[p][q] Pb_q, J_b[q] += sum_p Pa_p W[p][q]
     double db[PB], jb[PB];
 #pragma unroll
     for (int q = 0; q < PB; ++q) {

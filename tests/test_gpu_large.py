@@ -161,3 +161,15 @@ def test_cooperative_and_multi_launch_reductions_agree(monkeypatch):
     assert abs(ra.heat_of_formation_kcal - rb.heat_of_formation_kcal) < 1e-8
     assert np.abs(qa - qb).max() < 1e-9
     assert np.abs(ma - mb).max() < 1e-9
+
+
+def test_whole_gpu_path_is_reproducible(whole_gpu):
+    """Every sum of the whole-GPU path runs in a fixed order (per-atom Coulomb and electron-core
+    sums, fixed-order grid reductions, deterministic GEMMs): two solves agree to the last bit."""
+    z, xyz = workloads.water_cluster(34)
+    opts = native.options(p_tol=1e-8)
+    a = native.run(z, xyz * A2B, opts, want_density=True)
+    b = native.run(z, xyz * A2B, opts, want_density=True)
+    assert a["heat_of_formation_kcal"] == b["heat_of_formation_kcal"]
+    assert a["iterations"] == b["iterations"]
+    assert np.array_equal(a["density"], b["density"])
