@@ -268,7 +268,7 @@ class LargeSolver {
     // Mixed mode: the commutator and the density come from split-BF16 products until the density
     // settles (kMixedSwitch) or stops improving, then FP64 iterations close the SCF; only an FP64
     // iteration can satisfy the convergence test, so the result is the FP64 fixed point.
-    bool lowp = c_->precision == PM3GPU_PRECISION_MIXED;
+    bool lowp = c_->precision == PM3GPU_PRECISION_MIXED, prev_lowp = false;
     ++passes_;
     for (int iter = 0; iter < J.max_scf; ++iter) {
       iterations = iter + 1;
@@ -281,6 +281,24 @@ class LargeSolver {
       double* Fa = B_.F.as<double>();
       double* Fb = uhf ? B_.G.as<double>() : nullptr;
       double *Ea = nullptr, *Eb = nullptr, *Dh = nullptr;
+      // First FP64 iteration after split-BF16 ones: the newest history entry's commutator is a
+      // split-BF16 product. Its density (the previous iteration's input) is still in the other
+      // buffer, so it is redone in FP64 and its Gram row refreshed before the history is used.
+      if (prev_lowp && !lowp_iter && J.accel != 0 && len > 0 && (!uhf || J.damping == 0.0)) {
+        const int l = len - 1;
+        double* bl = slot(head, l, depth, slot_mats);
+        int rc = commutator(bl, B_.P[1 - cur].as<double>(), bl + nn_);
+        if (rc) return rc;
+        if (uhf && (rc = commutator(bl + 2 * nn_, B_.Q[1 - cur].as<double>(), bl + 3 * nn_))) return rc;
+        for (int k2 = 0; k2 < len; ++k2) {
+          double* bk = slot(head, k2, depth, slot_mats);
+          double v;
+          if ((rc = dot(bk + nn_, bl + nn_, uhf ? bk + 3 * nn_ : nullptr, uhf ? bl + 3 * nn_ : nullptr, &v))) return rc;
+          bg[k2 * kMaxDepth + l] = v;
+          bg[l * kMaxDepth + k2] = v;
+        }
+      }
+      prev_lowp = lowp_iter;
       if (J.accel != 0) {
         if (len == depth) {
           for (int i = 0; i + 1 < len; ++i)
