@@ -8,10 +8,13 @@ e_tol 1e-8 eV, p_tol 1e-7, stability search on), every molecule to convergence. 
 converged single points per second over the whole job. Under torchrun every rank solves its
 own 4096 molecules (seed offset by rank): weak scaling, no data-path collective.
 
-`value`: inputs (atom numbers and coordinates) already resident in HBM, CUDA-event time of the
-call on the stream the library launches on. `e2e`: the same through the host C ABI
-(pm3gpu_batch) from pinned host buffers, host<->device copies inside the timed region.
-L2 is flushed (a 512 MiB write) between timed steps, outside the timed region.
+`value`: inputs (atom numbers and coordinates) already resident in HBM, CUDA-event time on the
+device. `e2e`: the same through the host C ABI (pm3gpu_batch) from pinned host buffers,
+host<->device copies inside the timed region. By default three batches are in flight (three
+contexts, each with its own stream and host thread) and the device time spans all K steps; L2 is
+flushed (a 512 MiB write) before them and the per-CTA workspaces exceed L2. With `--inflight 1`
+each step is timed alone with a flush between steps. Before timing, the autotuner calibrates the
+launch choice on another sample of the same generator (`--no-autotune` skips it).
 `--impl reference` times the reference algorithm's CPU implementation (the C++ oracle that
 restates pm3-rs, linked to SciPy's OpenBLAS) on the host cores instead.
 """
@@ -92,6 +95,27 @@ def workload_spec(args):
     if args.workload == "radicals-2048":
         return RADICALS, {"multiplicity": 2, "want_gradient": True}, {"multiplicity": 2}, True, 2048
     return WORKLOAD, {}, {}, False, 4096
+
+
+# --------------------------------------------------------------------------- ranks
+def shard_seed(rank, base=1234):
+    """Seed of one rank's batch: every rank solves its own molecules (weak scaling; the batch
+    shards by molecules, so there is no data-path collective)."""
+    return base + 7919 * rank
+
+
+def reduce_over_ranks(tot, e_tot, conv, e_conv, dist, device):
+    """Whole-job numbers: the slowest rank's device times (ms) and the converged counts summed
+    over ranks. `dist` is torch.distributed or None for one process."""
+    if not dist:
+        return tot, e_tot, conv, e_conv
+    import torch
+
+    t_max = torch.tensor([tot, e_tot], dtype=torch.float64, device=device)
+    c_sum = torch.tensor([float(conv), float(e_conv)], dtype=torch.float64, device=device)
+    dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    dist.all_reduce(c_sum, op=dist.ReduceOp.SUM)
+    return float(t_max[0]), float(t_max[1]), int(c_sum[0]), int(c_sum[1])
 
 
 # --------------------------------------------------------------------------- GPU helpers
@@ -567,7 +591,7 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
 
-    mols = molecules(args.n_mol, seed=1234 + 7919 * rank, workload=args.workload)
+    mols = molecules(args.n_mol, seed=shard_seed(rank), workload=args.workload)
     from pm3_rs import workloads
 
     offs, z, xyz = workloads.pack(mols)
@@ -593,7 +617,7 @@ def main():
     D = ctypes.POINTER(ctypes.c_double)
     tuning = None
     if args.autotune:  # calibrate on another sample of the same generator, outside the timed region
-        tmols = molecules(256 if args.workload == "radicals-2048" else 1024, seed=777 + 7919 * rank,
+        tmols = molecules(256 if args.workload == "radicals-2048" else 1024, seed=shard_seed(rank, 777),
                           workload=args.workload)
         t_off, t_z, t_xyz = workloads.pack(tmols)
         t_off, t_z = np.ascontiguousarray(t_off, np.int32), np.ascontiguousarray(t_z, np.int32)
@@ -767,14 +791,7 @@ def main():
         h2d, d2h = xfer
     tot = sum(ms)
     e_tot = sum(e_ms)
-    stats = torch.tensor([tot, e_tot, float(conv), float(e_conv)], dtype=torch.float64, device=dev)
-    if dist:
-        t_max = stats[:2].clone()
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-        c_sum = stats[2:].clone()
-        dist.all_reduce(c_sum, op=dist.ReduceOp.SUM)
-        tot, e_tot = float(t_max[0]), float(t_max[1])
-        conv, e_conv = int(c_sum[0]), int(c_sum[1])
+    tot, e_tot, conv, e_conv = reduce_over_ranks(tot, e_tot, conv, e_conv, dist, dev)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
