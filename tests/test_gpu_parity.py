@@ -231,3 +231,30 @@ def test_edge_cases_and_errors():
     res = native.batch(np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros((0, 3)))
     assert len(res.status) == 0
     assert lib.pm3gpu_last_kernel_launches(_lib.default_context().ptr) == 0
+
+
+def test_uhf_gradient_matches_central_differences_of_gpu_energies():
+    """Radical gradient (UHF) against central differences of the GPU's own total energy, step
+    1e-4 A as the radicals configuration asks; all 6N displaced geometries go through one batch.
+    Tight SCF thresholds and no stability search, so every displaced solve stays on the same state.
+    The bar, 1e-5 eV/A, sits between the O(h^2) truncation (~1e-8) and the reference's own
+    finite-difference bound (5e-5 eV/Bohr, gradient.rs:733-759)."""
+    z, xyz = workloads.radical(10, 7)
+    z = np.asarray(z, dtype=np.int32)
+    xyz = np.asarray(xyz, dtype=np.float64)  # Angstrom
+    tight = dict(multiplicity=2, e_tol=1e-12, p_tol=1e-11, max_scf=1000, stability=0)
+    g = native.run(z, xyz * A2B, native.options(**tight), want_gradient=True)["gradient"]  # eV/Bohr
+    h = 1e-4
+    mols = []
+    for a in range(len(z)):
+        for k in range(3):
+            for sgn in (1.0, -1.0):
+                x = xyz.copy()
+                x[a, k] += sgn * h
+                mols.append((z, x))
+    offs, zz, xx = workloads.pack(mols)
+    res = native.batch(offs, zz, xx * A2B, native.options(**tight))
+    assert np.all(res.status == 0) and np.all(res.unrestricted)
+    e = res.total_ev.reshape(len(z), 3, 2)
+    fd = (e[:, :, 0] - e[:, :, 1]) / (2 * h)  # eV/A
+    assert np.abs(fd - g.reshape(-1, 3) * A2B).max() < 1e-5
