@@ -5,8 +5,10 @@
 // Matrices are row-major n x n FP64. cuBLAS sees a row-major matrix as its column-major
 // transpose; every call below is written in that view (comments give the row-major product).
 //
-// Eigensolver for large n: blocked Householder tridiagonalisation (panel kernels + two DGEMM
-// trailing updates per panel), division-free Sturm multisection for the lowest n_occ + 1
+// Eigensolver for large n: blocked Householder tridiagonalisation (one cooperative launch per
+// panel + one rank-64 DGEMM trailing update; five launches per column replayed from a CUDA graph
+// where a cooperative launch cannot hold the matrix), division-free Sturm multisection for the
+// lowest n_occ + 1
 // eigenvalues (warm-started from the previous iteration), twisted-factorisation eigenvectors of
 // the tridiagonal (one thread per vector), compact-WY back-transformation (DGEMM), then
 // Newton-Schulz steps X <- X (3I - X^T X)/2 until the occupied vectors are orthonormal to
@@ -181,11 +183,10 @@ class LargeSolver {
     CUDA_TRY(c_, B_.part.ensure(8 * (size_t)large::kRedBlocks));
     CUDA_TRY(c_, B_.part2.ensure(8 * (size_t)large::kRedBlocks));
     CUDA_TRY(c_, B_.scal.ensure(8 * 128));
-    CUDA_TRY(c_, cudaMemsetAsync(B_.hacc.p, 0, 80 * (size_t)N_, c_->stream));
     const long long np = (long long)N_ * (N_ - 1) / 2;
     const int gp = grid_for((size_t)std::max<long long>(np, 1));
     large::core_pairs_kernel<<<gp, large::kBlock, 0, c_->stream>>>(m_, B_.H.as<double>(), B_.W.as<double>(),
-                                                                  B_.hacc.as<double>(), B_.part.as<double>());
+                                                                  B_.part.as<double>());
     ++c_->launches;
     large::core_atoms_kernel<<<(N_ + large::kBlock / 32 - 1) / (large::kBlock / 32), large::kBlock, 0, c_->stream>>>(
         m_, B_.hacc.as<double>());

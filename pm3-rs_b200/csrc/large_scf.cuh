@@ -1,8 +1,10 @@
 // Whole-GPU kernels for one large molecule (basis beyond one CTA): the same run_pm3 SCF as the
 // per-CTA path, with every step spread over the device. Pair integrals, H_core and the Fock
-// build run one thread per atom pair (src/hamiltonian.rs:191-344, src/fock.rs:93-332); the dense
-// products (commutator, density, the eigensolver's trailing updates and back-transformation) are
-// cuBLAS DGEMMs issued by the host driver; the Householder panel, the Sturm multisection, the
+// build run one thread per atom pair (src/hamiltonian.rs:191-344, src/fock.rs:93-332), the sums
+// into each atom's diagonal block one warp per atom in a fixed order (no atomics: repeated solves
+// agree bit for bit); the dense products (commutator, density, the eigensolver's trailing updates
+// and back-transformation) are cuBLAS DGEMMs issued by the host driver; the multi-launch
+// Householder panel (the cooperative one is panel_coop.cuh), the Sturm multisection, the
 // twisted-factorisation eigenvectors, the compact-WY factors and all reductions are here.
 #pragma once
 #include <cuda_bf16.h>
@@ -100,8 +102,9 @@ __global__ void __launch_bounds__(kBlock) absdiff_max_kernel(const double* __res
 }
 
 // ---------------------------------------------------------------- H_core and the pair table
-__global__ void __launch_bounds__(kBlock) core_pairs_kernel(Mol m, double* H, double* W, double* hacc,
-                                                            double* partial) {
+// Pair table W, the resonance blocks of H and the core-core energy, one thread per pair; the
+// electron-core blocks are summed per atom by core_atoms_kernel.
+__global__ void __launch_bounds__(kBlock) core_pairs_kernel(Mol m, double* H, double* W, double* partial) {
   const long long np = pair_count(m.N);
   double ecc = 0.0;
   for (long long t = blockIdx.x * (long long)kBlock + threadIdx.x; t < np; t += (long long)gridDim.x * kBlock) {
@@ -115,7 +118,6 @@ __global__ void __launch_bounds__(kBlock) core_pairs_kernel(Mol m, double* H, do
     ecc += core_pair(m.elem[m.z[a]], m.elem[m.z[b]], eu, ev, *m.pairs, m.xyz + 3 * (size_t)a, m.xyz + 3 * (size_t)b,
                      m.ao[a], m.ao[b], (size_t)m.n, nullptr, nullptr, w, H);
   }
-  (void)hacc;
   block_partial(ecc, partial);
 }
 // Electron-core attraction blocks summed per atom (hamiltonian.rs:191-344): one warp per atom x,
