@@ -169,6 +169,51 @@ __global__ void __launch_bounds__(kBlock, 2)
   for (int j = 0; j < b; ++j) {
     const int i = p + j, s = i + 1;
     double* rowi = A + (size_t)i * n;
+    // GEMV tiles of this column (step B): which tiles does not depend on the reflector, and A22 is
+    // not written during the panel, so the first two copies go out before barrier 1.
+    const int I0 = s / kTile;  // first stripe that meets the trailing block
+    const int ntr = nts - I0;
+    const long long ntiles = (long long)ntr * (ntr + 1) / 2;
+    const long long t0 = ntiles * c / G, t1 = ntiles * (c + 1) / G;
+    const int my = (int)(t1 - t0);
+    int Ii = 0, Ji = 0;  // tile coordinates (relative to I0) of the next copy
+    {
+      int Ir = (int)((sqrt(8.0 * (double)t0 + 1.0) - 1.0) * 0.5);
+      while ((long long)(Ir + 1) * (Ir + 2) / 2 <= t0) ++Ir;
+      while ((long long)Ir * (Ir + 1) / 2 > t0) --Ir;
+      Ii = Ir;
+      Ji = (int)(t0 - (long long)Ir * (Ir + 1) / 2);
+    }
+    int Iv = Ii, Jv = Ji, Ic = Ii, Jc = Ji;  // next v fetch, next reduction
+    auto step = [](int& I, int& J) {
+      if (++J > I) {
+        ++I;
+        J = 0;
+      }
+    };
+    auto issue = [&](int k) {
+      if (k < my) {
+        double* T = tiles + (size_t)(k % kStages) * kTile * kTile;
+        const int rb = (I0 + Ii) * kTile, cb = (I0 + Ji) * kTile;
+        if (kEven) {
+#pragma unroll
+          for (int q = 0; q < kTile * kTile / 2 / kBlock; ++q) {
+            const int el = threadIdx.x + kBlock * q, r = rb + (el >> 5), col = cb + 2 * (el & 31);
+            const bool ok = r < n && col < n;
+            cp_async16(T + 2 * el, ok ? A + (size_t)r * n + col : A, ok);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < kTile * kTile / kBlock; ++q) {
+            const int el = threadIdx.x + kBlock * q, r = rb + (el >> 6), col = cb + (el & 63);
+            const bool ok = r < n && col < n;
+            cp_async8(T + el, ok ? A + (size_t)r * n + col : A, ok);
+          }
+        }
+        step(Ii, Ji);
+      }
+      cp_async_commit();  // one group per step, empty past the end: the wait counts stay fixed
+    };
     // ---------------------------------------------------------------- A: update row i
     {
       // Row i of V and W: entries j-1 were written by their owner in the previous step C with no
@@ -218,6 +263,8 @@ __global__ void __launch_bounds__(kBlock, 2)
         part_n[c] = u;
       }
     }
+    issue(0);
+    issue(1);
     if (!grid_sync(gs, gen)) return;
     // ---------------------------------------------------------------- B: reflector, GEMV, s
     if (warp == 0) {
@@ -241,55 +288,12 @@ __global__ void __launch_bounds__(kBlock, 2)
     }
     __syncthreads();
     const double sc = s_scal[0], tt = s_scal[1];
-    const int I0 = s / kTile;  // first stripe that meets the trailing block
-    double quadp = 0.0;        // this thread's share of v^T A22 v
+    double quadp = 0.0;  // this thread's share of v^T A22 v
     if (tt != 0.0) {
       // GEMV over a contiguous range of the trailing tiles (row-major order over I >= J >= I0):
       // a 3-stage cp.async pipeline keeps two 64 x 64 tiles in flight while a third is reduced.
       // Tiles are copied whole (only the matrix edge is zero-filled): entries outside the
       // trailing block meet v = 0 and add nothing to the rows and columns that are used.
-      const int ntr = nts - I0;
-      const long long ntiles = (long long)ntr * (ntr + 1) / 2;
-      const long long t0 = ntiles * c / G, t1 = ntiles * (c + 1) / G;
-      const int my = (int)(t1 - t0);
-      int Ii = 0, Ji = 0;  // tile coordinates (relative to I0) of the next copy
-      {
-        int Ir = (int)((sqrt(8.0 * (double)t0 + 1.0) - 1.0) * 0.5);
-        while ((long long)(Ir + 1) * (Ir + 2) / 2 <= t0) ++Ir;
-        while ((long long)Ir * (Ir + 1) / 2 > t0) --Ir;
-        Ii = Ir;
-        Ji = (int)(t0 - (long long)Ir * (Ir + 1) / 2);
-      }
-      int Iv = Ii, Jv = Ji, Ic = Ii, Jc = Ji;  // next v fetch, next reduction
-      auto step = [](int& I, int& J) {
-        if (++J > I) {
-          ++I;
-          J = 0;
-        }
-      };
-      auto issue = [&](int k) {
-        if (k < my) {
-          double* T = tiles + (size_t)(k % kStages) * kTile * kTile;
-          const int rb = (I0 + Ii) * kTile, cb = (I0 + Ji) * kTile;
-          if (kEven) {
-#pragma unroll
-            for (int q = 0; q < kTile * kTile / 2 / kBlock; ++q) {
-              const int el = threadIdx.x + kBlock * q, r = rb + (el >> 5), col = cb + 2 * (el & 31);
-              const bool ok = r < n && col < n;
-              cp_async16(T + 2 * el, ok ? A + (size_t)r * n + col : A, ok);
-            }
-          } else {
-#pragma unroll
-            for (int q = 0; q < kTile * kTile / kBlock; ++q) {
-              const int el = threadIdx.x + kBlock * q, r = rb + (el >> 6), col = cb + (el & 63);
-              const bool ok = r < n && col < n;
-              cp_async8(T + el, ok ? A + (size_t)r * n + col : A, ok);
-            }
-          }
-          step(Ii, Ji);
-        }
-        cp_async_commit();  // one group per step, empty past the end: the wait counts stay fixed
-      };
       auto vval = [&](int col) {  // v over the whole row: 0 before the trailing block and past n
         return (col < s || col >= n) ? 0.0 : (col == s ? 1.0 : __ldcg(rowi + col) * sc);
       };
@@ -306,8 +310,18 @@ __global__ void __launch_bounds__(kBlock, 2)
         }
         step(Iv, Jv);
       };
-      issue(0);
-      issue(1);
+      // s1 = W^T v, s2 = V^T v over rows > i, components < j (v_s = 1, v_r = a_r sc beyond):
+      // c < 32 is W-based (W at X[., 32 + k]), c >= 32 V-based (V at X[., k]). Done before the
+      // GEMV so that these blocks do not arrive last at barrier 2.
+      if (c < 64 && warp == 0) {
+        const int k = c & 31;
+        double tot = 0.0;
+        if (k < j) {
+          const double acc = warp_sum_cg(part_s + c, G, lane, 64);
+          tot = __ldcg(X + (size_t)s * kCoopLd + (c < 32 ? kPanel : 0) + k) + sc * acc;
+        }
+        if (lane == 0) s_tot[c] = tot;
+      }
       if (my > 0) fetch_v();
       for (int k = 0; k < my; ++k) {
         issue(k + 2);
@@ -352,17 +366,8 @@ __global__ void __launch_bounds__(kBlock, 2)
         }
       }
       cp_async_wait<0>();
-      // s1 = W^T v, s2 = V^T v over rows > i, components < j (v_s = 1, v_r = a_r sc beyond):
-      // c < 32 is W-based (W at X[., 32 + k]), c >= 32 V-based (V at X[., k])
-      if (c < 64 && warp == 0) {
-        const int k = c & 31;
-        double tot = 0.0;
-        if (k < j) {
-          const double acc = warp_sum_cg(part_s + c, G, lane, 64);
-          tot = __ldcg(X + (size_t)s * kCoopLd + (c < 32 ? kPanel : 0) + k) + sc * acc;
-        }
-        if (lane == 0) s_tot[c] = tot;
-      }
+    } else {
+      cp_async_wait<0>();  // the early copies land before the stages are reused
     }
     {  // block partial of v^T A22 v (every block writes one, zero without a reflection)
       quadp = warp_sum(quadp);
