@@ -244,7 +244,7 @@ int pm3gpu_last_large_trace(pm3gpu_ctx* ctx, double* rows, int max_rows);
  * atom block and atom-pair block of the initial density from element one-hots, 32 Gaussian
  * distance functions (6 A cutoff) and coordination counts; the SCF starts from the aufbau density
  * of that prediction's Fock matrix (guess =
- * PM3GPU_GUESS_LEARNED in the options). The plain SCF stays the judge: a molecule that does not
+ * PM3GPU_GUESS_LEARNED in the options). The plain SCF has the last word: a molecule that does not
  * converge from the learned start is solved again from the standard guess.
  *
  * pm3gpu_guess_train solves the given molecules with the plain SCF (their options), takes the

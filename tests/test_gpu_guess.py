@@ -1,7 +1,7 @@
 """Learned initial density (pm3gpu_guess_*): features and the BF16 network against a numpy
 restatement, training on converged densities, and SCF results that do not depend on the start.
 
-The SCF stays the judge: starting from the learned density (or from an untrained network's
+The SCF has the last word: starting from the learned density (or from an untrained network's
 garbage) the converged heat of formation and charges must equal the standard-guess results
 within the parity bars, because both runs converge to the same fixed point.
 """

@@ -1,6 +1,6 @@
 """GPU (pm3gpu through its C ABI) against the CPU oracle on the same inputs.
 
-Bars (from the north star): heat of formation within 1e-6 kcal/mol, Mulliken charges within
+Bars: heat of formation within 1e-6 kcal/mol, Mulliken charges within
 1e-5 e, analytic gradient components within 1e-6 kcal/mol/A; H_core and Fock elements within
 1e-10 eV (same FP64 formulas, different summation order).
 """
