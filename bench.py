@@ -459,6 +459,11 @@ def guess_main(args, rank):
     if rc != 0:
         raise RuntimeError(ctx.last_error())
     train_s = time.perf_counter() - t0
+    if args.save_guess:  # the trained parameters, for `--guess-params` of the batched workloads
+        params = np.zeros(_lib.GUESS_PARAMS, np.float32)
+        if lib.pm3gpu_guess_get_params(ctx.ptr, params.ctypes.data_as(F), _lib.GUESS_PARAMS) != 0:
+            raise RuntimeError(ctx.last_error())
+        params.tofile(args.save_guess)
     held = [m for m in workloads.organic_batch(args.n_mol or 4096, 20, 90, seed=90002) if basis_size(m[0]) <= 256]
     hoffs, hz, hxyz = workloads.pack(held)
     hoffs, hz, hxyz = np.ascontiguousarray(hoffs), np.ascontiguousarray(hz), np.ascontiguousarray(hxyz * A2B)
@@ -532,6 +537,11 @@ def main():
     ap.add_argument("--inflight", type=int, default=3,
                     help="batched workloads: batches in flight (contexts/streams/host threads); 1 times the batches "
                          "one after another")
+    ap.add_argument("--save-guess", default=None,
+                    help="learned-guess workload: write the trained parameters (float32) to this file")
+    ap.add_argument("--guess-params", default=None,
+                    help="batched workloads: start every molecule from the learned density of these parameters "
+                         "(float32, as written by --save-guess)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="batched workloads: skip the calibration that, before timing, measures the launch choices on a "
                          "sample of the same generator (another seed; 1024 organics or 256 radicals) and uses the faster")
@@ -602,6 +612,17 @@ def main():
     stream = torch.cuda.current_stream(dev)
     lib.pm3gpu_set_stream(ctx.ptr, ctypes.c_void_p(stream.cuda_stream))
     opts = native.options(**gpu_opts)
+    guess_params = None
+    if args.guess_params:  # learned initial density (the standard-guess pass stays as backup)
+        guess_params = np.fromfile(args.guess_params, dtype=np.float32)
+        opts.guess = _lib.GUESS_LEARNED
+
+    def load_guess(c):
+        if guess_params is not None and c.lib.pm3gpu_guess_set_params(
+                c.ptr, guess_params.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), len(guess_params)) != 0:
+            raise RuntimeError(c.last_error())
+
+    load_guess(ctx)
     results = (_lib.Result * n_mol)()
     charges = np.zeros(n_atoms)
     grads = np.zeros((n_atoms, 3)) if want_grad else None
@@ -688,6 +709,8 @@ def main():
             c = ctx if k == 0 else _lib.Context(local)
             if k > 0 and tuning is not None and lib.pm3gpu_load_tuning(c.ptr, path.encode()) != 0:
                 raise RuntimeError(c.last_error())
+            if k > 0:
+                load_guess(c)
             st = torch.cuda.Stream(dev)
             lib.pm3gpu_set_stream(c.ptr, ctypes.c_void_p(st.cuda_stream))
             slots.append({"ctx": c, "stream": st, "results": (_lib.Result * n_mol)(), "charges": np.zeros(n_atoms),
@@ -816,6 +839,7 @@ def main():
                    "l2": ("flushed before the overlapped steps (512 MiB write); per-CTA workspaces (> 126 MB) exceed L2"
                           if slots else "flushed between steps (512 MiB write)"),
                    "batches_in_flight": max(1, args.inflight),
+                   "guess": f"learned ({args.guess_params})" if guess_params is not None else "reference default (SAD)",
                    "submission": (f"slot k submits its first batch k x {1e3 * stagger:.0f} ms into the timed region "
                                   "(one batch time / slots), then back to back") if slots else "one batch at a time",
                    "converged_fraction": conv / (n_mol * args.steps * world),
