@@ -174,27 +174,34 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
       double acc[3 * kMaxDepth + 2];
 #pragma unroll
       for (int q = 0; q < 3 * kMaxDepth + 2; ++q) acc[q] = 0.0;
-      for (size_t k = tid; k < nn; k += kThreads) {
-        const double ea = Ea[k], fa = Fa[k];
-        const double eb = uhf ? Eb[k] : 0.0;
-        const double dn = keep ? Dh[k] : 0.0;
-        acc[3 * kMaxDepth] = fma(ea, ea, acc[3 * kMaxDepth]);
-        if (uhf) acc[3 * kMaxDepth] = fma(eb, eb, acc[3 * kMaxDepth]);
-        if (keep) acc[3 * kMaxDepth + 1] = fma(dn, fa, acc[3 * kMaxDepth + 1]);
+      // Every product pairs two symmetric (F, D) or two antisymmetric (E) matrices, so the sum
+      // over all n^2 elements is the diagonal plus twice the strict lower triangle: half the
+      // history reads. Rows go to warps, columns to lanes (coalesced).
+      for (int r = tid >> 5; r < n; r += kWarps)
+        for (int col = tid & 31; col <= r; col += 32) {
+          const size_t k = (size_t)r * n + col;
+          const double wgt = col == r ? 1.0 : 2.0;
+          const double ea = Ea[k], fa = Fa[k];
+          const double eb = uhf ? Eb[k] : 0.0;
+          const double dn = keep ? Dh[k] : 0.0;
+          double ee = ea * ea;
+          if (uhf) ee = fma(eb, eb, ee);
+          acc[3 * kMaxDepth] = fma(wgt, ee, acc[3 * kMaxDepth]);
+          if (keep) acc[3 * kMaxDepth + 1] = fma(wgt, dn * fa, acc[3 * kMaxDepth + 1]);
 #pragma unroll
-        for (int l = 0; l < kMaxDepth; ++l) {
-          if (l < len) {
-            const double* bl = c.hist + (size_t)((head + l) % depth) * slot_mats * nn;
-            double v = bl[nn + k] * ea;
-            if (uhf) v = fma(bl[3 * nn + k], eb, v);
-            acc[l] += v;
-            if (keep) {
-              acc[kMaxDepth + l] = fma(dn, bl[k], acc[kMaxDepth + l]);           // <D_new, F_l>
-              acc[2 * kMaxDepth + l] = fma(bl[2 * nn + k], fa, acc[2 * kMaxDepth + l]);  // <D_l, F_new>
+          for (int l = 0; l < kMaxDepth; ++l) {
+            if (l < len) {
+              const double* bl = c.hist + (size_t)((head + l) % depth) * slot_mats * nn;
+              double v = bl[nn + k] * ea;
+              if (uhf) v = fma(bl[3 * nn + k], eb, v);
+              acc[l] = fma(wgt, v, acc[l]);
+              if (keep) {
+                acc[kMaxDepth + l] = fma(wgt, dn * bl[k], acc[kMaxDepth + l]);             // <D_new, F_l>
+                acc[2 * kMaxDepth + l] = fma(wgt, bl[2 * nn + k] * fa, acc[2 * kMaxDepth + l]);  // <D_l, F_new>
+              }
             }
           }
         }
-      }
       block_sums<3 * kMaxDepth + 2>(acc, c.red, c.misc);
       if (tid == 0) {
         for (int l = 0; l < len; ++l) {
