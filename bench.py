@@ -216,8 +216,7 @@ DRAM_BYTES_PER_MOLECULE = 7.43e9 / 256
 def scf_flops(nao, n_occ, iters):
     """Algorithmic FP64 flops of the dense SCF algebra per molecule: per iteration and spin
     tridiagonalisation 4/3 n^3 + back-transformation 2 n^3 + commutator 2 n^3 + density
-    2 n^2 n_occ (the per-iteration formula of the hot-path measurement plan); `iters` counts
-    iterations times spins."""
+    2 n^2 n_occ; `iters` counts iterations times spins."""
     n = nao.astype(np.float64)
     return float(np.sum(iters * ((4.0 / 3.0) * n ** 3 + 2.0 * n ** 3 + 2.0 * n ** 3 + 2.0 * n * n * n_occ)))
 
@@ -683,7 +682,8 @@ def main():
             e.record(stream)
             torch.cuda.synchronize(dev)
             ms.append(s.elapsed_time(e))
-            st = np.array([r.status for r in results])
+            rv = np.ctypeslib.as_array(results)
+            st = rv["status"]
             conv += int((st == 0).sum())
             launches += lib.pm3gpu_last_kernel_launches(ctx.ptr)
             t = (ctypes.c_double * 8)()
@@ -692,10 +692,8 @@ def main():
             hb, db = ctypes.c_longlong(), ctypes.c_longlong()
             lib.pm3gpu_last_transfer_bytes(ctx.ptr, ctypes.byref(hb), ctypes.byref(db))
             xfer[0], xfer[1] = hb.value, db.value
-            nao = np.array([r.nao for r in results])
-            nocc = np.array([r.n_occ for r in results])
-            its = np.array([r.iterations for r in results])
-            spins = 1.0 + np.array([r.unrestricted for r in results], dtype=np.float64)
+            nao, nocc, its = rv["nao"], rv["n_occ"], rv["iterations"]
+            spins = 1.0 + rv["unrestricted"].astype(np.float64)
             flops += scf_flops(nao[st == 0], nocc[st == 0], its[st == 0] * spins[st == 0])
         return ms, conv, launches, kern_ms, flops
 
@@ -756,15 +754,12 @@ def main():
                     time.sleep(k * stagger)
                 for _ in range(k, steps, len(slots)):
                     run_slot(sl, host)
-                    res = sl["results"]
-                    st = np.array([r.status for r in res])
-                    acc[k][0] += int((st == 0).sum())
+                    res = np.ctypeslib.as_array(sl["results"])  # a view: no per-molecule Python work
+                    ok = res["status"] == 0
+                    acc[k][0] += int(ok.sum())
                     acc[k][1] += lib.pm3gpu_last_kernel_launches(sl["ctx"].ptr)
-                    ok = st == 0
-                    nao = np.array([r.nao for r in res])[ok]
-                    nocc = np.array([r.n_occ for r in res])[ok]
-                    its = np.array([r.iterations for r in res])[ok] * (1.0 + np.array([r.unrestricted for r in res])[ok])
-                    acc[k][2] += scf_flops(nao, nocc, its)
+                    its = res["iterations"][ok] * (1.0 + res["unrestricted"][ok])
+                    acc[k][2] += scf_flops(res["nao"][ok], res["n_occ"][ok], its)
                     hb, db = ctypes.c_longlong(), ctypes.c_longlong()
                     lib.pm3gpu_last_transfer_bytes(sl["ctx"].ptr, ctypes.byref(hb), ctypes.byref(db))
                     xfer[0], xfer[1] = hb.value, db.value
