@@ -215,7 +215,8 @@ int pm3gpu_set_large_threshold(pm3gpu_ctx* ctx, int nao);
  * Householder reduction as one cooperative launch per panel or as five launches per column
  * (bucket: basis size). Both variants of each choice give the same results. When cache_path is
  * not NULL the table is written there as JSON; pm3gpu_load_tuning reads such a file into another
- * context. pm3gpu_tuning_choice returns the choice a size would get (kind 0: CTAs per SM for a
+ * context (with ctx = NULL it only checks the file and returns its status).
+ * pm3gpu_tuning_choice returns the choice a size would get (kind 0: CTAs per SM for a
  * batch whose largest basis is `size`; kind 1: 1 = cooperative panels for basis `size`), or -1
  * when no tuned bucket covers it. */
 int pm3gpu_autotune(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,

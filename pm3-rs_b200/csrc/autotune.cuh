@@ -130,7 +130,8 @@ int write_tuning(pm3gpu_ctx* c, const char* path) {
 }
 
 // Reads the format write_tuning produces: every innermost {...} object with "nmax_le" is a batch
-// entry, with "n_le" a large entry; other keys are ignored.
+// entry, with "n_le" a large entry; other keys are ignored. With c == nullptr the file is only
+// checked (no device is touched).
 int read_tuning(pm3gpu_ctx* c, const char* path) {
   FILE* f = std::fopen(path, "r");
   if (!f) return fail(c, PM3GPU_INVALID_INPUT, std::string("cannot read tuning file ") + path);
@@ -167,6 +168,7 @@ int read_tuning(pm3gpu_ctx* c, const char* path) {
     }
   }
   if (tb.empty() && tl.empty()) return fail(c, PM3GPU_INVALID_INPUT, std::string("no tuning entries in ") + path);
+  if (!c) return PM3GPU_OK;
   for (const pm3gpu_ctx::Tune& e : tb) tune_store(c->tune_batch, e);
   for (const pm3gpu_ctx::Tune& e : tl) tune_store(c->tune_large, e);
   return PM3GPU_OK;

@@ -1536,7 +1536,8 @@ int pm3gpu_autotune(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t
 }
 
 int pm3gpu_load_tuning(pm3gpu_ctx* c, const char* path) {
-  if (!c || !path) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  if (!path) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  if (!c) return read_tuning(nullptr, path);  // check the file only
   std::lock_guard<std::mutex> lk(c->mu);
   return read_tuning(c, path);
 }

@@ -67,3 +67,21 @@ def test_unsupported_method_and_field_raise_before_any_gpu_work():
         native.single_point([8, 1, 1], np.zeros((3, 3)), reference="rohf")
     with pytest.raises(ValueError):
         native.single_point([8, 1, 1], np.zeros((2, 3)))
+
+
+def test_tuning_file_is_checked_without_a_device(tmp_path):
+    """pm3gpu_load_tuning with no context only parses the file (host code, no CUDA call)."""
+    lib = _lib.load()
+    good = tmp_path / "tuning.json"
+    good.write_text('{\n  "device": "B200",\n  "sms": 148,\n  "batch": [\n'
+                    '    {"nmax_le": 256, "ctas_per_sm": 1, "ms_1cta": 900.0, "ms_2cta": 950.0}\n  ],\n'
+                    '  "large": [\n    {"n_le": 512, "coop": 1, "ms_coop": 1.0, "ms_multi": 2.0}\n  ]\n}\n')
+    assert lib.pm3gpu_load_tuning(None, str(good).encode()) == _lib.OK
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"large": [{"n_le": 512, "coop": 2}]}')
+    assert lib.pm3gpu_load_tuning(None, str(bad).encode()) == _lib.INVALID_INPUT
+    empty = tmp_path / "empty.json"
+    empty.write_text('{"batch": [], "large": []}')
+    assert lib.pm3gpu_load_tuning(None, str(empty).encode()) == _lib.INVALID_INPUT
+    assert lib.pm3gpu_load_tuning(None, str(tmp_path / "missing.json").encode()) == _lib.INVALID_INPUT
+    assert lib.pm3gpu_tuning_choice(None, 0, 100) == -1
