@@ -642,8 +642,7 @@ def main():
         t_off, t_z, t_xyz = workloads.pack(tmols)
         t_off, t_z = np.ascontiguousarray(t_off, np.int32), np.ascontiguousarray(t_z, np.int32)
         t_xyz = np.ascontiguousarray(t_xyz)
-        path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                            f"tuning_{args.workload}.json")
+        path = os.path.join(tempfile.mkdtemp(prefix="pm3gpu_tuning_"), f"tuning_{args.workload}.json")
         if lib.pm3gpu_autotune(ctx.ptr, len(tmols), t_off.ctypes.data_as(I32), t_z.ctypes.data_as(I32),
                                t_xyz.ctypes.data_as(D), ctypes.byref(opts), path.encode()) != 0:
             raise RuntimeError(ctx.last_error())

@@ -102,9 +102,49 @@ int pm3gpu_supported_element(int z);
  * (sizes the caller's density / MO-energy buffers). Replaces Basis::build (src/basis.rs:39). */
 int pm3gpu_result_sizes(int n_atoms, const int32_t* z, int* nao);
 
+/* One element of a PM3 parameter set: the fields of Pm3Element (src/params.rs:20-92) that the
+ * s/p path reads, raw and derived, exactly as the reference's run_pm3 reads them from
+ * &Pm3Parameters (derived values are used as given, not re-derived). Energies in eV, exponents in
+ * Bohr^-1, alpha in Angstrom^-1, charge separations and additive terms in Bohr. */
+typedef struct {
+  int z;            /* atomic number (1..17) */
+  int n_orb;        /* 1 (s) or 4 (s, p) */
+  int npq;          /* principal quantum number of the valence s shell (Pm3Element::n), 1..3 */
+  int n_gauss;      /* core-core Gaussian corrections used, 0..4 */
+  double u_ss, u_pp, zeta_s, zeta_p, beta_s, beta_p;
+  double g_ss, g_sp, g_pp, g_p2, h_sp;
+  double alpha;          /* per-element core-core exponent */
+  double gauss[4][3];    /* (K, L, M) of each Gaussian */
+  double core_charge, occ_s, occ_p;
+  double eheat_ev, e_isol, mass;
+  double dd, qq, rho0, rho1, rho2;  /* electron-electron multipoles */
+  double ddp[7], po[10];            /* electron-core / core-core terms: ddp[2], ddp[3], po[1..3], po[9] */
+} pm3gpu_element;
+
+/* Pairwise core-core parameters PairParams (src/params.rs:104-109), symmetric in (zi, zj). */
+typedef struct {
+  int zi, zj;
+  double alpha, x;
+} pm3gpu_pair;
+
+/* Pm3Parameters::standard() (src/params.rs:133-137): the built-in PM3 set for the elements of
+ * the s/p path. Writes up to max_elems / max_pairs entries and the counts. */
+int pm3gpu_standard_parameters(pm3gpu_element* elems, int max_elems, int* n_elems, pm3gpu_pair* pairs,
+                               int max_pairs, int* n_pairs);
+
+/* The &Pm3Parameters argument of run_pm3 (src/scf.rs:450-452; Pm3Calculator::new, src/scf.rs:404-410):
+ * replaces the context's parameter set for every later call on it. Elements absent from `elems`
+ * are missing (molecules containing them return PM3GPU_MISSING_ELEMENT, as
+ * Pm3Parameters::element does, src/params.rs:139-141); pairs absent from `pairs` use the
+ * per-element core-core form. Returns PM3GPU_INVALID_INPUT (nothing changed) on an out-of-range
+ * or non-finite entry. The learned-guess network is independent of the parameters. */
+int pm3gpu_set_parameters(pm3gpu_ctx* ctx, const pm3gpu_element* elems, int n_elems, const pm3gpu_pair* pairs,
+                          int n_pairs);
+
 int pm3gpu_context_create(int device, pm3gpu_ctx** out);
 void pm3gpu_context_destroy(pm3gpu_ctx* ctx);
-/* Message of the last failing call on this context (owned by the context). */
+/* Message of the last failing call on this context (owned by the context). With ctx = NULL: the
+ * message of the last failing context-free call on this host thread (pm3gpu_load_tuning(NULL, ..)). */
 const char* pm3gpu_last_error_message(pm3gpu_ctx* ctx);
 /* Run subsequent work on an existing CUDA stream (cudaStream_t passed as void*); NULL
  * restores the context's own stream. */
@@ -137,7 +177,12 @@ int pm3gpu_single_point(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const do
  * atoms with 30 hydrogens); larger molecules return PM3GPU_RESOURCE_LIMIT with the needed size.
  * The stability-search rungs share the slots that fit and run one after another if only one does.
  * The first call on each device looks up the array's address (and may load this library's device
- * code), so make it before any stream capture begins. The caller clears nothing: each call resets
+ * code), so make it before any stream capture begins. A device reset invalidates that address
+ * with everything else on the device: create a new context after a reset (creating a context
+ * makes the next call look the address up again).
+ * The call always runs the one-CTA-per-molecule kernel: a molecule that
+ * pm3gpu_set_large_threshold sends to the whole-GPU path returns PM3GPU_RESOURCE_LIMIT here, so
+ * that the two entry points never run different algorithms on the same input. The caller clears nothing: each call resets
  * the queue counters and flags it needs at zero itself. All contexts of a process on one device
  * share the one array, so calls that overlap in time on that device (two contexts, or two
  * threads on different contexts) race and give wrong results; calls through one context are

@@ -101,6 +101,9 @@ def lib():
     L.oracle_core_core.restype = ctypes.c_double
     L.oracle_fixed_density_gradient.argtypes = [ctypes.c_int, _I, _D, _D, _D, _D, ctypes.c_int, _D]
     L.oracle_eigh.argtypes = [ctypes.c_int, _D, _D, _D]
+    L.oracle_set_parameters.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+    L.oracle_reset_parameters.argtypes = []
+    L.oracle_reset_parameters.restype = None
     try:
         import scipy.linalg.cython_blas as cb
         import scipy.linalg.cython_lapack as cl
@@ -110,6 +113,21 @@ def lib():
         L.oracle_set_lapack(None, None)
     _lib = L
     return L
+
+
+def set_parameters(elems, pairs):
+    """Run later calls with the given parameter set (run_pm3's &Pm3Parameters): ctypes arrays of
+    structures with the layout of oracle_element_params / oracle_pair_params (the GPU library's
+    pm3gpu_element / pm3gpu_pair have the same layout)."""
+    rc = lib().oracle_set_parameters(ctypes.cast(elems, ctypes.c_void_p), len(elems),
+                                     ctypes.cast(pairs, ctypes.c_void_p), len(pairs))
+    if rc != 0:
+        raise OracleError(1, "bad parameter set")
+
+
+def reset_parameters():
+    """Back to Pm3Parameters::standard()."""
+    lib().oracle_reset_parameters()
 
 
 def _ip(a):

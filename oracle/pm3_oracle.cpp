@@ -209,10 +209,13 @@ struct Params {
   }
   const Elem* get(int z) const { return (z > 0 && z < 19 && have[z]) ? &el[z] : nullptr; }
 };
-const Params& params() {
+// The parameter set in use: the standard one (Pm3Parameters::standard, params.rs:133-137) unless
+// oracle_set_parameters replaced it (the &Pm3Parameters argument of run_pm3, scf.rs:450-452).
+Params& params_mut() {
   static Params p;
   return p;
 }
+const Params& params() { return params_mut(); }
 
 // ---------------------------------------------------------------- integrals (integrals.rs)
 inline int pack(int a, int b) {
@@ -1583,6 +1586,47 @@ int oracle_nao(int n_atoms, const int* z) {
   }
   return nao;
 }
+
+// Replace the parameter set by the caller's Pm3Element / PairParams values, used as given (the
+// reference reads the derived multipole fields of Pm3Element directly and does not re-derive them).
+int oracle_set_parameters(const oracle_element_params* elems, int n_elems, const oracle_pair_params* pairs,
+                          int n_pairs) {
+  Params P;
+  for (int z = 0; z < 19; ++z) P.have[z] = false;
+  for (int i = 0; i < 19; ++i)
+    for (int j = 0; j < 19; ++j) P.have_pair[i][j] = false;
+  for (int k = 0; k < n_elems; ++k) {
+    const oracle_element_params& r = elems[k];
+    if (r.z <= 0 || r.z >= 19 || (r.n_orb != 1 && r.n_orb != 4) || r.n_gauss < 0 || r.n_gauss > 4) return 1;
+    Elem e;
+    e.z = r.z;
+    e.norb = r.n_orb;
+    e.n = r.npq;
+    e.uss = r.u_ss; e.upp = r.u_pp; e.zs = r.zeta_s; e.zp = r.zeta_p; e.bs = r.beta_s; e.bp = r.beta_p;
+    e.gss = r.g_ss; e.gsp = r.g_sp; e.gpp = r.g_pp; e.gp2 = r.g_p2; e.hsp = r.h_sp;
+    e.alpha = r.alpha;
+    for (int g = 0; g < r.n_gauss; ++g) e.gauss.push_back({r.gauss[g][0], r.gauss[g][1], r.gauss[g][2]});
+    e.core = r.core_charge; e.occ_s = r.occ_s; e.occ_p = r.occ_p;
+    e.eheat_ev = r.eheat_ev; e.e_isol = r.e_isol; e.mass = r.mass;
+    e.dd = r.dd; e.qq = r.qq; e.rho0 = r.rho0; e.rho1 = r.rho1; e.rho2 = r.rho2;
+    for (int i = 0; i < 10; ++i) e.po[i] = r.po[i];
+    for (int i = 0; i < 7; ++i) e.ddp[i] = r.ddp[i];
+    P.el[e.z] = e;
+    P.have[e.z] = true;
+  }
+  for (int k = 0; k < n_pairs; ++k) {
+    const oracle_pair_params& q = pairs[k];
+    if (q.zi <= 0 || q.zi >= 19 || q.zj <= 0 || q.zj >= 19) return 1;
+    int a = std::max(q.zi, q.zj), b = std::min(q.zi, q.zj);
+    P.pair_alpha[a][b] = P.pair_alpha[b][a] = q.alpha;
+    P.pair_x[a][b] = P.pair_x[b][a] = q.x;
+    P.have_pair[a][b] = P.have_pair[b][a] = true;
+  }
+  params_mut() = P;
+  return 0;
+}
+
+void oracle_reset_parameters(void) { params_mut() = Params(); }
 
 int oracle_element(int z, double* out) {
   const Elem* e = params().get(z);

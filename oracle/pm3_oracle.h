@@ -59,6 +59,31 @@ int oracle_single_point(int n_atoms, const int* z, const double* xyz_bohr,
                         double* density, double* mo_energies, double* gradient, char* err,
                         int errlen);
 
+/* One element of a parameter set: the Pm3Element fields of the s/p path (src/params.rs:20-92),
+ * raw and derived, used as given. Same layout as the GPU library's pm3gpu_element. */
+typedef struct {
+  int z, n_orb, npq, n_gauss;
+  double u_ss, u_pp, zeta_s, zeta_p, beta_s, beta_p;
+  double g_ss, g_sp, g_pp, g_p2, h_sp;
+  double alpha;
+  double gauss[4][3];
+  double core_charge, occ_s, occ_p;
+  double eheat_ev, e_isol, mass;
+  double dd, qq, rho0, rho1, rho2;
+  double ddp[7], po[10];
+} oracle_element_params;
+typedef struct {
+  int zi, zj;
+  double alpha, x;
+} oracle_pair_params;
+
+/* Replace the parameter set (run_pm3's &Pm3Parameters, src/scf.rs:450-452); elements absent from
+ * the set are missing. Returns 0, or 1 on an out-of-range entry. oracle_reset_parameters restores
+ * the standard set (Pm3Parameters::standard, src/params.rs:133-137). */
+int oracle_set_parameters(const oracle_element_params* elems, int n_elems, const oracle_pair_params* pairs,
+                          int n_pairs);
+void oracle_reset_parameters(void);
+
 /* Derived element constants: out[0..21] = n_orb, uss, upp, zs, zp, betas, betap, gss, gsp,
  * gpp, gp2, hsp, alpha, core, dd, qq, rho0, rho1, rho2, e_isol, eheat_ev, mass. */
 int oracle_element(int z, double* out);

@@ -155,12 +155,16 @@ int read_tuning(pm3gpu_ctx* c, const char* path) {
       return stop != obj.c_str() + colon + 1;
     };
     double le, ch, a = 0.0, b = 0.0;
+    // bucket bounds are basis sizes: finite, at least 1 and at most the whole-GPU path's reach
+    auto bad_le = [&](double v) { return !std::isfinite(v) || v < 1.0 || v > 1.0e6 || v != std::floor(v); };
     if (num("nmax_le", &le) && num("ctas_per_sm", &ch)) {
+      if (bad_le(le)) return fail(c, PM3GPU_INVALID_INPUT, "tuning file: nmax_le must be an integer in 1..1000000");
       num("ms_1cta", &a);
       num("ms_2cta", &b);
       if (ch != 1.0 && ch != 2.0) return fail(c, PM3GPU_INVALID_INPUT, "tuning file: ctas_per_sm must be 1 or 2");
       tb.push_back({(int)le, (int)ch, a, b});
     } else if (num("n_le", &le) && num("coop", &ch)) {
+      if (bad_le(le)) return fail(c, PM3GPU_INVALID_INPUT, "tuning file: n_le must be an integer in 1..1000000");
       num("ms_coop", &a);
       num("ms_multi", &b);
       if (ch != 0.0 && ch != 1.0) return fail(c, PM3GPU_INVALID_INPUT, "tuning file: coop must be 0 or 1");

@@ -82,6 +82,9 @@ struct MolPlan {
 
 }  // namespace
 
+// Clears the cached address of the allocation-free path's scratch array on `device`.
+void noalloc_forget(int device);
+
 struct pm3gpu_ctx {
   int device = 0;
   cudaStream_t own = nullptr, stream = nullptr;
@@ -132,8 +135,13 @@ int tune_lookup(const std::vector<pm3gpu_ctx::Tune>& t, int size, int dflt) {
   return dflt;
 }
 
+// Message of the last failure of a call made without a context (pm3gpu_load_tuning(NULL, ..)),
+// per host thread, so that a check without a device can still say what is wrong.
+thread_local std::string t_noctx_err;
+
 int fail(pm3gpu_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
+  else t_noctx_err = msg;
   return code;
 }
 #define CUDA_TRY(ctx, call)                                                                        \
@@ -147,6 +155,142 @@ bool supported(int z) { return z > 0 && z < kMaxZ && [&] {
     if (PM3_RAW_ELEMENTS[k].z == z) return true;
   return false;
 }(); }
+
+// Element z is in the s/p analytic path and present in the context's parameter set.
+bool has_elem(const pm3gpu_ctx* c, int z) { return supported(z) && c->h_elem[z].z == z; }
+
+// ---------------------------------------------------------------- parameter sets
+// The public pm3gpu_element (the Pm3Element fields of the s/p path) from the context's form.
+void elem_to_public(const ElemDev& e, pm3gpu_element& o) {
+  std::memset(&o, 0, sizeof(o));
+  o.z = e.z;
+  o.n_orb = e.norb;
+  o.npq = e.npq;
+  o.n_gauss = e.ngauss;
+  o.u_ss = e.uss;
+  o.u_pp = e.upp;
+  o.zeta_s = e.zs;
+  o.zeta_p = e.zp;
+  o.beta_s = e.bs;
+  o.beta_p = e.bp;
+  o.g_ss = e.gss;
+  o.g_sp = e.gsp;
+  o.g_pp = e.gpp;
+  o.g_p2 = e.gp2;
+  o.h_sp = e.hsp;
+  o.alpha = e.alpha;
+  for (int g = 0; g < e.ngauss && g < 4; ++g) {
+    o.gauss[g][0] = e.gk[g];
+    o.gauss[g][1] = e.gl[g];
+    o.gauss[g][2] = e.gm[g];
+  }
+  o.core_charge = e.core;
+  o.occ_s = e.occ_s;
+  o.occ_p = e.occ_p;
+  o.eheat_ev = e.eheat_ev;
+  o.e_isol = e.e_isol;
+  o.mass = e.mass;
+  o.dd = e.dd;
+  o.qq = e.qq;
+  o.rho0 = e.rho0;
+  o.rho1 = e.rho1;
+  o.rho2 = e.rho2;
+  // params.rs:694-709: po(1,2,3,7,9) and ddp(2,3) of a main-group element
+  o.po[1] = e.po1;
+  o.po[2] = e.po2;
+  o.po[3] = e.po3;
+  o.po[7] = e.rho0;
+  o.po[9] = e.po9;
+  if (e.norb == 4) {
+    o.ddp[2] = e.ddp2;
+    o.ddp[3] = e.qq * std::sqrt(2.0);
+  }
+}
+
+// The context's form of one public element; false (with the reason) when it is out of range.
+bool elem_from_public(const pm3gpu_element& i, ElemDev& e, std::string& why) {
+  const std::string tag = "parameter set, Z=" + std::to_string(i.z) + ": ";
+  if (!supported(i.z)) {
+    why = tag + "element outside the s/p analytic path";
+    return false;
+  }
+  if (i.n_orb != 1 && i.n_orb != 4) {
+    why = tag + "n_orb must be 1 or 4";
+    return false;
+  }
+  if (i.npq < 1 || i.npq > 3) {
+    why = tag + "npq must be 1, 2 or 3";
+    return false;
+  }
+  if (i.n_gauss < 0 || i.n_gauss > 4) {
+    why = tag + "n_gauss must be 0..4";
+    return false;
+  }
+  const double* d = &i.u_ss;
+  const double* d_end = reinterpret_cast<const double*>(reinterpret_cast<const char*>(&i) + sizeof(i));
+  for (; d < d_end; ++d)
+    if (!std::isfinite(*d)) {
+      why = tag + "non-finite value";
+      return false;
+    }
+  if (i.n_orb == 4 && (i.zeta_p <= 0.0 || i.dd <= 0.0 || i.qq <= 0.0)) {
+    why = tag + "an s/p element needs zeta_p, dd and qq > 0";
+    return false;
+  }
+  if (i.zeta_s <= 0.0 || i.g_ss <= 0.0 || i.rho0 <= 0.0 || i.po[9] <= 0.0 || i.core_charge < 0.0) {
+    why = tag + "zeta_s, g_ss, rho0 and po[9] must be > 0 and core_charge >= 0";
+    return false;
+  }
+  e = ElemDev{};
+  e.z = i.z;
+  e.norb = i.n_orb;
+  e.npq = i.npq;
+  e.ngauss = i.n_gauss;
+  e.uss = i.u_ss;
+  e.upp = i.u_pp;
+  e.zs = i.zeta_s;
+  e.zp = i.zeta_p;
+  e.bs = i.beta_s;
+  e.bp = i.beta_p;
+  e.gss = i.g_ss;
+  e.gsp = i.g_sp;
+  e.gpp = i.g_pp;
+  e.gp2 = i.g_p2;
+  e.hsp = i.h_sp;
+  e.alpha = i.alpha;
+  e.core = i.core_charge;
+  e.dd = i.dd;
+  e.qq = i.qq;
+  e.rho0 = i.rho0;
+  e.rho1 = i.rho1;
+  e.rho2 = i.rho2;
+  e.po1 = i.po[1];
+  e.po2 = i.po[2];
+  e.po3 = i.po[3];
+  e.po9 = i.po[9];
+  e.ddp2 = i.ddp[2];
+  e.qq_core = i.ddp[3] / std::sqrt(2.0);  // MOPAC spcore divides ddp(3) by sqrt 2
+  e.occ_s = i.occ_s;
+  e.occ_p = i.occ_p;
+  e.e_isol = i.e_isol;
+  e.eheat_ev = i.eheat_ev;
+  e.mass = i.mass;
+  for (int g = 0; g < i.n_gauss; ++g) {
+    e.gk[g] = i.gauss[g][0];
+    e.gl[g] = i.gauss[g][1];
+    e.gm[g] = i.gauss[g][2];
+  }
+  return true;
+}
+
+// Pair table entry as repulsion.rs:75-90 reads it: xfac only when |x| > 1e-5, alpha 1.2 when
+// the stored alpb is below 1e-6.
+void pair_to_dev(int zi, int zj, double alpb, double xfac, PairDev& P) {
+  const int use = std::fabs(xfac) > 1.0e-5;
+  P.alpha[zi][zj] = P.alpha[zj][zi] = alpb < 1.0e-6 ? 1.2 : alpb;
+  P.x[zi][zj] = P.x[zj][zi] = xfac;
+  P.has[zi][zj] = P.has[zj][zi] = use;
+}
 
 // Validate one molecule and resolve its electron counts (scf.rs:456-520).
 void plan_molecule(const pm3gpu_ctx* c, const int32_t* z, const double* xyz, int natom, const pm3gpu_options* o,
@@ -167,6 +311,11 @@ void plan_molecule(const pm3gpu_ctx* c, const int32_t* z, const double* xyz, int
   double core = 0.0;
   for (int a = 0; a < natom; ++a) {
     const int zz = z[a];
+    if (supported(zz) && !has_elem(c, zz)) {  // left out of the context's parameter set
+      m.status = PM3GPU_MISSING_ELEMENT;
+      m.msg = "missing PM3 parameter block for Z=" + std::to_string(zz);
+      return;
+    }
     if (!supported(zz)) {
       const bool pm3_has = zz >= 1 && zz <= 107 && zz != 87;
       m.status = pm3_has ? PM3GPU_UNSUPPORTED : PM3GPU_MISSING_ELEMENT;
@@ -254,6 +403,51 @@ JobDesc make_job(const MolPlan& m, int guess, int accel, double shift, double da
   j.shift = shift;
   j.damping = damp;
   return j;
+}
+
+// Stability search of run_pm3 (scf.rs:599-715). The first pass's flag: 0 no search, 1 search
+// when its frontier gap is below 6 eV (or it did not converge), 2 search whatever it gives. A
+// level shift or damping in the options turns the search off (scf.rs:599-609).
+int stability_mode(const MolPlan& p, const pm3gpu_options* o) {
+  if (p.steered) return 0;
+  if (o->stability == PM3GPU_STABILITY_ALWAYS) return 2;
+  return o->stability == PM3GPU_STABILITY_AUTO ? 1 : 0;
+}
+
+// The rungs the search tries, in the reference's order, skipping those it skips
+// (scf.rs:610-678): restricted rungs for an open shell, the two unrestricted rungs for a closed
+// shell (which may end in a spin-pure state). Writes at most 7 to out; returns the count.
+int stability_rungs(const MolPlan& p, const pm3gpu_options* o, Rung* out) {
+  const int primary = o->guess == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_CORE : PM3GPU_GUESS_SAD;
+  const int other = primary == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_SAD : PM3GPU_GUESS_CORE;
+  const bool closed = !p.use_uhf;
+  const Rung all[7] = {{primary, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                       {other, o->accelerator, 0.0, 0.0, false},
+                       {other, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                       {PM3GPU_GUESS_SYMMETRY_BROKEN, o->accelerator, 0.0, 0.0, false},
+                       {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
+                       {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, -2.0, 0.0, closed},
+                       {primary, PM3GPU_ACCEL_CDIIS, 0.0, 0.85, closed}};
+  int n = 0;
+  for (const Rung& r : all)
+    if (r.unrestricted == closed) out[n++] = r;
+  return n;
+}
+
+// run_pm3's selection (scf.rs:680-715): whether the outcome `cand` of rung `r` replaces the
+// current state `cur`. A converged unrestricted rung of a closed shell counts only when it is
+// spin-pure, and then as a restricted state (cand_unres cleared, alpha frontier taken).
+bool rung_replaces(const Rung& r, JobOut& cand, bool& cand_unres, const JobOut& cur) {
+  if (!cand.converged) return false;
+  if (r.unrestricted) {
+    if (!(cand.spin_max < 1.0e-8)) return false;
+    cand_unres = false;
+    cand.homo = cand.homo_a;
+    cand.lumo = cand.lumo_a;
+    cand.has_homo = cand.has_homo_a;
+    cand.has_lumo = cand.has_lumo_a;
+  }
+  return !cur.converged || cand.electronic < cur.electronic - 1.0e-6;
 }
 
 long long pair_table_doubles(const pm3gpu_ctx* c, const int32_t* z, int natom) {
@@ -363,7 +557,6 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   for (const JobDesc& j : jobs) naos.push_back(j.nao);
   const int ctas = c->force_ctas ? c->force_ctas : tune_lookup(c->tune_batch, nmax, 0);
   const SmemLayout L = make_layout(amax, nmax, c->smem_optin, c->smem_per_sm, &naos, ctas);
-  CUDA_TRY(c, cudaFuncSetAttribute(scf_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes));
   int per_sm = 0;
   CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scf_batch_kernel, kThreads, L.bytes));
   if (per_sm < 1) return fail(c, PM3GPU_RESOURCE_LIMIT, "SCF kernel does not fit on an SM");
@@ -535,37 +728,19 @@ int run_large(pm3gpu_ctx* c, const MolPlan& p, const int32_t* hz, const int32_t*
   bool st_unres = (fj.flags & kJobUhf) != 0;
   const double first_ev = st.o.electronic;
   int paths = 1;
-  const bool search = o->stability == PM3GPU_STABILITY_OFF
-                          ? false
-                          : (o->stability == PM3GPU_STABILITY_ALWAYS ? !p.steered : (!p.steered && st.o.gap < 6.0));
+  const int smode = stability_mode(p, o);
+  const bool search = smode == 2 || (smode == 1 && st.o.gap < 6.0);
   if (search) {  // scf.rs:610-715
-    const int primary = o->guess == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_CORE : PM3GPU_GUESS_SAD;
-    const int other = primary == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_SAD : PM3GPU_GUESS_CORE;
-    const bool closed = !p.use_uhf;
-    const Rung all[7] = {{primary, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                         {other, o->accelerator, 0.0, 0.0, false},
-                         {other, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                         {PM3GPU_GUESS_SYMMETRY_BROKEN, o->accelerator, 0.0, 0.0, false},
-                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, -2.0, 0.0, closed},
-                         {primary, PM3GPU_ACCEL_CDIIS, 0.0, 0.85, closed}};
-    for (const Rung& r : all) {
-      if (r.unrestricted != closed) continue;
+    Rung rungs[7];
+    const int nr = stability_rungs(p, o, rungs);
+    for (int k = 0; k < nr; ++k) {
+      const Rung& r = rungs[k];
       ++paths;
       const JobDesc rj = make_job(p, r.guess, r.accel, r.shift, r.damp, r.unrestricted, 0);
       LargeRun cand;
       if (S.scf(rj, cand) != PM3GPU_OK) continue;
-      if (!cand.o.converged) continue;
       bool cand_unres = (rj.flags & kJobUhf) != 0;
-      if (r.unrestricted) {  // a spin-pure unrestricted closed shell is a restricted state
-        if (!(cand.o.spin_max < 1.0e-8)) continue;
-        cand_unres = false;
-        cand.o.homo = cand.o.homo_a;
-        cand.o.lumo = cand.o.lumo_a;
-        cand.o.has_homo = cand.o.has_homo_a;
-        cand.o.has_lumo = cand.o.has_lumo_a;
-      }
-      if (!st.o.converged || cand.o.electronic < st.o.electronic - 1.0e-6) {
+      if (rung_replaces(r, cand.o, cand_unres, st.o)) {
         st = std::move(cand);
         st_unres = cand_unres;
         if ((rc = save(st)) != PM3GPU_OK) return rc;
@@ -804,24 +979,14 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
     j.mol = m;
     assign_offsets(j, want, tot);
     // the rungs run_pm3 would try, in its order, skipping those it skips (scf.rs:610-678)
-    j.stab = 0;
-    if (o->stability == PM3GPU_STABILITY_ALWAYS && !p.steered) j.stab = 2;
-    if (o->stability == PM3GPU_STABILITY_AUTO && !p.steered) j.stab = 1;
+    j.stab = stability_mode(p, o);
     j.rung0 = (int)rjobs.size();
     j.nrung = 0;
     if (j.stab) {
-      const int primary = o->guess == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_CORE : PM3GPU_GUESS_SAD;
-      const int other = primary == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_SAD : PM3GPU_GUESS_CORE;
-      const bool closed = !p.use_uhf;
-      const Rung all[7] = {{primary, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                           {other, o->accelerator, 0.0, 0.0, false},
-                           {other, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                           {PM3GPU_GUESS_SYMMETRY_BROKEN, o->accelerator, 0.0, 0.0, false},
-                           {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                           {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, -2.0, 0.0, closed},
-                           {primary, PM3GPU_ACCEL_CDIIS, 0.0, 0.85, closed}};
-      for (const Rung& r : all) {
-        if (r.unrestricted != closed) continue;
+      Rung rungs[7];
+      const int nr = stability_rungs(p, o, rungs);
+      for (int k = 0; k < nr; ++k) {
+        const Rung& r = rungs[k];
         JobDesc rj = make_job(p, r.guess, r.accel, r.shift, r.damp, r.unrestricted, 0);
         rj.mol = m;
         rj.stab = 0;
@@ -922,16 +1087,7 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
       cand.o = R.rout[fj.rung0 + r];
       cand.job = &rj;
       cand.unrestricted = (rj.flags & kJobUhf) != 0;
-      if (!cand.o.converged) continue;
-      if (p.rungs[r].unrestricted) {  // a spin-pure unrestricted closed shell is a restricted state
-        if (!(cand.o.spin_max < 1.0e-8)) continue;
-        cand.unrestricted = false;
-        cand.o.homo = cand.o.homo_a;
-        cand.o.lumo = cand.o.lumo_a;
-        cand.o.has_homo = cand.o.has_homo_a;
-        cand.o.has_lumo = cand.o.has_lumo_a;
-      }
-      if (!st.o.converged || cand.o.electronic < st.o.electronic - 1.0e-6) st = cand;
+      if (rung_replaces(p.rungs[r], cand.o, cand.unrestricted, st.o)) st = cand;
     }
     chosen[m] = st;
     double e_isol = 0.0, eheat = 0.0;
@@ -1047,6 +1203,62 @@ void pm3gpu_default_options(pm3gpu_options* o) {  // scf.rs:259-287
 
 int pm3gpu_supported_element(int z) { return supported(z) ? 1 : 0; }
 
+int pm3gpu_standard_parameters(pm3gpu_element* elems, int max_elems, int* n_elems, pm3gpu_pair* pairs, int max_pairs,
+                               int* n_pairs) {
+  if (max_elems < 0 || max_pairs < 0 || (max_elems > 0 && !elems) || (max_pairs > 0 && !pairs))
+    return fail(nullptr, PM3GPU_INVALID_INPUT, "bad argument");
+  ElemDev el[kMaxZ];
+  derive_elements(el, nullptr);
+  int ne = 0;
+  for (int z = 1; z < kMaxZ; ++z)
+    if (supported(z) && el[z].z == z) {
+      if (ne < max_elems) elem_to_public(el[z], elems[ne]);
+      ++ne;
+    }
+  int np = 0;
+  for (int k = 0; k < PM3_N_RAW_PAIRS; ++k) {
+    const Pm3RawPair& r = PM3_RAW_PAIRS[k];
+    if (!supported(r.zi) || !supported(r.zj)) continue;
+    if (np < max_pairs) pairs[np] = pm3gpu_pair{r.zi, r.zj, r.alpb, r.xfac};
+    ++np;
+  }
+  if (n_elems) *n_elems = ne;
+  if (n_pairs) *n_pairs = np;
+  return (ne > max_elems || np > max_pairs) ? fail(nullptr, PM3GPU_RESOURCE_LIMIT, "output arrays too small")
+                                            : PM3GPU_OK;
+}
+
+int pm3gpu_set_parameters(pm3gpu_ctx* c, const pm3gpu_element* elems, int n_elems, const pm3gpu_pair* pairs,
+                          int n_pairs) {
+  if (!c || n_elems < 0 || n_pairs < 0 || (n_elems > 0 && !elems) || (n_pairs > 0 && !pairs))
+    return fail(c, PM3GPU_INVALID_INPUT, "bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  ElemDev el[kMaxZ];
+  for (int z = 0; z < kMaxZ; ++z) el[z] = ElemDev{};
+  std::string why;
+  for (int k = 0; k < n_elems; ++k) {
+    ElemDev e;
+    if (!elem_from_public(elems[k], e, why)) return fail(c, PM3GPU_INVALID_INPUT, why);
+    if (el[e.z].z != 0) return fail(c, PM3GPU_INVALID_INPUT, "parameter set: Z=" + std::to_string(e.z) + " twice");
+    el[e.z] = e;
+  }
+  PairDev P{};
+  for (int k = 0; k < n_pairs; ++k) {
+    const pm3gpu_pair& q = pairs[k];
+    if (!supported(q.zi) || !supported(q.zj) || !std::isfinite(q.alpha) || !std::isfinite(q.x))
+      return fail(c, PM3GPU_INVALID_INPUT, "parameter set: bad pair entry " + std::to_string(k));
+    pair_to_dev(q.zi, q.zj, q.alpha, q.x, P);
+  }
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  CUDA_TRY(c, cudaMemcpy(c->elem.p, el, sizeof(el), cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(c->pairs.p, &P, sizeof(PairDev), cudaMemcpyHostToDevice));
+  std::memcpy(c->h_elem, el, sizeof(el));
+  c->h_pairs = P;
+  c->err.clear();
+  return PM3GPU_OK;
+}
+
 int pm3gpu_result_sizes(int n_atoms, const int32_t* z, int* nao) {
   ElemDev el[kMaxZ];
   derive_elements(el, nullptr);
@@ -1085,7 +1297,14 @@ int pm3gpu_context_create(int device, pm3gpu_ctx** out) {
   c->sms = prop.multiProcessorCount;
   c->smem_optin = (int)prop.sharedMemPerBlockOptin;
   c->smem_per_sm = (int)prop.sharedMemPerMultiprocessor;
+  // The dynamic shared-memory limit is an attribute of the kernel for the whole process, not of
+  // one context: it is raised once to the device's opt-in maximum, so that concurrent contexts
+  // never lower it under one another's launches (each launch asks for its own layout's bytes).
+  if ((e = cudaFuncSetAttribute(scf_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, c->smem_optin)) !=
+      cudaSuccess)
+    return bail(e);
   derive_elements(c->h_elem, &c->h_pairs);
+  noalloc_forget(device);
   {
     const char* pe = std::getenv("PM3GPU_PROFILE");
     c->profile = pe && pe[0] && pe[0] != '0';
@@ -1125,7 +1344,7 @@ void pm3gpu_context_destroy(pm3gpu_ctx* c) {
   delete c;
 }
 
-const char* pm3gpu_last_error_message(pm3gpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
+const char* pm3gpu_last_error_message(pm3gpu_ctx* c) { return c ? c->err.c_str() : t_noctx_err.c_str(); }
 
 int pm3gpu_set_stream(pm3gpu_ctx* c, void* stream) {
   if (!c) return PM3GPU_INVALID_INPUT;
@@ -1213,7 +1432,7 @@ static int single_stage(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const doub
   if (n_atoms < 1 || n_atoms > kMaxN) return fail(c, PM3GPU_INVALID_INPUT, "atom count outside 1..256");
   int nao = 0;
   for (int a = 0; a < n_atoms; ++a) {
-    if (!supported(z[a])) return fail(c, PM3GPU_UNSUPPORTED, "unsupported element Z=" + std::to_string(z[a]));
+    if (!has_elem(c, z[a])) return fail(c, PM3GPU_UNSUPPORTED, "unsupported element Z=" + std::to_string(z[a]));
     for (int k = 0; k < 3; ++k)
       if (!std::isfinite(xyz[3 * a + k])) return fail(c, PM3GPU_INVALID_INPUT, "non-finite coordinate");
     nao += c->h_elem[z[a]].norb;
@@ -1335,7 +1554,7 @@ int pm3gpu_guess_predict(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const in
   if (!c->has_guess_model) return fail(c, PM3GPU_INVALID_INPUT, "no learned guess model");
   const int total_atoms = offs[n_mol];
   for (int a = 0; a < total_atoms; ++a)
-    if (!supported(z[a])) return fail(c, PM3GPU_UNSUPPORTED, "unsupported element");
+    if (!has_elem(c, z[a])) return fail(c, PM3GPU_UNSUPPORTED, "unsupported element");
   std::vector<int> a0(n_mol), na(n_mol);
   for (int m = 0; m < n_mol; ++m) {
     a0[m] = offs[m];
@@ -1382,7 +1601,7 @@ int pm3gpu_guess_train(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int3
   std::vector<int> nao(n_mol);
   for (int m = 0; m < n_mol; ++m) {
     int k = 0;
-    for (int a = offs[m]; a < offs[m + 1]; ++a) k += supported(z[a]) ? c->h_elem[z[a]].norb : 0;
+    for (int a = offs[m]; a < offs[m + 1]; ++a) k += has_elem(c, z[a]) ? c->h_elem[z[a]].norb : 0;
     nao[m] = k;
     doff[m] = dtot;
     dtot += (size_t)k * k;
@@ -1616,6 +1835,8 @@ size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // Device address of the scratch array on the context's device (which must be current). Resolved
 // once per device and cached; the first resolution may also load this library's device code.
+// Creating a context on a device clears its entry (noalloc_forget), so that after a device reset
+// and a new context the address is looked up again in the new module image.
 int noalloc_scratch(pm3gpu_ctx* c, unsigned char** base) {
   if (c->device < 0 || c->device >= kNoAllocMaxDevices)
     return fail(c, PM3GPU_INVALID_INPUT, "device ordinal outside the allocation-free path's table");
@@ -1632,6 +1853,16 @@ int noalloc_scratch(pm3gpu_ctx* c, unsigned char** base) {
   return PM3GPU_OK;
 }
 
+}  // namespace
+
+void noalloc_forget(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return;
+  std::lock_guard<std::mutex> lk(g_noalloc_setup_mu);
+  g_noalloc_base[device] = nullptr;
+}
+
+namespace {
+
 int noalloc_run(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz, const pm3gpu_options* o,
                 pm3gpu_result* result, double* charges) {
   std::memset(result, 0, sizeof(*result));
@@ -1646,6 +1877,14 @@ int noalloc_run(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz,
     c->err = p.msg;
     return p.status;
   }
+  if (p.large) {  // pm3gpu_single_point would run the whole-GPU algorithm, which needs allocations
+    char msg[200];
+    std::snprintf(msg, sizeof msg,
+                  "molecule (nao=%d) is at or above the context's whole-GPU threshold (%d); the allocation-free "
+                  "path runs only the one-CTA-per-molecule kernel",
+                  p.nao, c->large_min);
+    return fail(c, PM3GPU_RESOURCE_LIMIT, msg);
+  }
   // the first pass and the stability rungs run_pm3 would try, in its order (scf.rs:599-715)
   JobDesc jobs[kNoAllocMaxJobs];
   Rung rungs[kNoAllocMaxJobs - 1];
@@ -1655,28 +1894,16 @@ int noalloc_run(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz,
   JobDesc& fj = jobs[0];
   fj.mol = 0;
   fj.charge_off = 0;
-  fj.stab = 0;
-  if (o->stability == PM3GPU_STABILITY_ALWAYS && !p.steered) fj.stab = 2;
-  if (o->stability == PM3GPU_STABILITY_AUTO && !p.steered) fj.stab = 1;
+  fj.stab = stability_mode(p, o);
   if (fj.stab) {
-    const int primary = o->guess == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_CORE : PM3GPU_GUESS_SAD;
-    const int other = primary == PM3GPU_GUESS_CORE ? PM3GPU_GUESS_SAD : PM3GPU_GUESS_CORE;
-    const bool closed = !p.use_uhf;
-    const Rung all[7] = {{primary, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                         {other, o->accelerator, 0.0, 0.0, false},
-                         {other, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                         {PM3GPU_GUESS_SYMMETRY_BROKEN, o->accelerator, 0.0, 0.0, false},
-                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, 0.0, 0.0, false},
-                         {PM3GPU_GUESS_SYMMETRY_BROKEN, PM3GPU_ACCEL_NONE, -2.0, 0.0, closed},
-                         {primary, PM3GPU_ACCEL_CDIIS, 0.0, 0.85, closed}};
-    for (const Rung& r : all) {
-      if (r.unrestricted != closed) continue;
+    const int nplan = stability_rungs(p, o, rungs);
+    for (int k = 0; k < nplan; ++k) {
+      const Rung& r = rungs[k];
       JobDesc rj = make_job(p, r.guess, r.accel, r.shift, r.damp, r.unrestricted, 0);
       rj.mol = 0;
       rj.stab = 0;
       rj.nrung = 0;
       rj.charge_off = (long long)(1 + nr) * n_atoms;
-      rungs[nr] = r;
       jobs[1 + nr] = rj;
       ++nr;
     }
@@ -1711,7 +1938,6 @@ int noalloc_run(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz,
   if (rc != PM3GPU_OK) return rc;
 
   const SmemLayout L = make_layout(n_atoms, p.nao, c->smem_optin);
-  CUDA_TRY(c, cudaFuncSetAttribute(scf_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes));
   int per_sm = 0;
   CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scf_batch_kernel, kThreads, L.bytes));
   if (per_sm < 1) return fail(c, PM3GPU_RESOURCE_LIMIT, "SCF kernel does not fit on an SM");
@@ -1777,16 +2003,7 @@ int noalloc_run(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz,
     ++paths;
     JobOut cand = outs[1 + r];
     bool cand_unres = (jobs[1 + r].flags & kJobUhf) != 0;
-    if (!cand.converged) continue;
-    if (rungs[r].unrestricted) {  // a spin-pure unrestricted closed shell is a restricted state
-      if (!(cand.spin_max < 1.0e-8)) continue;
-      cand_unres = false;
-      cand.homo = cand.homo_a;
-      cand.lumo = cand.lumo_a;
-      cand.has_homo = cand.has_homo_a;
-      cand.has_lumo = cand.has_lumo_a;
-    }
-    if (!st.converged || cand.electronic < st.electronic - 1.0e-6) {
+    if (rung_replaces(rungs[r], cand, cand_unres, st)) {
       st = cand;
       st_job = 1 + r;
       st_unres = cand_unres;

@@ -11,14 +11,18 @@ Covered elements: the s/p elements with Z <= 17 except He and Ne, i.e. exactly t
 which the reference takes its closed-form Slater overlap (``src/overlap.rs:269``, MOPAC
 ``diat2``) and its s/p multipole integrals (``src/integrals.rs``).
 
-Usage: python oracle/gen_param_table.py [reference_root]
+Usage: python pm3-rs_b200/gen_param_table.py <reference_root>
+
+(<reference_root> is the root of a pm3-rs checkout; it is required.)
 """
 import csv
 import os
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-OUT = os.path.join(os.path.dirname(__file__), "..", "pm3-rs_b200", "csrc", "pm3_param_table.h")
+if len(sys.argv) != 2:
+    sys.exit("usage: python pm3-rs_b200/gen_param_table.py <pm3-rs checkout root>")
+REF = sys.argv[1]
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "pm3_param_table.h")
 SUPPORTED = [1, 3, 4, 5, 6, 7, 8, 9, 11, 12, 13, 14, 15, 16, 17]
 
 
@@ -37,7 +41,7 @@ def main():
     ele = {int(r["z"]): r for r in rows(os.path.join(REF, "src/data/element_data.csv"))}
     pairs = rows(os.path.join(REF, "src/data/pm3_pair_parameters.csv"))
     out = []
-    out.append("// Generated by oracle/gen_param_table.py -- do not edit by hand.")
+    out.append("// Generated by pm3-rs_b200/gen_param_table.py -- do not edit by hand.")
     out.append("// PM3 raw parameters (MOPAC v23.2.5 parameters_for_PM3_C.F90, parameters_C.F90,")
     out.append("// alpb_and_xfac_pm3.F90; Apache-2.0), as tabulated in pm3-rs src/data/*.csv.")
     out.append("// Published scientific constants; units: eV, Bohr^-1 (zeta), Angstrom^-1 (alpha).")

@@ -65,6 +65,26 @@ class Result(ctypes.Structure):
     ]
 
 
+class Element(ctypes.Structure):
+    """pm3gpu_element: the Pm3Element fields of the s/p path (pm3-rs src/params.rs:20-92)."""
+    _fields_ = [
+        ("z", ctypes.c_int), ("n_orb", ctypes.c_int), ("npq", ctypes.c_int), ("n_gauss", ctypes.c_int),
+        ("u_ss", ctypes.c_double), ("u_pp", ctypes.c_double), ("zeta_s", ctypes.c_double),
+        ("zeta_p", ctypes.c_double), ("beta_s", ctypes.c_double), ("beta_p", ctypes.c_double),
+        ("g_ss", ctypes.c_double), ("g_sp", ctypes.c_double), ("g_pp", ctypes.c_double), ("g_p2", ctypes.c_double),
+        ("h_sp", ctypes.c_double), ("alpha", ctypes.c_double), ("gauss", (ctypes.c_double * 3) * 4),
+        ("core_charge", ctypes.c_double), ("occ_s", ctypes.c_double), ("occ_p", ctypes.c_double),
+        ("eheat_ev", ctypes.c_double), ("e_isol", ctypes.c_double), ("mass", ctypes.c_double),
+        ("dd", ctypes.c_double), ("qq", ctypes.c_double), ("rho0", ctypes.c_double), ("rho1", ctypes.c_double),
+        ("rho2", ctypes.c_double), ("ddp", ctypes.c_double * 7), ("po", ctypes.c_double * 10),
+    ]
+
+
+class Pair(ctypes.Structure):
+    """pm3gpu_pair: PairParams (pm3-rs src/params.rs:104-109)."""
+    _fields_ = [("zi", ctypes.c_int), ("zj", ctypes.c_int), ("alpha", ctypes.c_double), ("x", ctypes.c_double)]
+
+
 # Every symbol include/pm3gpu.h declares.
 EXPORTS = [
     "pm3gpu_default_options", "pm3gpu_supported_element", "pm3gpu_result_sizes",
@@ -76,6 +96,7 @@ EXPORTS = [
     "pm3gpu_set_precision", "pm3gpu_last_large_trace", "pm3gpu_autotune", "pm3gpu_load_tuning",
     "pm3gpu_tuning_choice",
     "pm3gpu_guess_train", "pm3gpu_guess_set_params", "pm3gpu_guess_get_params", "pm3gpu_guess_predict",
+    "pm3gpu_standard_parameters", "pm3gpu_set_parameters",
 ]
 
 _lib = None
@@ -134,8 +155,25 @@ def load() -> ctypes.CDLL:
     L.pm3gpu_last_phase_cycles.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     L.pm3gpu_last_transfer_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
                                              ctypes.POINTER(ctypes.c_longlong)]
+    _P = ctypes.POINTER(ctypes.c_int)
+    L.pm3gpu_standard_parameters.argtypes = [ctypes.POINTER(Element), ctypes.c_int, _P, ctypes.POINTER(Pair),
+                                             ctypes.c_int, _P]
+    L.pm3gpu_set_parameters.argtypes = [ctypes.c_void_p, ctypes.POINTER(Element), ctypes.c_int, ctypes.POINTER(Pair),
+                                        ctypes.c_int]
     _lib = L
     return L
+
+
+def standard_parameters():
+    """Pm3Parameters::standard() of the s/p path as (elements, pairs) ctypes arrays."""
+    L = load()
+    ne, npair = ctypes.c_int(), ctypes.c_int()
+    L.pm3gpu_standard_parameters(None, 0, ctypes.byref(ne), None, 0, ctypes.byref(npair))
+    elems, pairs = (Element * ne.value)(), (Pair * npair.value)()
+    rc = L.pm3gpu_standard_parameters(elems, ne.value, ctypes.byref(ne), pairs, npair.value, ctypes.byref(npair))
+    if rc != OK:
+        raise RuntimeError(f"pm3gpu_standard_parameters failed with status {rc}")
+    return elems, pairs
 
 
 class Context:

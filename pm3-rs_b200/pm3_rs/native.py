@@ -68,9 +68,11 @@ def _ip(a):
 
 
 def run(z, xyz_bohr, opts: _lib.Options, want_density=False, want_mo_energies=False, want_gradient=False,
-        device: int = 0) -> dict:
-    """run_pm3 on one molecule (Bohr in, eV out). Raises ValueError on any non-OK status."""
-    ctx = _lib.default_context(device)
+        device: int = 0, context: _lib.Context | None = None) -> dict:
+    """run_pm3 on one molecule (Bohr in, eV out). Raises ValueError on any non-OK status.
+    `context` selects a context other than the device's default one (e.g. one given its own
+    parameter set with pm3gpu_set_parameters)."""
+    ctx = context if context is not None else _lib.default_context(device)
     lib = ctx.lib
     z = np.ascontiguousarray(z, dtype=np.int32)
     xyz = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(len(z), 3)

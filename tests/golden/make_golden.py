@@ -1,8 +1,8 @@
 """Extract the golden fixtures the parity tests use from the pm3-rs reference tree.
 
-Run in the build container only (it reads the reference checkout, default /root/reference):
+Run where a pm3-rs checkout is available (its root is a required argument):
 
-    python tests/golden/make_golden.py [reference_root]
+    python tests/golden/make_golden.py <reference_root>
 
 Writes tests/golden/mopac_sp.json: the rows of pm3-rs ``tests/data/mopac_oracle.tsv`` (MOPAC
 v23.2.5 PM3 PRECISE NOMM results, the acceptance set of ``tests/mopac_oracle.rs``) whose atoms
@@ -13,7 +13,9 @@ import json
 import os
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py <pm3-rs checkout root>")
+REF = sys.argv[1]
 HERE = os.path.dirname(os.path.abspath(__file__))
 SYM = {"H": 1, "Li": 3, "Be": 4, "B": 5, "C": 6, "N": 7, "O": 8, "F": 9, "Na": 11, "Mg": 12, "Al": 13,
        "Si": 14, "P": 15, "S": 16, "Cl": 17}
