@@ -286,6 +286,17 @@ int pm3gpu_set_precision(pm3gpu_ctx* ctx, int mode);
  * most max_rows rows and returns the total number of rows. */
 int pm3gpu_last_large_trace(pm3gpu_ctx* ctx, double* rows, int max_rows);
 
+/* Checks of every eigensolve of the whole-GPU path (no counterpart in the reference, whose
+ * eigensolver is faer's, src/linalg.rs:221-263). Each eigensolve orthonormalises the occupied
+ * vectors X by Newton-Schulz steps until max |X^T X - I| < 1e-13 (at most 5 steps; a defect still
+ * at or above 1e-11 after them returns PM3GPU_LINALG). With pm3gpu_set_large_checks(ctx, 1) each
+ * eigensolve also measures max |F X - X diag(eps)| over the occupied pairs (one more n x n x
+ * n_occ DGEMM). pm3gpu_last_large_checks copies rows of 6 doubles of the last whole-GPU solve
+ * (pass, iteration, spin, orthonormality defect, eigen residual in eV or NaN when not measured,
+ * Newton-Schulz steps taken), at most max_rows, and returns the number of rows. */
+int pm3gpu_set_large_checks(pm3gpu_ctx* ctx, int on);
+int pm3gpu_last_large_checks(pm3gpu_ctx* ctx, double* rows, int max_rows);
+
 /* Learned initial density (no counterpart in the reference). A 3 x 256 BF16 MLP predicts every
  * atom block and atom-pair block of the initial density from element one-hots, 32 Gaussian
  * distance functions (6 A cutoff) and coordination counts; the SCF starts from the aufbau density
@@ -308,6 +319,13 @@ int pm3gpu_guess_set_params(pm3gpu_ctx* ctx, const float* params, int n_params);
 int pm3gpu_guess_predict(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
                          const double* xyz_bohr, float* features, float* outputs);
 int pm3gpu_guess_get_params(pm3gpu_ctx* ctx, float* params, int n_params);
+/* One forward and backward pass of the network at its current parameters, as a training step
+ * computes it (no parameter update): rows feature rows (64 floats each, rounded to BF16 on entry),
+ * targets and 0/1 masks (8 floats per row). loss = inv_count * sum mask (Y - T)^2; grads
+ * receives dloss/dparams (PM3GPU_GUESS_PARAMS floats, the layout of pm3gpu_guess_get_params).
+ * Exposes the hand-written backward kernels so they can be checked against a restatement. */
+int pm3gpu_guess_gradients(pm3gpu_ctx* ctx, int rows, const float* features, const float* targets,
+                           const float* mask, float inv_count, float* loss, float* grads);
 
 /* Wall-clock ms per phase of the last whole-GPU solve (core, Fock, DIIS, tridiagonalise,
  * eigenvalues, eigenvectors, back-transform, orthonormalise, density), when the context was

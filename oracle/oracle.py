@@ -157,6 +157,26 @@ class OracleError(RuntimeError):
         self.code = code
 
 
+def cut_short(z, xyz_bohr, max_scf, **opts) -> dict:
+    """run_pm3 stopped after `max_scf` SCF iterations (no stability search): the state the
+    reference's loop leaves (src/scf.rs:1290-1316) -- the density of the last iteration, its
+    electronic energy from a fresh Fock matrix and the RMS change of the last step."""
+    z = np.ascontiguousarray(z, dtype=np.int32)
+    xyz = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1, 3)
+    n_ao = nao(z)
+    o = options(max_scf=max_scf, stability=0, **opts)
+    r = Result()
+    charges = np.zeros(len(z))
+    dens = np.zeros((n_ao, n_ao))
+    err = ctypes.create_string_buffer(512)
+    code = lib().oracle_single_point(len(z), _ip(z), _dp(xyz), ctypes.byref(o), ctypes.byref(r), _dp(charges),
+                                     _dp(dens), None, None, err, 512)
+    if code not in (0, 4):
+        raise OracleError(code, err.value.decode())
+    return {"electronic_ev": r.electronic_ev, "last_change": r.last_change, "iterations": r.iterations,
+            "converged": bool(r.converged), "density": dens}
+
+
 def single_point(z, xyz_bohr, want_density=False, want_gradient=False, **opts) -> dict:
     """run_pm3 on one molecule (positions in Bohr); returns a dict of results (eV, Debye)."""
     z = np.ascontiguousarray(z, dtype=np.int32)

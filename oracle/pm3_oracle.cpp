@@ -1838,6 +1838,9 @@ int oracle_single_point(int n_atoms, const int* z, const double* xyz_bohr, const
   res->n_beta = state.n_beta;
   res->last_change = state.last_change;
   if (!state.converged) {
+    // the density of the last iteration still goes out, so that a run cut after k iterations can
+    // be compared with another implementation's first k iterations
+    if (density) std::memcpy(density, state.density.data(), sizeof(double) * (size_t)m.nao * m.nao);
     char msg[160];
     std::snprintf(msg, sizeof msg, "PM3 SCF did not converge after %d iterations (error=%.3e)", state.iterations, state.last_change);
     set_err(errbuf, errlen, msg);

@@ -48,10 +48,11 @@ struct LargeBufs {
   DevBuf Gm, Mm, Tm, Z1, Z2, blocks, Gk;
   DevBuf mh[2], ml[2], c32;  // mixed mode: BF16 hi / lo parts of two operands, FP32 product
   DevBuf gsync, vw, wv;      // cooperative panels: grid barrier, X = [V | W] and Y = [W | V]
+  DevBuf Fchk;               // eigen-residual check: the diagonalised matrix rebuilt
   void release() {
     for (DevBuf* b : {&ao, &sprow, &sroff, &H, &W, &hacc, &dpk, &jacc, &part, &part2, &scal, &P[0], &P[1], &Q[0], &Q[1], &Pt,
                       &F, &G, &hist, &A, &d, &e, &e2, &tau, &lam, &dlam, &blk, &V, &Wp, &y, &wtmp, &ps, &s64, &vcol, &tp, &ctr, &refl, &X, &Xt,
-                      &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk, &mh[0], &mh[1], &ml[0], &ml[1], &c32, &gsync, &vw, &wv})
+                      &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk, &mh[0], &mh[1], &ml[0], &ml[1], &c32, &gsync, &vw, &wv, &Fchk})
       b->release();
     blas_ws.release();
     tg.reset();
@@ -405,6 +406,16 @@ class LargeSolver {
         std::vector<double>& tri = spin == 0 ? R.tri_a : R.tri_b;
         int rc = eigensolve(work_matrix(), kv, occ, lam, dl, iter > 0, &tri);
         if (rc) return rc;
+        double resid = NAN;
+        if (c_->large_checks && occ > 0) {  // max |F X - X diag(lam)| of the occupied pairs
+          CUDA_TRY(c_, B_.Fchk.ensure(8 * nn_));
+          large::combine_kernel<<<grid_for(nn_), large::kBlock, 0, c_->stream>>>(cb, spin == 0 ? Pc : Qc, shift, n,
+                                                                                B_.Fchk.as<double>());
+          ++c_->launches;
+          if ((rc = eigen_residual(B_.Fchk.as<double>(), occ, &resid))) return rc;
+        }
+        c_->lchecks.insert(c_->lchecks.end(), {(double)passes_, (double)iter, (double)spin, last_defect_, resid,
+                                               (double)last_ns_steps_});
         double* Pold = spin == 0 ? Pc : Qc;
         double* Pnew = spin == 0 ? Pn : Qn;
         rc = density_from_x(occ, occ, uhf ? 1.0 : 2.0, Pnew, lowp_iter);
@@ -988,11 +999,15 @@ class LargeSolver {
                                large::kPanel, &one, Xr, (int)K));
     }
     tick(kLgBack);
-    // ---- 5. orthonormalise: X <- X (3I - X^T X) / 2 until max |X^T X - I| < 1e-13
+    // ---- 5. orthonormalise: X <- X (3I - X^T X) / 2 until max |X^T X - I| < 1e-13; at most
+    // kNsSteps updates, the defect measured after each. A defect still at or above kOrthAccept
+    // after the last update is a linear-algebra failure (PM3GPU_LINALG), not a silent result.
     CUDA_TRY(c_, B_.Mm.ensure(8 * K * K));
     CUDA_TRY(c_, B_.Gk.ensure(8 * K * K));
     double* Gk = B_.Gk.as<double>();
-    for (int step = 0; step < 4; ++step) {
+    last_ns_steps_ = 0;
+    last_defect_ = INFINITY;
+    for (int step = 0; step <= kNsSteps; ++step) {
       BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_T, (int)K, (int)K, n, &one, X, (int)K, X, (int)K, &zero,
                                Gk, (int)K));
       large::orth_defect_kernel<<<large::kRedBlocks, large::kBlock, 0, c_->stream>>>(Gk, (int)K, B_.part.as<double>());
@@ -1002,8 +1017,18 @@ class LargeSolver {
       CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
       double defect = 0.0;
       for (double v : mx) defect = std::max(defect, v);
+      last_defect_ = defect;
       if (!(defect < 0.5)) return fail(c_, PM3GPU_LINALG, "large eigensolver: eigenvectors far from orthonormal");
       if (defect < 1.0e-13) break;
+      if (step == kNsSteps) {
+        char msg[160];
+        std::snprintf(msg, sizeof msg,
+                      "large eigensolver: occupied vectors orthonormal only to %.3e after %d Newton-Schulz steps",
+                      defect, kNsSteps);
+        if (!(defect < kOrthAccept)) return fail(c_, PM3GPU_LINALG, msg);
+        break;
+      }
+      ++last_ns_steps_;
       large::ns_matrix_kernel<<<grid_for(K * K), large::kBlock, 0, c_->stream>>>(Gk, B_.Mm.as<double>(), (int)K);
       ++c_->launches;
       // X M (row-major) -> column-major M Xc (M symmetric)
@@ -1013,6 +1038,28 @@ class LargeSolver {
       X = B_.X.as<double>();
     }
     tick(kLgOrth);
+    return PM3GPU_OK;
+  }
+
+  // Largest |F X - X diag(lam)| over the k occupied eigenpairs of the last eigensolve (X = B_.X,
+  // lam = B_.lam), F symmetric row-major: one DGEMM and a max reduction.
+  int eigen_residual(const double* F, int k, double* out) {
+    const int n = n_;
+    const double one = 1.0, zero = 0.0;
+    CUDA_TRY(c_, B_.Xt.ensure(8 * (size_t)n * k));
+    // row-major Y = F X  ->  column-major Yc = Xc F (F symmetric)
+    BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, k, n, n, &one, B_.X.as<double>(), k, F, n, &zero,
+                             B_.Xt.as<double>(), k));
+    large::eig_residual_kernel<<<large::kRedBlocks, large::kBlock, 0, c_->stream>>>(
+        B_.Xt.as<double>(), B_.X.as<double>(), B_.lam.as<double>(), n, k, B_.part.as<double>());
+    ++c_->launches;
+    CUDA_TRY(c_, cudaGetLastError());
+    std::vector<double> mx(large::kRedBlocks);
+    CUDA_TRY(c_, cudaMemcpyAsync(mx.data(), B_.part.p, 8 * mx.size(), cudaMemcpyDeviceToHost, c_->stream));
+    CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+    double r = 0.0;
+    for (double v : mx) r = std::max(r, v);
+    *out = r;
     return PM3GPU_OK;
   }
 
@@ -1072,6 +1119,12 @@ class LargeSolver {
   }
 
   double pivmin_ = 0.0, tnorm_ = 0.0;
+  // Newton-Schulz bookkeeping of the last eigensolve: defect max |X^T X - I| after the last
+  // measured step, and the number of updates applied
+  static constexpr int kNsSteps = 5;
+  static constexpr double kOrthAccept = 1.0e-11;
+  double last_defect_ = 0.0;
+  int last_ns_steps_ = 0;
   std::chrono::steady_clock::time_point t0_ = std::chrono::steady_clock::now();
 
  public:

@@ -364,8 +364,31 @@ __global__ void __launch_bounds__(kBlock) ns_matrix_kernel(const double* G, doub
 __global__ void __launch_bounds__(kBlock) orth_defect_kernel(const double* G, int k, double* partial) {
   const size_t kk = (size_t)k * k;
   double s = 0.0;
-  for (size_t q = blockIdx.x * (size_t)kBlock + threadIdx.x; q < kk; q += (size_t)gridDim.x * kBlock)
-    s = fmax(s, fabs(G[q] - ((q / k) == (q % k) ? 1.0 : 0.0)));
+  for (size_t q = blockIdx.x * (size_t)kBlock + threadIdx.x; q < kk; q += (size_t)gridDim.x * kBlock) {
+    const double v = fabs(G[q] - ((q / k) == (q % k) ? 1.0 : 0.0));
+    s = v == v ? fmax(s, v) : INFINITY;  // fmax would drop a NaN
+  }
+  s = warp_max(s);
+  __shared__ double red[kBlock / 32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < kBlock / 32; ++i) t = fmax(t, red[i]);
+    partial[blockIdx.x] = t;
+  }
+}
+
+// Eigen residual of k computed eigenpairs: per-block partial maxima of |Y - X diag(lam)| with
+// Y = F X (row-major n x k each); NaN counts as infinite.
+__global__ void __launch_bounds__(kBlock) eig_residual_kernel(const double* Y, const double* X, const double* lam,
+                                                               int n, int k, double* partial) {
+  const size_t nk = (size_t)n * k;
+  double s = 0.0;
+  for (size_t q = blockIdx.x * (size_t)kBlock + threadIdx.x; q < nk; q += (size_t)gridDim.x * kBlock) {
+    const double v = fabs(Y[q] - X[q] * lam[q % k]);
+    s = v == v ? fmax(s, v) : INFINITY;
+  }
   s = warp_max(s);
   __shared__ double red[kBlock / 32];
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;

@@ -119,6 +119,8 @@ struct pm3gpu_ctx {
   int precision = PM3GPU_PRECISION_FP64;  // arithmetic of the whole-GPU path's dense products
   bool coop_panels = true;    // Householder panels as cooperative launches (PM3GPU_COOP_PANELS=0: off)
   std::vector<double> ltrace;  // per-iteration record of the last whole-GPU solve (5 per row)
+  bool large_checks = false;   // whole-GPU path: eigen residual of every eigensolve (one more DGEMM)
+  std::vector<double> lchecks;  // per-eigensolve checks of the last whole-GPU solve (6 per row)
   // learned initial density: FP32 master parameters, BF16 copy, Adam moments, gradients
   bool has_guess_model = false;
   long long adam_steps = 0;
@@ -699,6 +701,7 @@ int run_large(pm3gpu_ctx* c, const MolPlan& p, const int32_t* hz, const int32_t*
               double* mo_energies, double* gradient) {
   for (double& t : c->large_ms) t = 0.0;
   c->ltrace.clear();
+  c->lchecks.clear();
   if (!c->blas) BLAS_TRY(c, cublasCreate(&c->blas));
   BLAS_TRY(c, cublasSetStream(c->blas, c->stream));
   if (!c->lbuf) c->lbuf = new LargeBufs();
@@ -905,6 +908,45 @@ int mlp_forward(pm3gpu_ctx* c, const __nv_bfloat16* X, long long rows, float* Y)
   gemm_bf16<false, false>(c, (int)rows, kOut, kHid, in, kHid, P + kW4, kOut, Y, kOut);
   bias_act_kernel<<<gblocks(rows * kOut), 256, 0, c->stream>>>(Y, c->gp.as<float>() + kB4, kOut, rows, nullptr, 0);
   ++c->launches;
+  CUDA_TRY(c, cudaGetLastError());
+  return PM3GPU_OK;
+}
+
+// Forward and backward pass of the network on B rows X (BF16), targets T and masks Mk (FP32):
+// loss = inv_count * sum Mk (Y - T)^2 (its partial sums are added into *accum), gradient of
+// every parameter into c->gg (layout of the parameter vector). dY, dZ are rounded to BF16 for the
+// GEMMs; dH and the parameter gradients are FP32. Needs c->gY, gdY, gdH, gdZ for B rows.
+int mlp_loss_grad(pm3gpu_ctx* c, const __nv_bfloat16* X, const float* T, const float* Mk, int B, float inv_count,
+                  float* accum) {
+  using namespace guess;
+  int rc = mlp_forward(c, X, B, c->gY.as<float>());
+  if (rc != PM3GPU_OK) return rc;
+  float* gg = c->gg.as<float>();
+  const __nv_bfloat16* Pb = c->gpb.as<__nv_bfloat16>();
+  const int woff[3] = {kW1, kW2, kW3}, boff[3] = {kB1, kB2, kB3};
+  loss_kernel<<<gblocks((long long)B * kOut), 256, 0, c->stream>>>(c->gY.as<float>(), T, Mk, (long long)B * kOut,
+                                                                    inv_count, c->gdY.as<__nv_bfloat16>(), accum);
+  // output layer
+  gemm_bf16<true, false>(c, kHid, kOut, B, c->gH[2].as<__nv_bfloat16>(), kHid, c->gdY.as<__nv_bfloat16>(), kOut,
+                         gg + kW4, kOut);
+  colsum_kernel<<<kOut, 256, 0, c->stream>>>(c->gdY.as<__nv_bfloat16>(), kOut, B, gg + kB4);
+  gemm_bf16<false, true>(c, B, kHid, kOut, c->gdY.as<__nv_bfloat16>(), kOut, Pb + kW4, kOut, c->gdH.as<float>(), kHid);
+  c->launches += 4;
+  // hidden layers, last to first
+  for (int l = 2; l >= 0; --l) {
+    dact_kernel<<<gblocks((long long)B * kHid), 256, 0, c->stream>>>(c->gdH.as<float>(), c->gZ[l].as<float>(),
+                                                                     (long long)B * kHid, c->gdZ.as<__nv_bfloat16>());
+    const __nv_bfloat16* in = l > 0 ? c->gH[l - 1].as<__nv_bfloat16>() : X;
+    const int kin = l > 0 ? kHid : kIn;
+    gemm_bf16<true, false>(c, kin, kHid, B, in, kin, c->gdZ.as<__nv_bfloat16>(), kHid, gg + woff[l], kHid);
+    colsum_kernel<<<kHid, 256, 0, c->stream>>>(c->gdZ.as<__nv_bfloat16>(), kHid, B, gg + boff[l]);
+    c->launches += 3;
+    if (l > 0) {
+      gemm_bf16<false, true>(c, B, kHid, kHid, c->gdZ.as<__nv_bfloat16>(), kHid, Pb + woff[l], kHid, c->gdH.as<float>(),
+                             kHid);
+      ++c->launches;
+    }
+  }
   CUDA_TRY(c, cudaGetLastError());
   return PM3GPU_OK;
 }
@@ -1687,8 +1729,6 @@ int pm3gpu_guess_train(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int3
   std::mt19937_64 shuf(seed ^ 0x9e3779b97f4a7c15ull);
   float* gp = c->gp.as<float>();
   float* gg = c->gg.as<float>();
-  const __nv_bfloat16* Pb = c->gpb.as<__nv_bfloat16>();
-  const int woff[3] = {kW1, kW2, kW3}, boff[3] = {kB1, kB2, kB3};
   const int nbatch = (int)(rows / B);
   for (int ep = 0; ep < epochs; ++ep) {
     std::shuffle(idx.begin(), idx.end(), shuf);
@@ -1698,28 +1738,9 @@ int pm3gpu_guess_train(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int3
       gather_rows_kernel<<<gblocks((long long)B * kIn), 256, 0, c->stream>>>(
           c->gidx.as<long long>() + (size_t)bi * B, B, c->gX.as<__nv_bfloat16>(), c->gT.as<float>(), c->gM.as<float>(),
           c->gXb.as<__nv_bfloat16>(), c->gTb.as<float>(), c->gMb.as<float>());
-      rc = mlp_forward(c, c->gXb.as<__nv_bfloat16>(), B, c->gY.as<float>());
+      rc = mlp_loss_grad(c, c->gXb.as<__nv_bfloat16>(), c->gTb.as<float>(), c->gMb.as<float>(), B,
+                         (float)(1.0 / (mask_per_row * B)), accum);
       if (rc != PM3GPU_OK) return rc;
-      loss_kernel<<<gblocks((long long)B * kOut), 256, 0, c->stream>>>(
-          c->gY.as<float>(), c->gTb.as<float>(), c->gMb.as<float>(), (long long)B * kOut,
-          (float)(1.0 / (mask_per_row * B)), c->gdY.as<__nv_bfloat16>(), accum);
-      // output layer
-      gemm_bf16<true, false>(c, kHid, kOut, B, c->gH[2].as<__nv_bfloat16>(), kHid, c->gdY.as<__nv_bfloat16>(), kOut,
-                             gg + kW4, kOut);
-      colsum_kernel<<<kOut, 256, 0, c->stream>>>(c->gdY.as<__nv_bfloat16>(), kOut, B, gg + kB4);
-      gemm_bf16<false, true>(c, B, kHid, kOut, c->gdY.as<__nv_bfloat16>(), kOut, Pb + kW4, kOut, c->gdH.as<float>(), kHid);
-      // hidden layers, last to first
-      for (int l = 2; l >= 0; --l) {
-        dact_kernel<<<gblocks((long long)B * kHid), 256, 0, c->stream>>>(c->gdH.as<float>(), c->gZ[l].as<float>(),
-                                                                         (long long)B * kHid, c->gdZ.as<__nv_bfloat16>());
-        const __nv_bfloat16* in = l > 0 ? c->gH[l - 1].as<__nv_bfloat16>() : c->gXb.as<__nv_bfloat16>();
-        const int kin = l > 0 ? kHid : kIn;
-        gemm_bf16<true, false>(c, kin, kHid, B, in, kin, c->gdZ.as<__nv_bfloat16>(), kHid, gg + woff[l], kHid);
-        colsum_kernel<<<kHid, 256, 0, c->stream>>>(c->gdZ.as<__nv_bfloat16>(), kHid, B, gg + boff[l]);
-        if (l > 0)
-          gemm_bf16<false, true>(c, B, kHid, kHid, c->gdZ.as<__nv_bfloat16>(), kHid, Pb + woff[l], kHid,
-                                 c->gdH.as<float>(), kHid);
-      }
       ++c->adam_steps;
       const float b1 = 0.9f, b2 = 0.999f;
       const float c1 = 1.0f - std::pow(b1, (float)c->adam_steps), c2 = 1.0f - std::pow(b2, (float)c->adam_steps);
@@ -1735,6 +1756,43 @@ int pm3gpu_guess_train(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int3
     }
   }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return PM3GPU_OK;
+}
+
+int pm3gpu_guess_gradients(pm3gpu_ctx* c, int rows, const float* features, const float* targets, const float* mask,
+                           float inv_count, float* loss, float* grads) {
+  using namespace guess;
+  if (!c || rows < 1 || !features || !targets || !mask || !grads || !std::isfinite(inv_count))
+    return fail(c, PM3GPU_INVALID_INPUT, "bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  c->err.clear();
+  if (!c->has_guess_model) return fail(c, PM3GPU_INVALID_INPUT, "no learned guess model");
+  c->launches = 0;
+  const size_t B = (size_t)rows;
+  std::vector<__nv_bfloat16> xb(B * kIn);
+  for (size_t k = 0; k < xb.size(); ++k) xb[k] = __float2bfloat16(features[k]);
+  CUDA_TRY(c, c->gXb.ensure(2 * kIn * B));
+  CUDA_TRY(c, c->gTb.ensure(4 * kOut * B));
+  CUDA_TRY(c, c->gMb.ensure(4 * kOut * B));
+  CUDA_TRY(c, c->gY.ensure(4 * kOut * B));
+  CUDA_TRY(c, c->gdY.ensure(2 * kOut * B));
+  CUDA_TRY(c, c->gdH.ensure(4 * kHid * B));
+  CUDA_TRY(c, c->gdZ.ensure(2 * kHid * B));
+  CUDA_TRY(c, c->gg.ensure(4 * (size_t)kParams));
+  CUDA_TRY(c, c->gpart.ensure(4 * 1024));
+  CUDA_TRY(c, cudaMemcpyAsync(c->gXb.p, xb.data(), 2 * kIn * B, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->gTb.p, targets, 4 * kOut * B, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->gMb.p, mask, 4 * kOut * B, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->gpart.p, 0, 4, c->stream));
+  int rc = mlp_loss_grad(c, c->gXb.as<__nv_bfloat16>(), c->gTb.as<float>(), c->gMb.as<float>(), rows, inv_count,
+                         c->gpart.as<float>());
+  if (rc != PM3GPU_OK) return rc;
+  float l = 0.0f;
+  CUDA_TRY(c, cudaMemcpyAsync(&l, c->gpart.p, 4, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(grads, c->gg.p, 4 * (size_t)kParams, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (loss) *loss = l * inv_count;
   return PM3GPU_OK;
 }
 
@@ -1783,6 +1841,21 @@ int pm3gpu_last_large_trace(pm3gpu_ctx* c, double* rows, int max_rows) {
   std::lock_guard<std::mutex> lk(c->mu);
   const int total = (int)(c->ltrace.size() / 5);
   if (rows && max_rows > 0) std::copy_n(c->ltrace.begin(), 5 * (size_t)std::min(total, max_rows), rows);
+  return total;
+}
+
+int pm3gpu_set_large_checks(pm3gpu_ctx* c, int on) {
+  if (!c) return PM3GPU_INVALID_INPUT;
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->large_checks = on != 0;
+  return PM3GPU_OK;
+}
+
+int pm3gpu_last_large_checks(pm3gpu_ctx* c, double* rows, int max_rows) {
+  if (!c) return 0;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const int total = (int)(c->lchecks.size() / 6);
+  if (rows && max_rows > 0) std::memcpy(rows, c->lchecks.data(), 8 * 6 * (size_t)std::min(total, max_rows));
   return total;
 }
 

@@ -96,7 +96,8 @@ EXPORTS = [
     "pm3gpu_set_precision", "pm3gpu_last_large_trace", "pm3gpu_autotune", "pm3gpu_load_tuning",
     "pm3gpu_tuning_choice",
     "pm3gpu_guess_train", "pm3gpu_guess_set_params", "pm3gpu_guess_get_params", "pm3gpu_guess_predict",
-    "pm3gpu_standard_parameters", "pm3gpu_set_parameters",
+    "pm3gpu_standard_parameters", "pm3gpu_set_parameters", "pm3gpu_guess_gradients",
+    "pm3gpu_set_large_checks", "pm3gpu_last_large_checks",
 ]
 
 _lib = None
@@ -146,12 +147,15 @@ def load() -> ctypes.CDLL:
     L.pm3gpu_load_tuning.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
     L.pm3gpu_tuning_choice.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.pm3gpu_last_large_trace.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
+    L.pm3gpu_set_large_checks.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.pm3gpu_last_large_checks.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     _F = ctypes.POINTER(ctypes.c_float)
     L.pm3gpu_guess_train.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, ctypes.POINTER(Options), ctypes.c_int,
                                      ctypes.c_int, ctypes.c_float, ctypes.c_uint, _F]
     L.pm3gpu_guess_set_params.argtypes = [ctypes.c_void_p, _F, ctypes.c_int]
     L.pm3gpu_guess_get_params.argtypes = [ctypes.c_void_p, _F, ctypes.c_int]
     L.pm3gpu_guess_predict.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, _F, _F]
+    L.pm3gpu_guess_gradients.argtypes = [ctypes.c_void_p, ctypes.c_int, _F, _F, _F, ctypes.c_float, _F, _F]
     L.pm3gpu_last_phase_cycles.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     L.pm3gpu_last_transfer_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
                                              ctypes.POINTER(ctypes.c_longlong)]

@@ -188,10 +188,12 @@ class BatchResult:
         return self.charges[self.offsets[m]:self.offsets[m + 1]]
 
 
-def batch(offsets, z, xyz_bohr, opts=None, want_gradient=False, device: int = 0) -> BatchResult:
+def batch(offsets, z, xyz_bohr, opts=None, want_gradient=False, device: int = 0,
+          context: _lib.Context | None = None) -> BatchResult:
     """run_pm3 over many molecules in one persistent launch. Molecule m owns atoms
-    [offsets[m], offsets[m+1]) of z / xyz_bohr (Bohr). ``opts``: one Options or a list."""
-    ctx = _lib.default_context(device)
+    [offsets[m], offsets[m+1]) of z / xyz_bohr (Bohr). ``opts``: one Options or a list.
+    ``context``: a context other than the device's default one."""
+    ctx = context if context is not None else _lib.default_context(device)
     lib = ctx.lib
     offsets = np.ascontiguousarray(offsets, dtype=np.int32)
     z = np.ascontiguousarray(z, dtype=np.int32)

@@ -10,6 +10,7 @@ import ctypes
 import numpy as np
 import pytest
 
+import guess_mlp_ref as MLP
 from helpers import A2B
 from pm3_rs import _lib, native, workloads
 
@@ -117,3 +118,74 @@ def test_training_lowers_the_loss_and_keeps_results():
     p = np.zeros(NP, np.float32)
     assert ctx.lib.pm3gpu_guess_get_params(ctx.ptr, p.ctypes.data_as(F), NP) == 0
     assert np.all(np.isfinite(p))
+
+
+# ---------------------------------------------------------------- backward pass vs the restatement
+BLOCKS = ["W1", "b1", "W2", "b2", "W3", "b3", "W4", "b4"]
+
+
+def _blocks(g):
+    out, off = {}, 0
+    for li, (fi, fo) in enumerate(MLP.SIZES):
+        out[f"W{li + 1}"] = g[off:off + fi * fo]
+        off += fi * fo
+        out[f"b{li + 1}"] = g[off:off + fo]
+        off += fo
+    return out
+
+
+def test_backward_pass_matches_the_fp64_restatement(random_model):
+    """Every dW / db of one hand-written BF16 backward pass (pm3gpu_guess_gradients) against the
+    FP64 restatement in oracle/guess_mlp_ref.py, which rounds to BF16 at the same points: per
+    block, relative Frobenius error below 2e-3 and largest entry error below 2e-2 of the block's
+    largest entry (what is left is FP32 accumulation order and rare one-ulp BF16 flips)."""
+    ctx, p = random_model
+    mols = [workloads.organic(n, 90 + n) for n in (12, 19, 27)]
+    offs, z, xyz = _pack(mols)
+    feat, _ = _predict(ctx, offs, z, xyz)  # real feature rows (ragged count: not a multiple of 64)
+    rng = np.random.default_rng(8)
+    rows = feat.shape[0]
+    tgt = rng.standard_normal((rows, 8)).astype(np.float32) * 0.3
+    mask = (rng.random((rows, 8)) < 0.7).astype(np.float32)
+    mask[:, 5:] = 0.0
+    inv = np.float32(1.0 / (3.5 * rows))
+    loss = np.zeros(1, np.float32)
+    g = np.zeros(NP, np.float32)
+    rc = ctx.lib.pm3gpu_guess_gradients(ctx.ptr, rows, feat.ctypes.data_as(F), tgt.ctypes.data_as(F),
+                                        mask.ctypes.data_as(F), inv, loss.ctypes.data_as(F), g.ctypes.data_as(F))
+    assert rc == 0, ctx.last_error()
+    ref_loss, ref = MLP.loss_and_grad(p, feat, tgt, mask, float(inv))
+    assert abs(loss[0] - ref_loss) <= 1e-4 * ref_loss
+    got_b, ref_b = _blocks(g.astype(np.float64)), _blocks(ref)
+    for name in BLOCKS:
+        a, b = got_b[name], ref_b[name]
+        assert np.linalg.norm(b) > 0.0, name
+        assert np.linalg.norm(a - b) <= 2e-3 * np.linalg.norm(b), (name, np.linalg.norm(a - b) / np.linalg.norm(b))
+        assert np.abs(a - b).max() <= 2e-2 * np.abs(b).max(), name
+
+
+def test_trained_network_cuts_scf_iterations():
+    """What the trained network gains over the standard (SAD) start: trained on the plain SCF's
+    own converged densities of 1024 organics, it lowers the mean SCF iteration count of 128
+    held-out organics by at least 15%, every molecule converges, and the results equal the
+    standard-guess ones within the parity bars (both runs reach the same fixed point)."""
+    ctx = _lib.Context()
+    try:
+        train = workloads.organic_batch(1024, 5, 40, seed=501)
+        offs, z, xyz = _pack(train)
+        losses = np.zeros(8, np.float32)
+        rc = ctx.lib.pm3gpu_guess_train(ctx.ptr, len(train), offs.ctypes.data_as(I32), z.ctypes.data_as(I32),
+                                        xyz.ctypes.data_as(D), ctypes.byref(native.options()), 8, 1024, 1e-3, 3,
+                                        losses.ctypes.data_as(F))
+        assert rc == 0, ctx.last_error()
+        held = workloads.organic_batch(128, 10, 40, seed=502)
+        offs, z, xyz = _pack(held)
+        std = native.batch(offs, z, xyz, native.options(), context=ctx)
+        lrn = native.batch(offs, z, xyz, native.options(guess=_lib.GUESS_LEARNED), context=ctx)
+        assert np.all(std.status == 0) and np.all(lrn.status == 0)
+        assert np.abs(lrn.heat_of_formation_kcal - std.heat_of_formation_kcal).max() < HOF_TOL
+        it_std, it_lrn = std.iterations.mean(), lrn.iterations.mean()
+        print(f"mean SCF iterations: standard guess {it_std:.2f}, learned guess {it_lrn:.2f}")
+        assert it_lrn <= 0.85 * it_std, (it_std, it_lrn)
+    finally:
+        ctx.close()
