@@ -77,14 +77,29 @@ def cpu_throughput(mols, cores, steps=1, warmup=0, opts=None):
     return rates
 
 
-def molecules(n_mol, seed, workload="organics-4096"):
+def molecules(n_mol, seed, workload="organics-4096", only=None):
     from pm3_rs import workloads
 
     if workload == "radicals-2048":
-        mols = workloads.radical_batch(n_mol, 10, 80, seed=seed)
+        mols = workloads.radical_batch(n_mol, 10, 80, seed=seed, only=only)
     else:
-        mols = workloads.organic_batch(n_mol, 5, 60, seed=seed)
+        mols = workloads.organic_batch(n_mol, 5, 60, seed=seed, only=only)
     return [(z, xyz * A2B) for z, xyz in mols]
+
+
+def rank_molecules(n_per_rank, rank, world, workload="organics-4096", seed=1234):
+    """This rank's part of ONE batch of n_per_rank x world molecules: the batch is partitioned over
+    the ranks by the longest-processing-time rule on a size cost (atoms^3; the atom counts are drawn
+    without building the molecules), and each rank builds only its own molecules. Weak scaling."""
+    from pm3_rs import sharding, workloads
+
+    n = n_per_rank * world
+    if workload == "radicals-2048":
+        sizes = np.random.default_rng(seed).integers(10, 81, n)
+    else:
+        sizes = workloads.organic_batch_sizes(n, 5, 60, seed)
+    parts = sharding.partition_costs(sizes.astype(np.float64) ** 3, world)
+    return molecules(n, seed, workload, only=parts[rank])
 
 
 RADICALS = "radicals-2048: seeded C/H/N/O/S organics of 10-80 atoms minus one H (doublets), UHF PM3 FP64 + analytic gradients, reference default options"
@@ -422,6 +437,226 @@ def water_main(args, rank):
     print(json.dumps(line))
 
 
+def _oracle_water_first_iteration(args):
+    """Oracle SCF of the water cluster cut after one iteration: its time, and the comparison with
+    the GPU's state after one iteration from the same SAD start (density loaded from `path`)."""
+    nw, path, gpu_e, gpu_dp = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from pm3_rs import workloads
+
+    z, xyz = workloads.water_cluster(nw, grid=WATER_GRID)
+    t = time.perf_counter()
+    ref = O.cut_short(z, xyz * A2B, 1)
+    t = time.perf_counter() - t
+    gpu = np.load(path, mmap_mode="r")
+    dmax, fro_g, fro_r = 0.0, 0.0, 0.0
+    for r0 in range(0, gpu.shape[0], 1000):  # in row blocks: two 1.15 GB matrices
+        g, o = np.asarray(gpu[r0:r0 + 1000]), ref["density"][r0:r0 + 1000]
+        dmax = max(dmax, float(np.abs(g - o).max()))
+        fro_g += float((g * g).sum())
+        fro_r += float((o * o).sum())
+    return {"seconds": t, "electronic_ev_oracle": ref["electronic_ev"], "electronic_ev_gpu": gpu_e,
+            "abs_delta_electronic_ev": abs(gpu_e - ref["electronic_ev"]),
+            "rms_density_change_oracle": ref["last_change"], "rms_density_change_gpu": gpu_dp,
+            "max_abs_delta_density": dmax, "frobenius_density_gpu": fro_g ** 0.5, "frobenius_density_oracle": fro_r ** 0.5}
+
+
+def large_record(args, dev, stream):
+    """The 6000-atom half of the metric: one 2000-water cluster (12000 basis functions) on the
+    whole-GPU path, FP64 and mixed (split-BF16 tcgen05 products, FP64 closing iterations) seconds per
+    SCF, the mixed result's heat-of-formation and gradient error against FP64, parity of the first
+    iteration against the CPU oracle at full size, and the CPU oracle's time (setup + 1 and + 2
+    iterations at full size, extrapolated; it runs on the host cores while the GPU solves)."""
+    import ctypes
+    import multiprocessing as mp
+
+    import torch
+
+    from pm3_rs import _lib, native, workloads
+
+    nw = 2000
+    z, xyz = workloads.water_cluster(nw, grid=WATER_GRID)
+    z = np.ascontiguousarray(z, np.int32)
+    x = np.ascontiguousarray(xyz * A2B)
+    n_atoms, n = len(z), 6 * nw
+    I32, D = ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)
+    ctx = _lib.Context(0)
+    lib = ctx.lib
+    lib.pm3gpu_set_stream(ctx.ptr, ctypes.c_void_p(stream.cuda_stream))
+    # warm-up and full-size parity: one SCF iteration from the SAD start, with the eigensolver checks
+    lib.pm3gpu_set_large_checks(ctx.ptr, 1)
+    r1 = _lib.Result()
+    q = np.zeros(n_atoms)
+    dens = np.zeros((n, n))
+    o1 = native.options(max_scf=1, stability=0)
+    rc = lib.pm3gpu_single_point(ctx.ptr, n_atoms, z.ctypes.data_as(I32), x.ctypes.data_as(D), ctypes.byref(o1),
+                                 ctypes.byref(r1), q.ctypes.data_as(D), dens.ctypes.data_as(D), None)
+    if rc != _lib.SCF_NOT_CONVERGED:
+        raise RuntimeError(ctx.last_error())
+    chk = np.zeros((8, 6))
+    nchk = lib.pm3gpu_last_large_checks(ctx.ptr, chk.ctypes.data_as(D), 8)
+    lib.pm3gpu_set_large_checks(ctx.ptr, 0)
+    tmp = tempfile.mkdtemp(prefix="pm3gpu_water_")
+    dpath = os.path.join(tmp, "gpu_iteration1.npy")
+    np.save(dpath, dens)
+    del dens
+    # CPU legs on the host cores (two kept free for the GPU's host thread) while the GPU solves
+    cores = os.cpu_count() or 1
+    threads = max(1, cores - 2)
+    os.environ["OPENBLAS_NUM_THREADS"] = str(threads)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    pool = mp.get_context("spawn").Pool(1)
+    first = pool.apply_async(_oracle_water_first_iteration, ((nw, dpath, r1.electronic_ev, r1.last_change),))
+    second = pool.apply_async(_oracle_water_iters, ((nw, 2),))
+    out = {}
+    for name, mode in (("fp64", _lib.PRECISION_FP64), ("mixed", _lib.PRECISION_MIXED)):
+        lib.pm3gpu_set_precision(ctx.ptr, mode)
+        r, g = _lib.Result(), np.zeros(3 * n_atoms)
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        rc = lib.pm3gpu_gradient(ctx.ptr, n_atoms, z.ctypes.data_as(I32), x.ctypes.data_as(D),
+                                 ctypes.byref(native.options()), ctypes.byref(r), q.ctypes.data_as(D),
+                                 g.ctypes.data_as(D))
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        if rc != 0:
+            raise RuntimeError(ctx.last_error())
+        t = (ctypes.c_double * 8)()
+        lib.pm3gpu_last_timings(ctx.ptr, t, 8)
+        nrow = lib.pm3gpu_last_large_trace(ctx.ptr, None, 0)
+        tr = np.zeros((max(nrow, 1), 5))
+        lib.pm3gpu_last_large_trace(ctx.ptr, tr.ctypes.data_as(D), nrow)
+        out[name] = {"s_per_scf": t[3] * 1e-3, "e2e_s_per_call": s.elapsed_time(e) * 1e-3,
+                     "iterations": r.iterations, "split_bf16_iterations": int(tr[:nrow, 4].sum()),
+                     "heat_of_formation_kcal": r.heat_of_formation_kcal,
+                     "gradient_kcal_per_A": g * (23.06054783061903 / 0.529177210903)}
+    lib.pm3gpu_set_precision(ctx.ptr, _lib.PRECISION_FP64)
+    ctx.close()
+    par = first.get()
+    t2 = second.get()
+    pool.close()
+    pool.join()
+    os.unlink(dpath)
+    os.rmdir(tmp)
+    fp, mx = out["fp64"], out["mixed"]
+    per_iter = max(t2 - par["seconds"], 0.0)
+    setup = max(par["seconds"] - per_iter, 0.0)
+    cpu_total = setup + fp["iterations"] * per_iter
+    return {
+        "workload": "water-2000: 2000 H2O (6000 atoms, 12000 basis functions), RHF PM3, reference default options",
+        "fp64": {k: v for k, v in fp.items() if k != "gradient_kcal_per_A"},
+        "mixed": {k: v for k, v in mx.items() if k != "gradient_kcal_per_A"},
+        "s_per_scf_unit_note": "SCF passes on the device (CUDA events), without the gradient; e2e_s_per_call is the "
+                               "whole pm3gpu_gradient call from host buffers (copies, SCF, gradient)",
+        "mixed_vs_fp64": {"delta_hof_kcal": mx["heat_of_formation_kcal"] - fp["heat_of_formation_kcal"],
+                          "max_gradient_component_error_kcal_per_A": float(np.abs(mx["gradient_kcal_per_A"] -
+                                                                                  fp["gradient_kcal_per_A"]).max()),
+                          "tuned_over_plain_s_per_scf": fp["s_per_scf"] / mx["s_per_scf"] if mx["s_per_scf"] else None},
+        "first_iteration_vs_oracle": {k: v for k, v in par.items() if k != "seconds"},
+        "eigensolver_checks_first_iteration": {"orthonormality_defect": float(chk[0, 3]) if nchk else None,
+                                               "max_abs_F_C_minus_C_eps_ev": float(chk[0, 4]) if nchk else None,
+                                               "newton_schulz_steps": int(chk[0, 5]) if nchk else None},
+        "cpu_baseline": {"value": cpu_total, "unit": "s/SCF", "cores": threads, "kind": "port",
+                         "sample": f"setup + 1 and + 2 iterations at full size ({setup:.1f} s setup, {per_iter:.1f} s per "
+                                   f"iteration), extrapolated to the FP64 run's {fp['iterations']} iterations"},
+        "gpu_over_cpu_fp64": cpu_total / fp["s_per_scf"] if fp["s_per_scf"] else None,
+    }
+
+
+def tuned_arm(args, lib, ctx0, make_slots, measure, plain_opts, gpu_opts, plain, n_mol):
+    """The tuned form of the same workload, timed exactly like the plain arm: the launch choice from
+    the autotuner (calibrated on another sample of the generator), the learned initial density trained
+    before timing on the plain SCF's own converged densities of other molecules of the generator, and
+    mixed precision where the path has it. Reports its rate, the ratio to the plain arm, how far its
+    heats of formation are from the plain ones (same molecules), and the plain single-molecule rate
+    (pm3gpu_single_point one molecule at a time) for context."""
+    import ctypes
+
+    import torch
+
+    from pm3_rs import _lib, native, workloads
+
+    I32, D, F32 = ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float)
+
+    def packed(ms):
+        o, zz, xx = workloads.pack(ms)
+        return np.ascontiguousarray(o, np.int32), np.ascontiguousarray(zz, np.int32), np.ascontiguousarray(xx)
+
+    t0 = time.perf_counter()
+    rad = args.workload == "radicals-2048"
+    c_off, c_z, c_xyz = packed(molecules(256 if rad else 1024, seed=777, workload=args.workload))
+    path = os.path.join(tempfile.mkdtemp(prefix="pm3gpu_tuning_"), f"tuning_{args.workload}.json")
+    if lib.pm3gpu_autotune(ctx0.ptr, len(c_off) - 1, c_off.ctypes.data_as(I32), c_z.ctypes.data_as(I32),
+                           c_xyz.ctypes.data_as(D), ctypes.byref(plain_opts), path.encode()) != 0:
+        raise RuntimeError(ctx0.last_error())
+    tuning = json.load(open(path))
+    n_train = max(64, args.tuned_train // (4 if rad else 1))
+    t_off, t_z, t_xyz = packed(molecules(n_train, seed=9001, workload=args.workload))
+    epochs = 6
+    losses = np.zeros(epochs, np.float32)
+    tctx = _lib.Context(0)
+    if lib.pm3gpu_guess_train(tctx.ptr, len(t_off) - 1, t_off.ctypes.data_as(I32), t_z.ctypes.data_as(I32),
+                              t_xyz.ctypes.data_as(D), ctypes.byref(plain_opts), epochs, 4096, 1e-3, 7,
+                              losses.ctypes.data_as(F32)) != 0:
+        raise RuntimeError(tctx.last_error())
+    params = np.zeros(_lib.GUESS_PARAMS, np.float32)
+    if lib.pm3gpu_guess_get_params(tctx.ptr, params.ctypes.data_as(F32), _lib.GUESS_PARAMS) != 0:
+        raise RuntimeError(tctx.last_error())
+    tctx.close()
+    setup_s = time.perf_counter() - t0
+
+    def setup(c):
+        if lib.pm3gpu_load_tuning(c.ptr, path.encode()) != 0 or \
+                lib.pm3gpu_guess_set_params(c.ptr, params.ctypes.data_as(F32), _lib.GUESS_PARAMS) != 0 or \
+                lib.pm3gpu_set_precision(c.ptr, _lib.PRECISION_MIXED) != 0:
+            raise RuntimeError(c.last_error())
+
+    slots = make_slots(args.inflight, setup)
+    o = native.options(**gpu_opts)
+    o.guess = _lib.GUESS_LEARNED
+    r = measure(slots, o)
+    for sl in slots:
+        sl["ctx"].close()
+    both = (plain["status"] == 0) & (r["status"] == 0)
+    dhf = np.abs(r["hof"][both] - plain["hof"][both])
+    value = r["conv"] / (r["t_dev"] * 1e-3)
+    plain_value = plain["conv"] / (plain["t_dev"] * 1e-3)
+    # the plain path one molecule at a time (the drop-in run_pm3 call), on the first molecules
+    single_n = 128
+    sc = _lib.Context(0)
+    res, q = _lib.Result(), np.zeros(512)
+    conv1 = 0
+    mols1 = molecules(args.n_mol, seed=1234, workload=args.workload, only=range(single_n))
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for zz, xx in mols1:
+        zz = np.ascontiguousarray(zz, np.int32)
+        xx = np.ascontiguousarray(xx)
+        rc = lib.pm3gpu_single_point(sc.ptr, len(zz), zz.ctypes.data_as(I32), xx.ctypes.data_as(D),
+                                     ctypes.byref(plain_opts), ctypes.byref(res), q.ctypes.data_as(D), None, None)
+        conv1 += int(rc == 0)
+    single_rate = conv1 / (time.perf_counter() - t1)
+    sc.close()
+    return {
+        "value": value, "unit": "SCF/s", "e2e": r["e_conv"] / (r["t_host"] * 1e-3),
+        "tuned_over_plain": value / plain_value,
+        "e2e_tuned_over_plain": (r["e_conv"] / r["t_host"]) / (plain["e_conv"] / plain["t_host"]),
+        "max_abs_dhf_kcal_vs_plain": float(dhf.max()) if dhf.size else None,
+        "molecules_dhf_above_0.01_kcal": int((dhf > 0.01).sum()),
+        "converged_fraction": r["conv"] / (n_mol * args.steps),
+        "modes": {"launch": "autotuned (calibration sample: 1024 other molecules of the generator)",
+                  "guess": f"learned, trained before timing on {len(t_off) - 1} other molecules ({epochs} epochs)",
+                  "precision": "mixed (split-BF16 tcgen05 products where the path has them, FP64 closing iterations)"},
+        "setup_seconds": setup_s, "train_loss_per_epoch": [float(v) for v in losses], "tuning": tuning.get("batch"),
+        "gpu_launches": r["launches"], "clocks": r["clocks"],
+        "plain_single_molecule_scf_per_s": single_rate,
+        "single_molecule_sample": f"first {single_n} molecules through pm3gpu_single_point one at a time (wall clock)",
+        "tuned_over_plain_single_molecule": value / single_rate if single_rate else None,
+    }
+
+
 def basis_size(zs):
     return int(sum(1 if int(v) == 1 else 4 for v in zs))
 
@@ -540,9 +775,15 @@ def main():
     ap.add_argument("--guess-params", default=None,
                     help="batched workloads: start every molecule from the learned density of these parameters "
                          "(float32, as written by --save-guess)")
-    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
-                    help="batched workloads: skip the calibration that, before timing, measures the launch choices on a "
-                         "sample of the same generator (another seed; 1024 organics or 256 radicals) and uses the faster")
+    ap.add_argument("--no-tuned", dest="tuned", action="store_false",
+                    help="batched workloads: skip the tuned arm (autotuned launch choice, learned initial density "
+                         "trained before timing, mixed precision where the path has it) reported beside the plain one")
+    ap.add_argument("--tuned-train", type=int, default=8192,
+                    help="tuned arm: molecules (same generator, another seed) whose converged densities train the "
+                         "learned initial density before timing")
+    ap.add_argument("--no-large", dest="large", action="store_false",
+                    help="organics workload: skip the 6000-atom record (2000-water cluster, FP64 and mixed s/SCF, "
+                         "first-iteration parity against the CPU oracle, CPU time extrapolated)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="water-2000 workload: FP64 throughout, or split-BF16 density and commutator products "
                          "with FP64 closing iterations (reports the heat-of-formation and gradient error against FP64)")
@@ -567,7 +808,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        mols = molecules(args.n_mol, seed=1234, workload=args.workload)[: args.cpu_sample]
+        mols = molecules(args.n_mol, seed=1234, workload=args.workload, only=range(min(args.cpu_sample, args.n_mol)))
         rates = cpu_throughput(mols, cores, steps=args.steps, warmup=0, opts=oracle_opts)
         n = sum(r[0] for r in rates)
         t = sum(r[1] for r in rates)
@@ -600,31 +841,15 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
 
-    mols = molecules(args.n_mol, seed=shard_seed(rank), workload=args.workload)
+    mols = rank_molecules(args.n_mol, rank, world, workload=args.workload)
     from pm3_rs import workloads
 
     offs, z, xyz = workloads.pack(mols)
     n_mol, n_atoms = len(mols), len(z)
-    ctx = _lib.Context(local)
-    lib = ctx.lib
+    I32 = ctypes.POINTER(ctypes.c_int32)
+    D = ctypes.POINTER(ctypes.c_double)
+    F32 = ctypes.POINTER(ctypes.c_float)
     stream = torch.cuda.current_stream(dev)
-    lib.pm3gpu_set_stream(ctx.ptr, ctypes.c_void_p(stream.cuda_stream))
-    opts = native.options(**gpu_opts)
-    guess_params = None
-    if args.guess_params:  # learned initial density (the standard-guess pass stays as backup)
-        guess_params = np.fromfile(args.guess_params, dtype=np.float32)
-        opts.guess = _lib.GUESS_LEARNED
-
-    def load_guess(c):
-        if guess_params is not None and c.lib.pm3gpu_guess_set_params(
-                c.ptr, guess_params.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), len(guess_params)) != 0:
-            raise RuntimeError(c.last_error())
-
-    load_guess(ctx)
-    results = (_lib.Result * n_mol)()
-    charges = np.zeros(n_atoms)
-    grads = np.zeros((n_atoms, 3)) if want_grad else None
-    pgr = torch.zeros(3 * n_atoms, dtype=torch.float64).pin_memory() if want_grad else None
     d_z = torch.from_numpy(z).to(dev)
     d_xyz = torch.from_numpy(np.ascontiguousarray(xyz)).to(dev)
     d_off = torch.from_numpy(offs).to(dev)
@@ -632,108 +857,48 @@ def main():
     h_off = np.ascontiguousarray(offs)
     pz = torch.from_numpy(z).pin_memory()
     pxyz = torch.from_numpy(np.ascontiguousarray(xyz)).pin_memory()
-    pq = torch.zeros(n_atoms, dtype=torch.float64).pin_memory()
-    I32 = ctypes.POINTER(ctypes.c_int32)
-    D = ctypes.POINTER(ctypes.c_double)
-    tuning = None
-    if args.autotune:  # calibrate on another sample of the same generator, outside the timed region
-        tmols = molecules(256 if args.workload == "radicals-2048" else 1024, seed=shard_seed(rank, 777),
-                          workload=args.workload)
-        t_off, t_z, t_xyz = workloads.pack(tmols)
-        t_off, t_z = np.ascontiguousarray(t_off, np.int32), np.ascontiguousarray(t_z, np.int32)
-        t_xyz = np.ascontiguousarray(t_xyz)
-        path = os.path.join(tempfile.mkdtemp(prefix="pm3gpu_tuning_"), f"tuning_{args.workload}.json")
-        if lib.pm3gpu_autotune(ctx.ptr, len(tmols), t_off.ctypes.data_as(I32), t_z.ctypes.data_as(I32),
-                               t_xyz.ctypes.data_as(D), ctypes.byref(opts), path.encode()) != 0:
-            raise RuntimeError(ctx.last_error())
-        tuning = json.load(open(path))["batch"]
-
-    def run_device():
-        rc = lib.pm3gpu_batch_device_inputs(ctx.ptr, n_mol, ctypes.c_void_p(d_off.data_ptr()),
-                                            ctypes.c_void_p(d_z.data_ptr()), ctypes.c_void_p(d_xyz.data_ptr()),
-                                            h_off.ctypes.data_as(I32), h_z.ctypes.data_as(I32), ctypes.byref(opts),
-                                            results, charges.ctypes.data_as(D),
-                                            grads.ctypes.data_as(D) if want_grad else None)
-        if rc != 0:
-            raise RuntimeError(ctx.last_error())
-
-    def run_host():
-        rc = lib.pm3gpu_batch(ctx.ptr, n_mol, h_off.ctypes.data_as(I32), ctypes.cast(pz.data_ptr(), I32),
-                              ctypes.cast(pxyz.data_ptr(), D), ctypes.byref(opts), 0, results,
-                              ctypes.cast(pq.data_ptr(), D), ctypes.cast(pgr.data_ptr(), D) if want_grad else None)
-        if rc != 0:
-            raise RuntimeError(ctx.last_error())
-
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     peak = fp64_gemm_peak(dev)
-
     xfer = [0, 0]
+    lib = _lib.load()
 
-    def timed(fn, steps):
-        ms, conv, launches, kern_ms, flops = [], 0, 0, 0.0, 0.0
-        for _ in range(steps):
-            flush.fill_(1.0)
-            torch.cuda.synchronize(dev)
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            fn()
-            e.record(stream)
-            torch.cuda.synchronize(dev)
-            ms.append(s.elapsed_time(e))
-            rv = np.ctypeslib.as_array(results)
-            st = rv["status"]
-            conv += int((st == 0).sum())
-            launches += lib.pm3gpu_last_kernel_launches(ctx.ptr)
-            t = (ctypes.c_double * 8)()
-            lib.pm3gpu_last_timings(ctx.ptr, t, 8)
-            kern_ms += t[5]
-            hb, db = ctypes.c_longlong(), ctypes.c_longlong()
-            lib.pm3gpu_last_transfer_bytes(ctx.ptr, ctypes.byref(hb), ctypes.byref(db))
-            xfer[0], xfer[1] = hb.value, db.value
-            nao, nocc, its = rv["nao"], rv["n_occ"], rv["iterations"]
-            spins = 1.0 + rv["unrestricted"].astype(np.float64)
-            flops += scf_flops(nao[st == 0], nocc[st == 0], its[st == 0] * spins[st == 0])
-        return ms, conv, launches, kern_ms, flops
-
-    # Batches in flight: `inflight` contexts, each with its own stream, result buffers and host
-    # thread (ctypes releases the GIL inside the library call), so the tail of one batch (the last
-    # single-CTA jobs) overlaps the bulk of the next. Every step is still one full pass over the
-    # whole batch; the timed region spans all K steps on the device.
-    slots = []
-    if args.inflight > 1:
-        for k in range(args.inflight):
-            c = ctx if k == 0 else _lib.Context(local)
-            if k > 0 and tuning is not None and lib.pm3gpu_load_tuning(c.ptr, path.encode()) != 0:
-                raise RuntimeError(c.last_error())
-            if k > 0:
-                load_guess(c)
+    def make_slots(n, setup=None):
+        """`n` batches in flight: contexts, each with its own stream, result buffers and host thread
+        (ctypes releases the GIL inside the library call)."""
+        out = []
+        for _ in range(max(1, n)):
+            c = _lib.Context(local)
+            if setup:
+                setup(c)
             st = torch.cuda.Stream(dev)
             lib.pm3gpu_set_stream(c.ptr, ctypes.c_void_p(st.cuda_stream))
-            slots.append({"ctx": c, "stream": st, "results": (_lib.Result * n_mol)(), "charges": np.zeros(n_atoms),
-                          "grads": np.zeros((n_atoms, 3)) if want_grad else None,
-                          "pq": torch.zeros(n_atoms, dtype=torch.float64).pin_memory(),
-                          "pgr": torch.zeros(3 * n_atoms, dtype=torch.float64).pin_memory() if want_grad else None})
+            out.append({"ctx": c, "stream": st, "results": (_lib.Result * n_mol)(), "charges": np.zeros(n_atoms),
+                        "grads": np.zeros((n_atoms, 3)) if want_grad else None,
+                        "pq": torch.zeros(n_atoms, dtype=torch.float64).pin_memory(),
+                        "pgr": torch.zeros(3 * n_atoms, dtype=torch.float64).pin_memory() if want_grad else None})
+        return out
 
-    def run_slot(sl, host):
+    def run_slot(sl, host, o):
         c, res = sl["ctx"], sl["results"]
         if host:
             rc = lib.pm3gpu_batch(c.ptr, n_mol, h_off.ctypes.data_as(I32), ctypes.cast(pz.data_ptr(), I32),
-                                  ctypes.cast(pxyz.data_ptr(), D), ctypes.byref(opts), 0, res,
+                                  ctypes.cast(pxyz.data_ptr(), D), ctypes.byref(o), 0, res,
                                   ctypes.cast(sl["pq"].data_ptr(), D),
                                   ctypes.cast(sl["pgr"].data_ptr(), D) if want_grad else None)
         else:
             rc = lib.pm3gpu_batch_device_inputs(c.ptr, n_mol, ctypes.c_void_p(d_off.data_ptr()),
                                                 ctypes.c_void_p(d_z.data_ptr()), ctypes.c_void_p(d_xyz.data_ptr()),
-                                                h_off.ctypes.data_as(I32), h_z.ctypes.data_as(I32), ctypes.byref(opts),
+                                                h_off.ctypes.data_as(I32), h_z.ctypes.data_as(I32), ctypes.byref(o),
                                                 res, sl["charges"].ctypes.data_as(D),
                                                 sl["grads"].ctypes.data_as(D) if want_grad else None)
         if rc != 0:
             raise RuntimeError(c.last_error())
 
-    def timed_inflight(host, steps, stagger=0.0):
-        """K steps over the slots; slot k submits its first batch k * stagger seconds after the
-        timed region opens (the earlier slots keep the GPU busy meanwhile), so that one batch's
-        bulk fills the SMs the previous batch's last jobs leave idle."""
+    def timed_inflight(slots, o, host, steps, stagger=0.0):
+        """K steps over the slots (each step one full pass over the batch); slot k submits its first
+        batch k * stagger seconds after the timed region opens, then back to back, so that one batch's
+        bulk fills the SMs the previous batch's last jobs leave idle. Device time (CUDA events) spans
+        all K steps."""
         import threading
 
         flush.fill_(1.0)
@@ -742,7 +907,7 @@ def main():
         s.record(stream)
         for sl in slots:
             sl["stream"].wait_event(s)
-        acc = [[0, 0, 0.0] for _ in slots]  # converged, launches, flops
+        acc = [[0, 0, 0.0, 0.0] for _ in slots]  # converged, launches, flops, kernel ms
         errs = []
 
         def worker(k):
@@ -751,13 +916,16 @@ def main():
                 if stagger > 0.0:
                     time.sleep(k * stagger)
                 for _ in range(k, steps, len(slots)):
-                    run_slot(sl, host)
+                    run_slot(sl, host, o)
                     res = np.ctypeslib.as_array(sl["results"])  # a view: no per-molecule Python work
                     ok = res["status"] == 0
                     acc[k][0] += int(ok.sum())
                     acc[k][1] += lib.pm3gpu_last_kernel_launches(sl["ctx"].ptr)
                     its = res["iterations"][ok] * (1.0 + res["unrestricted"][ok])
                     acc[k][2] += scf_flops(res["nao"][ok], res["n_occ"][ok], its)
+                    t = (ctypes.c_double * 8)()
+                    lib.pm3gpu_last_timings(sl["ctx"].ptr, t, 8)
+                    acc[k][3] += t[5]
                     hb, db = ctypes.c_longlong(), ctypes.c_longlong()
                     lib.pm3gpu_last_transfer_bytes(sl["ctx"].ptr, ctypes.byref(hb), ctypes.byref(db))
                     xfer[0], xfer[1] = hb.value, db.value
@@ -777,88 +945,113 @@ def main():
             stream.wait_event(ev)
         e.record(stream)
         torch.cuda.synchronize(dev)
-        total = s.elapsed_time(e)
-        return total, sum(a[0] for a in acc), sum(a[1] for a in acc), sum(a[2] for a in acc)
+        return (s.elapsed_time(e), sum(a[0] for a in acc), sum(a[1] for a in acc), sum(a[2] for a in acc),
+                sum(a[3] for a in acc))
 
-    if slots:
-        timed_inflight(False, max(args.warmup, len(slots)))  # W warm-up steps, spread over the slots
+    def measure(slots, o):
+        """Warm-up (W steps), then K device-resident steps (clocks sampled) and K host-API steps."""
+        timed_inflight(slots, o, False, max(args.warmup, len(slots)))
         t0 = time.perf_counter()
-        run_slot(slots[0], False)  # one batch alone: the submission interval of the slots
-        stagger = (time.perf_counter() - t0) / len(slots)
+        run_slot(slots[0], False, o)  # one batch alone: the submission interval of the slots
+        stagger = (time.perf_counter() - t0) / len(slots) if len(slots) > 1 else 0.0
         if dist:
             dist.barrier()
         torch.cuda.synchronize(dev)
         with ClockSampler(gpu_uuid(local)) as clk:
-            t_dev, conv, launches, flops = timed_inflight(False, args.steps, stagger)
+            t_dev, conv, launches, flops, kern_ms = timed_inflight(slots, o, False, args.steps, stagger)
         clocks = clk.summary()
-        ms, kern_ms = [t_dev], t_dev  # overlapped batches: the roofline uses the whole device time
-        timed_inflight(True, len(slots))
+        hof = np.ctypeslib.as_array(slots[0]["results"])["heat_of_formation_kcal"].copy()
+        st = np.ctypeslib.as_array(slots[0]["results"])["status"].copy()
+        timed_inflight(slots, o, True, len(slots))
         if dist:
             dist.barrier()
-        t_host, e_conv, _, _ = timed_inflight(True, args.steps, stagger)
-        e_ms = [t_host]
-        h2d, d2h = xfer
-        results = slots[0]["results"]
-    else:
-        for _ in range(args.warmup):
-            run_device()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-        with ClockSampler(gpu_uuid(local)) as clk:
-            ms, conv, launches, kern_ms, flops = timed(run_device, args.steps)
-        clocks = clk.summary()
-        for _ in range(max(1, args.warmup // 2)):
-            run_host()
-        if dist:
-            dist.barrier()
-        e_ms, e_conv, _, _, _ = timed(run_host, args.steps)
-        h2d, d2h = xfer
-    tot = sum(ms)
-    e_tot = sum(e_ms)
-    tot, e_tot, conv, e_conv = reduce_over_ranks(tot, e_tot, conv, e_conv, dist, dev)
+        t_host, e_conv, _, _, _ = timed_inflight(slots, o, True, args.steps, stagger)
+        return {"t_dev": t_dev, "conv": conv, "launches": launches, "flops": flops, "kern_ms": kern_ms,
+                "t_host": t_host, "e_conv": e_conv, "clocks": clocks, "stagger": stagger, "hof": hof, "status": st,
+                "h2d": xfer[0], "d2h": xfer[1]}
+
+    # ------------------------------------------------------------ plain arm: the headline value
+    opts = native.options(**gpu_opts)
+    guess_params = None
+    if args.guess_params:  # learned initial density (the standard-guess pass stays as backup)
+        guess_params = np.fromfile(args.guess_params, dtype=np.float32)
+        opts.guess = _lib.GUESS_LEARNED
+
+    def plain_setup(c):
+        if guess_params is not None and lib.pm3gpu_guess_set_params(
+                c.ptr, guess_params.ctypes.data_as(F32), len(guess_params)) != 0:
+            raise RuntimeError(c.last_error())
+
+    plain_slots = make_slots(args.inflight, plain_setup)
+    plain = measure(plain_slots, opts)
+
+    # ------------------------------------------------------------ tuned arm (one GPU only)
+    tuned = None
+    if world == 1 and args.tuned:
+        tuned = tuned_arm(args, lib, plain_slots[0]["ctx"], make_slots, measure, opts, gpu_opts, plain, n_mol)
+    for sl in plain_slots:
+        sl["ctx"].close()
+
+    tot, e_tot, conv, e_conv = reduce_over_ranks(plain["t_dev"], plain["t_host"], plain["conv"], plain["e_conv"], dist,
+                                                 dev)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
     value = conv / (tot * 1e-3)
     e2e = e_conv / (e_tot * 1e-3)
-    achieved = flops / (kern_ms * 1e-3) / 1e12 if kern_ms > 0 else None
+    kern_ms = plain["t_dev"] if len(plain_slots) > 1 else plain["kern_ms"]
+    achieved = plain["flops"] / (kern_ms * 1e-3) / 1e12 if kern_ms > 0 else None
     line = {
         "metric": METRIC, "value": value, "unit": "SCF/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc, "molecules_per_step_per_gpu": n_mol, "parallelism": f"dp{world}",
-                   "l2": ("flushed before the overlapped steps (512 MiB write); per-CTA workspaces (> 126 MB) exceed L2"
-                          if slots else "flushed between steps (512 MiB write)"),
+        "config": {"workload": desc, "arm": "plain FP64: reference default options and guess, built-in launch choice",
+                   "molecules_per_step_per_gpu": n_mol, "parallelism": f"dp{world}",
+                   "sharding": ("one batch of molecules x ranks split by the longest-processing-time rule on atoms^3"
+                                if world > 1 else "one GPU"),
+                   "l2": "flushed before the timed steps (512 MiB write); per-CTA workspaces (> 126 MB) exceed L2",
                    "batches_in_flight": max(1, args.inflight),
                    "guess": f"learned ({args.guess_params})" if guess_params is not None else "reference default (SAD)",
-                   "submission": (f"slot k submits its first batch k x {1e3 * stagger:.0f} ms into the timed region "
-                                  "(one batch time / slots), then back to back") if slots else "one batch at a time",
-                   "converged_fraction": conv / (n_mol * args.steps * world),
-                   "tuning": tuning or "built-in launch choice (--no-autotune)"},
-        "e2e": {"value": e2e, "unit": "SCF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches,
-        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                   "submission": (f"slot k submits its first batch k x {1e3 * plain['stagger']:.0f} ms into the timed "
+                                  "region (one batch time / slots), then back to back")
+                   if args.inflight > 1 else "one batch at a time",
+                   "converged_fraction": conv / (n_mol * args.steps * world)},
+        "e2e": {"value": e2e, "unit": "SCF/s", "h2d_bytes_per_step": plain["h2d"], "d2h_bytes_per_step": plain["d2h"]},
+        "gpu_launches": plain["launches"],
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": (achieved / peak) if achieved else None,
                      "traffic": DRAM_BYTES_PER_MOLECULE * n_mol,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one scf_batch_kernel launch "
+                                       "over 256 molecules of this workload at the same launch choice, scaled by "
+                                       "molecules per launch",
                      "kernel": "scf_batch_kernel", "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run",
-                     "flops_per_step": flops / args.steps, "kernel_ms_per_step": kern_ms / args.steps},
-        "clocks": clocks,
+                     "flops_per_step": plain["flops"] / args.steps, "kernel_ms_per_step": kern_ms / args.steps},
+        "clocks": plain["clocks"],
     }
+    if tuned:
+        line["tuned"] = tuned
     if args.phases:
-        run_device()
+        os.environ["PM3GPU_PROFILE"] = "1"
+        pc = _lib.Context(local)
+        lib.pm3gpu_set_stream(pc.ptr, ctypes.c_void_p(stream.cuda_stream))
+        sl = {"ctx": pc, "results": (_lib.Result * n_mol)(), "charges": np.zeros(n_atoms),
+              "grads": np.zeros((n_atoms, 3)) if want_grad else None}
+        run_slot(sl, False, opts)
         cyc = (ctypes.c_double * 16)()
-        k = lib.pm3gpu_last_phase_cycles(ctx.ptr, cyc, 16)
+        k = lib.pm3gpu_last_phase_cycles(pc.ptr, cyc, 16)
         tot_c = sum(cyc[i] for i in range(k)) or 1.0
         print(json.dumps({"phase_share": {PHASES[i]: round(cyc[i] / tot_c, 4) for i in range(min(k, len(PHASES)))},
                           "cta_cycles": tot_c}), file=sys.stderr)
+        pc.close()
     if world == 1 and not args.no_cpu_baseline:
         sample = mols[: args.cpu_sample]
         r = cpu_throughput(sample, os.cpu_count() or 1, steps=1, opts=oracle_opts)
         line["cpu_baseline"] = {"value": r[0][0] / r[0][1], "unit": "SCF/s", "cores": os.cpu_count(),
                                 "kind": "port",
                                 "sample": f"first {len(sample)} of the {n_mol} molecules, one oracle process per core"}
+    if world == 1 and args.large and args.workload == "organics-4096":
+        line["large_6k"] = large_record(args, dev, stream)
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

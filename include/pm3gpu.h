@@ -226,8 +226,10 @@ int pm3gpu_fock(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const double* xy
                 const double* p_tot, const double* p_alpha, const double* p_beta, double* f_alpha,
                 double* f_beta);
 
-/* Phase timings of the last call (milliseconds, CUDA events): [0] upload, [1] first SCF
- * pass, [2] stability-search pass, [3] unused, [4] total, [5] time inside the SCF kernels.
+/* Phase timings of the last call (milliseconds, CUDA events): [0] upload, [1] the batched launch
+ * (first passes and stability rungs of the per-CTA molecules), [2] selection, whole-GPU molecules
+ * and gradients, [3] the SCF passes of the whole-GPU molecules alone (first pass and stability
+ * rungs, no gradient), [4] total, [5] time inside the batched SCF kernel.
  * Returns the count written. */
 int pm3gpu_last_timings(pm3gpu_ctx* ctx, double* ms, int max_entries);
 
@@ -274,10 +276,19 @@ int pm3gpu_tuning_choice(pm3gpu_ctx* ctx, int kind, int size);
  * tensor-core GEMMs (x = hi + lo, products hi*hi + hi*lo + lo*hi, FP32 accumulation) while the
  * density is far from converged, then closes the SCF with FP64 iterations: integrals, Fock build,
  * eigensolver, DIIS solve, energies and gradients stay FP64, and only an FP64 iteration can pass
- * the convergence test. The per-CTA path (n <= 256) is FP64 in both modes. Default FP64. */
+ * the convergence test. The per-CTA path (n <= 256) is FP64 in both modes. Default FP64.
+ * The split products run on a hand-written tcgen05 kernel (see pm3gpu_split_gemm). */
 #define PM3GPU_PRECISION_FP64 0
 #define PM3GPU_PRECISION_MIXED 1
 int pm3gpu_set_precision(pm3gpu_ctx* ctx, int mode);
+
+/* The mixed mode's split-BF16 product by itself (no counterpart in the reference): out (m x n,
+ * row-major FP32) = A B^T for A (m x k, leading dimension lda) and B (n x k, ldb), row-major FP64
+ * host arrays, each operand split into BF16 hi + lo and the products hi hi + hi lo + lo hi
+ * accumulated in FP32 on the tcgen05 tensor cores in one launch. Exposes the kernel the
+ * whole-GPU path's mixed mode runs, for checks against an FP64 product. */
+int pm3gpu_split_gemm(pm3gpu_ctx* ctx, int m, int n, int k, const double* a, int lda, const double* b, int ldb,
+                      float* out);
 
 /* Per-iteration convergence record of the last whole-GPU solve (no counterpart in the
  * reference, whose PM3_TIMING trace, scf.rs:1206-1296, prints phase times only): rows of 5 doubles (pass: 1 = first SCF, 2.. = stability rungs;

@@ -49,11 +49,14 @@ struct LargeBufs {
   DevBuf mh[2], ml[2], c32;  // mixed mode: BF16 hi / lo parts of two operands, FP32 product
   DevBuf gsync, vw, wv;      // cooperative panels: grid barrier, X = [V | W] and Y = [W | V]
   DevBuf Fchk;               // eigen-residual check: the diagonalised matrix rebuilt
+  DevBuf tcerr;              // error flag of the tcgen05 split-BF16 GEMM
+  bool tcerr_zeroed = false;
   void release() {
     for (DevBuf* b : {&ao, &sprow, &sroff, &H, &W, &hacc, &dpk, &jacc, &part, &part2, &scal, &P[0], &P[1], &Q[0], &Q[1], &Pt,
                       &F, &G, &hist, &A, &d, &e, &e2, &tau, &lam, &dlam, &blk, &V, &Wp, &y, &wtmp, &ps, &s64, &vcol, &tp, &ctr, &refl, &X, &Xt,
-                      &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk, &mh[0], &mh[1], &ml[0], &ml[1], &c32, &gsync, &vw, &wv, &Fchk})
+                      &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk, &mh[0], &mh[1], &ml[0], &ml[1], &c32, &gsync, &vw, &wv, &Fchk, &tcerr})
       b->release();
+    tcerr_zeroed = false;
     blas_ws.release();
     tg.reset();
   }
@@ -620,10 +623,11 @@ class LargeSolver {
   // E = F P - P F (scf.rs:1039-1054): row-major F P is cuBLAS's column-major P F.
   // Mixed mode (lowp) takes the product from split-BF16 tensor-core GEMMs with FP32 accumulation.
   int commutator(const double* F, const double* P, double* E, bool lowp = false) {
-    if (lowp) {
+    if (lowp) {  // C = F P^T = F P (P symmetric), both operands K-major rows
       int rc;
-      if ((rc = split(P, nn_, 0)) || (rc = split(F, nn_, 1)) ||
-          (rc = gemm_split(CUBLAS_OP_N, CUBLAS_OP_N, n_, n_, n_, n_, 0, 1)))
+      const int ldp = (n_ + 7) & ~7;
+      if ((rc = split(F, n_, n_, n_, ldp, 0)) || (rc = split(P, n_, n_, n_, ldp, 1)) ||
+          (rc = gemm_split(n_, n_, n_, ldp, 0, 1)))
         return rc;
       return combine_transpose(E, 1.0, -1.0);
     }
@@ -639,11 +643,11 @@ class LargeSolver {
       CUDA_TRY(c_, cudaMemsetAsync(P, 0, 8 * nn_, c_->stream));
       return PM3GPU_OK;
     }
-    if (lowp) {  // both operands are X: one split; the result is symmetrised
+    if (lowp) {  // C = X X^T over the first k columns: one split; the result is symmetrised
       const double* X = B_.X.as<double>();
+      const int ldp = (k + 7) & ~7;
       int rc;
-      if ((rc = split(X, (size_t)n_ * ld, 0)) || (rc = gemm_split(CUBLAS_OP_T, CUBLAS_OP_N, n_, k, ld, ld, 0, 0)))
-        return rc;
+      if ((rc = split(X, n_, k, ld, ldp, 0)) || (rc = gemm_split(n_, n_, k, ldp, 0, 0))) return rc;
       return combine_transpose(P, 0.5 * w, 0.5 * w);
     }
     const double zero = 0.0;
@@ -652,25 +656,38 @@ class LargeSolver {
     return PM3GPU_OK;
   }
 
-  // Split x (cnt doubles) into the BF16 hi / lo pair of operand slot s.
-  int split(const double* x, size_t cnt, int s) {
+  // Split the rows x cols matrix x (leading dimension ldx) into the BF16 hi / lo pair of operand
+  // slot s, stored with leading dimension ldo (a multiple of 8, zero beyond cols).
+  int split(const double* x, int rows, int cols, int ldx, int ldo, int s) {
+    const size_t cnt = (size_t)rows * ldo;
     CUDA_TRY(c_, B_.mh[s].ensure(2 * cnt));
     CUDA_TRY(c_, B_.ml[s].ensure(2 * cnt));
-    large::split_bf16_kernel<<<grid_for(cnt), large::kBlock, 0, c_->stream>>>(x, B_.mh[s].as<__nv_bfloat16>(),
-                                                                             B_.ml[s].as<__nv_bfloat16>(), cnt);
+    large::split_pad_kernel<<<grid_for(cnt), large::kBlock, 0, c_->stream>>>(
+        x, rows, cols, ldx, B_.mh[s].as<__nv_bfloat16>(), B_.ml[s].as<__nv_bfloat16>(), ldo);
     ++c_->launches;
     CUDA_TRY(c_, cudaGetLastError());
     return PM3GPU_OK;
   }
-  // c32 = op(A) op(B), column-major m x m with inner dimension k, A and B the split operands of
-  // slots sa and sb: hi lo + lo hi first, then hi hi, all accumulated in FP32 on the tensor cores.
-  int gemm_split(cublasOperation_t ta, cublasOperation_t tb, int m, int k, int lda, int ldb, int sa, int sb) {
-    CUDA_TRY(c_, B_.c32.ensure(4 * (size_t)m * m));
-    const void* term[3][2] = {{B_.mh[sa].p, B_.ml[sb].p}, {B_.ml[sa].p, B_.mh[sb].p}, {B_.mh[sa].p, B_.mh[sb].p}};
-    const float one = 1.0f, zero = 0.0f;
-    for (int t = 0; t < 3; ++t)
-      BLAS_TRY(c_, cublasGemmEx(blas(), ta, tb, m, m, k, &one, term[t][0], CUDA_R_16BF, lda, term[t][1], CUDA_R_16BF, ldb,
-                                t == 0 ? &zero : &one, B_.c32.p, CUDA_R_32F, m, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT));
+  // c32 (m x m row-major FP32) = A B^T with A the split operand of slot sa and B that of slot sb
+  // (m x k each, leading dimension ld): hi hi + hi lo + lo hi accumulated in FP32 in tensor memory
+  // by the hand-written tcgen05 kernel (tc_gemm.cuh), one launch.
+  int gemm_split(int m, int m2, int k, int ld, int sa, int sb) {
+    CUDA_TRY(c_, B_.c32.ensure(4 * (size_t)m * m2));
+    CUDA_TRY(c_, B_.tcerr.ensure(sizeof(int)));
+    if (!B_.tcerr_zeroed) {
+      CUDA_TRY(c_, cudaMemsetAsync(B_.tcerr.p, 0, sizeof(int), c_->stream));
+      B_.tcerr_zeroed = true;
+    }
+    if (!tc::launch_split_gemm(m, m2, k, B_.mh[sa].as<__nv_bfloat16>(), B_.ml[sa].as<__nv_bfloat16>(), ld,
+                               B_.mh[sb].as<__nv_bfloat16>(), B_.ml[sb].as<__nv_bfloat16>(), ld, B_.c32.as<float>(), m2,
+                               B_.tcerr.as<int>(), c_->stream))
+      return fail(c_, PM3GPU_CUDA_ERROR, "split-BF16 GEMM: tensor map or kernel attribute could not be set");
+    ++c_->launches;
+    CUDA_TRY(c_, cudaGetLastError());
+    int flag = 0;
+    CUDA_TRY(c_, cudaMemcpyAsync(&flag, B_.tcerr.p, sizeof(int), cudaMemcpyDeviceToHost, c_->stream));
+    CUDA_TRY(c_, cudaStreamSynchronize(c_->stream));
+    if (flag) return fail(c_, PM3GPU_CUDA_ERROR, "split-BF16 GEMM: a pipeline wait in the kernel ran out");
     return PM3GPU_OK;
   }
   // out = a c32 + b c32^T in FP64 (row-major n x n).

@@ -305,6 +305,21 @@ __global__ void __launch_bounds__(kBlock) split_bf16_kernel(const double* __rest
     lo[k] = __double2bfloat16(v - (double)__bfloat162float(h));
   }
 }
+// The same split of a row-major rows x cols matrix (leading dimension ldx) into hi / lo copies with
+// leading dimension ldo >= cols, the columns beyond cols zero (TMA wants 16-byte rows).
+__global__ void __launch_bounds__(kBlock) split_pad_kernel(const double* __restrict__ x, int rows, int cols, int ldx,
+                                                           __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
+                                                           int ldo) {
+  const size_t cnt = (size_t)rows * ldo;
+  for (size_t k = blockIdx.x * (size_t)kBlock + threadIdx.x; k < cnt; k += (size_t)gridDim.x * kBlock) {
+    const size_t r = k / ldo;
+    const int c = (int)(k - r * ldo);
+    const double v = c < cols ? x[r * ldx + c] : 0.0;
+    const __nv_bfloat16 h = __double2bfloat16(v);
+    hi[k] = h;
+    lo[k] = __double2bfloat16(v - (double)__bfloat162float(h));
+  }
+}
 // out[i][j] = a C[i][j] + b C[j][i] (row-major n x n, C in FP32, out in FP64): the commutator's
 // antisymmetrisation (a = 1, b = -1) and the density's symmetrisation (a = b = w / 2). One block
 // per 32 x 32 output tile; the mirrored tile is read through shared memory so both reads and the

@@ -20,6 +20,7 @@
 #include "panel_coop.cuh"
 #include "guess_mlp.cuh"
 #include "scf_job.cuh"
+#include "tc_gemm.cuh"
 
 using namespace pm3gpu;
 
@@ -119,6 +120,7 @@ struct pm3gpu_ctx {
   int precision = PM3GPU_PRECISION_FP64;  // arithmetic of the whole-GPU path's dense products
   bool coop_panels = true;    // Householder panels as cooperative launches (PM3GPU_COOP_PANELS=0: off)
   std::vector<double> ltrace;  // per-iteration record of the last whole-GPU solve (5 per row)
+  DevBuf tcbuf[7];             // pm3gpu_split_gemm: A, B (FP64), A hi / lo, B hi / lo, C; tcerr
   bool large_checks = false;   // whole-GPU path: eigen residual of every eigensolve (one more DGEMM)
   std::vector<double> lchecks;  // per-eigensolve checks of the last whole-GPU solve (6 per row)
   // learned initial density: FP32 master parameters, BF16 copy, Adam moments, gradients
@@ -725,6 +727,7 @@ int run_large(pm3gpu_ctx* c, const MolPlan& p, const int32_t* hz, const int32_t*
   const JobDesc fj = p.steered ? make_job(p, o->guess, o->accelerator, o->level_shift_ev, o->damping, false, 0)
                                : make_job(p, o->guess, o->accelerator, 0.0, 0.0, false, 0);
   LargeRun st;
+  CUDA_TRY(c, cudaEventRecord(c->kev[0], c->stream));  // the SCF passes alone (timings[3])
   rc = S.scf(fj, st);
   if (rc != PM3GPU_OK) return rc;
   if ((rc = save(st)) != PM3GPU_OK) return rc;
@@ -749,6 +752,13 @@ int run_large(pm3gpu_ctx* c, const MolPlan& p, const int32_t* hz, const int32_t*
         if ((rc = save(st)) != PM3GPU_OK) return rc;
       }
     }
+  }
+  {
+    CUDA_TRY(c, cudaEventRecord(c->kev[1], c->stream));
+    CUDA_TRY(c, cudaEventSynchronize(c->kev[1]));
+    float scf_ms = 0.f;
+    CUDA_TRY(c, cudaEventElapsedTime(&scf_ms, c->kev[0], c->kev[1]));
+    c->timings[3] += scf_ms;
   }
   double e_isol = 0.0, eheat = 0.0;
   for (int a = 0; a < p.natom; ++a) {
@@ -987,6 +997,7 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
               pm3gpu_result* results, double* charges, double* gradients, double* density, double* mo_energies,
               double* all_dens = nullptr, const size_t* all_dens_off = nullptr) {
   c->launches = 0;
+  c->timings[3] = 0.0;
   c->timings[5] = 0.0;
   c->h2d = c->d2h = 0;
   for (int k = 0; k < kPhases; ++k) c->phase_cycles[k] = 0.0;
@@ -1214,7 +1225,6 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
   c->timings[0] = ms[0];
   c->timings[1] = ms[1];
   c->timings[2] = ms[2];
-  c->timings[3] = 0.0;
   c->timings[4] = ms[3];
   return PM3GPU_OK;
 }
@@ -1377,6 +1387,7 @@ void pm3gpu_context_destroy(pm3gpu_ctx* c) {
     delete c->lbuf;
   }
   c->lsel.release();
+  for (DevBuf& b : c->tcbuf) b.release();
   for (DevBuf* b : {&c->gp, &c->gpb, &c->gm, &c->gv, &c->gg, &c->gqmols, &c->gatom, &c->gao, &c->gcoord, &c->gX, &c->gY,
                     &c->gZ[0], &c->gZ[1], &c->gZ[2], &c->gH[0], &c->gH[1], &c->gH[2], &c->gdH, &c->gdZ, &c->gT, &c->gM,
                     &c->gidx, &c->gXb, &c->gTb, &c->gMb, &c->gdY, &c->gpart, &c->gguess, &c->gdens})
@@ -1842,6 +1853,45 @@ int pm3gpu_last_large_trace(pm3gpu_ctx* c, double* rows, int max_rows) {
   const int total = (int)(c->ltrace.size() / 5);
   if (rows && max_rows > 0) std::copy_n(c->ltrace.begin(), 5 * (size_t)std::min(total, max_rows), rows);
   return total;
+}
+
+int pm3gpu_split_gemm(pm3gpu_ctx* c, int m, int n, int k, const double* a, int lda, const double* b, int ldb,
+                      float* out) {
+  if (!c || m < 1 || n < 1 || k < 1 || !a || !b || !out || lda < k || ldb < k)
+    return fail(c, PM3GPU_INVALID_INPUT, "bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  c->err.clear();
+  c->launches = 0;
+  const int ldp = (k + 7) & ~7;
+  DevBuf* B = c->tcbuf;
+  CUDA_TRY(c, B[0].ensure(8 * (size_t)m * lda));
+  CUDA_TRY(c, B[1].ensure(8 * (size_t)n * ldb));
+  for (int q = 0; q < 2; ++q) CUDA_TRY(c, B[2 + q].ensure(2 * (size_t)m * ldp));
+  for (int q = 0; q < 2; ++q) CUDA_TRY(c, B[4 + q].ensure(2 * (size_t)n * ldp));
+  CUDA_TRY(c, B[6].ensure(4 * (size_t)m * n + 256));
+  CUDA_TRY(c, cudaMemcpyAsync(B[0].p, a, 8 * (size_t)m * lda, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(B[1].p, b, 8 * (size_t)n * ldb, cudaMemcpyHostToDevice, c->stream));
+  int* derr = reinterpret_cast<int*>(B[6].as<char>() + 4 * (size_t)m * n);
+  CUDA_TRY(c, cudaMemsetAsync(derr, 0, sizeof(int), c->stream));
+  auto blocks = [](size_t cnt) { return (unsigned)std::min<size_t>((cnt + 255) / 256, 65535); };
+  large::split_pad_kernel<<<blocks((size_t)m * ldp), large::kBlock, 0, c->stream>>>(
+      B[0].as<double>(), m, k, lda, B[2].as<__nv_bfloat16>(), B[3].as<__nv_bfloat16>(), ldp);
+  large::split_pad_kernel<<<blocks((size_t)n * ldp), large::kBlock, 0, c->stream>>>(
+      B[1].as<double>(), n, k, ldb, B[4].as<__nv_bfloat16>(), B[5].as<__nv_bfloat16>(), ldp);
+  CUDA_TRY(c, cudaGetLastError());
+  if (!tc::launch_split_gemm(m, n, k, B[2].as<__nv_bfloat16>(), B[3].as<__nv_bfloat16>(), ldp,
+                             B[4].as<__nv_bfloat16>(), B[5].as<__nv_bfloat16>(), ldp, B[6].as<float>(), n, derr,
+                             c->stream))
+    return fail(c, PM3GPU_CUDA_ERROR, "split-BF16 GEMM: tensor map or kernel attribute could not be set");
+  c->launches = 3;
+  CUDA_TRY(c, cudaGetLastError());
+  int flag = 0;
+  CUDA_TRY(c, cudaMemcpyAsync(out, B[6].p, 4 * (size_t)m * n, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(&flag, derr, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (flag) return fail(c, PM3GPU_CUDA_ERROR, "split-BF16 GEMM: a pipeline wait in the kernel ran out");
+  return PM3GPU_OK;
 }
 
 int pm3gpu_set_large_checks(pm3gpu_ctx* c, int on) {

@@ -1,7 +1,9 @@
 """pm3_rs on B200: the molecular PM3 single point of pm3-rs, computed by the pm3gpu CUDA
 library (sm_100a). Import-compatible with pm3-rs's ``pm3_rs`` for the single-point entry
-points (``single_point``, ``gradient``, ``forces``), plus ``batch`` for many molecules."""
+points (``single_point``, ``gradient``, ``forces``), plus ``batch`` for many molecules and
+``batch_on_devices`` to spread one batch over several GPUs."""
 from .native import ANGSTROM_TO_BOHR, EV_TO_HARTREE, BatchResult, batch, forces, gradient, options, run, single_point
+from .sharding import batch_on_devices, partition
 
-__all__ = ["single_point", "gradient", "forces", "batch", "run", "options", "BatchResult", "ANGSTROM_TO_BOHR",
-           "EV_TO_HARTREE"]
+__all__ = ["single_point", "gradient", "forces", "batch", "batch_on_devices", "partition", "run", "options",
+           "BatchResult", "ANGSTROM_TO_BOHR", "EV_TO_HARTREE"]

@@ -168,6 +168,7 @@ class BatchResult:
     """Column arrays of a batched solve (one row per molecule)."""
 
     def __init__(self, results, charges, gradients, offsets):
+        self.raw = list(results)
         self.status = np.array([r.status for r in results], dtype=np.int32)
         self.heat_of_formation_kcal = np.array([r.heat_of_formation_kcal for r in results])
         self.total_ev = np.array([r.total_ev for r in results])

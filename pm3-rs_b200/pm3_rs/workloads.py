@@ -252,17 +252,23 @@ def radical(n_atoms: int, seed: int):
     raise RuntimeError("no hydrogen to remove")
 
 
-def organic_batch(n_mol: int, lo: int = 5, hi: int = 60, seed: int = 1234):
-    """List of (z, xyz_angstrom) for ``n_mol`` organics with sizes uniform in [lo, hi]."""
-    rng = np.random.default_rng(seed)
-    sizes = rng.integers(lo, hi + 1, n_mol)
-    return [organic(int(s), seed * 1000003 + i) for i, s in enumerate(sizes)]
+def organic_batch(n_mol: int, lo: int = 5, hi: int = 60, seed: int = 1234, only=None):
+    """List of (z, xyz_angstrom) for ``n_mol`` organics with sizes uniform in [lo, hi]. With
+    ``only`` (molecule indices), just those molecules of the same batch, in that order."""
+    sizes = organic_batch_sizes(n_mol, lo, hi, seed)
+    idx = range(n_mol) if only is None else only
+    return [organic(int(sizes[i]), seed * 1000003 + int(i)) for i in idx]
 
 
-def radical_batch(n_mol: int, lo: int = 10, hi: int = 80, seed: int = 4321):
-    rng = np.random.default_rng(seed)
-    sizes = rng.integers(lo, hi + 1, n_mol)
-    return [radical(int(s), seed * 1000003 + i) for i, s in enumerate(sizes)]
+def organic_batch_sizes(n_mol: int, lo: int = 5, hi: int = 60, seed: int = 1234):
+    """Atom counts of the molecules of ``organic_batch`` (cheap: no molecule is built)."""
+    return np.random.default_rng(seed).integers(lo, hi + 1, n_mol)
+
+
+def radical_batch(n_mol: int, lo: int = 10, hi: int = 80, seed: int = 4321, only=None):
+    sizes = np.random.default_rng(seed).integers(lo, hi + 1, n_mol)
+    idx = range(n_mol) if only is None else only
+    return [radical(int(sizes[i]), seed * 1000003 + int(i)) for i in idx]
 
 
 def pack(mols):

@@ -1,10 +1,11 @@
 """The multi-process bench path on CPU: two gloo ranks (127.0.0.1).
 
-Under torchrun every rank solves its own shard of molecules (weak scaling, no data-path
-collective); the whole-job line takes the slowest rank's device time and the sum of the
-converged counts. The reference arm runs on rank 0 only; the other ranks exit without work.
+Under torchrun the ranks split ONE batch of molecules (n per rank x ranks) by the
+longest-processing-time partition (weak scaling, no data-path collective): every molecule lands on
+exactly one rank and the ranks' cost shares are balanced. The whole-job line takes the slowest
+rank's device time and the sum of the converged counts. The reference arm runs on rank 0 only; the
+other ranks exit without work.
 """
-import hashlib
 import importlib.util
 import os
 import socket
@@ -38,10 +39,13 @@ def _rank(rank, world, port, out):
         bench = _bench()
         from pm3_rs import workloads
 
-        mols = workloads.organic_batch(16, 5, 20, seed=bench.shard_seed(rank))
-        digest = hashlib.sha256(b"".join(np.asarray(x).tobytes() for _, x in mols)).hexdigest()
+        mols = bench.rank_molecules(16, rank, world)
+        # the same molecules as the one global batch builds, identified by their coordinates
+        full = bench.molecules(16 * world, 1234)
+        mine = [next(i for i, (_, fx) in enumerate(full) if np.array_equal(fx, x)) for _, x in mols]
+        cost = float(sum(float(len(zz)) ** 3 for zz, _ in mols))
         digests = [None] * world
-        dist.all_gather_object(digests, digest)
+        dist.all_gather_object(digests, (sorted(mine), cost))
         # rank-dependent device times and counts: the job line takes the max and the sum
         tot, e_tot, conv, e_conv = bench.reduce_over_ranks(100.0 + 10 * rank, 50.0 - rank, 7 + rank, 5 + rank, dist,
                                                            "cpu")
@@ -62,7 +66,9 @@ def test_two_gloo_ranks_shard_and_reduce():
         p.join(timeout=60)
         assert p.exitcode == 0
     for rank, digests, tot, e_tot, conv, e_conv in got:
-        assert digests[0] != digests[1]  # each rank has its own molecules
+        (a, ca), (b, cb) = digests
+        assert sorted(a + b) == list(range(32)) and not set(a) & set(b)  # one batch, split
+        assert abs(ca - cb) <= 60.0 ** 3  # within one largest molecule's cost
         assert (tot, e_tot, conv, e_conv) == (110.0, 50.0, 15, 11)
 
 
