@@ -10,7 +10,8 @@
 //      on the unreduced block holding the eigenvalue (T is split where |e_i| <= 1000 eps ||T||,
 //      which separates exact degeneracies); members of a within-block cluster (gap below
 //      1e-7 ||T||) after the first are redone by inverse iteration with re-orthogonalisation.
-//   4. Back-transformation Z = Q Y, one warp per pair of vectors held in registers.
+//   4. Back-transformation Z = Q Y, one warp per 2, 4 or 8 vectors held in registers (fewer rows
+//      per lane for smaller bases, more vectors).
 // Only the eigenpairs the SCF needs are formed (the occupied block, plus one more value for
 // the frontier gap). Eigenvalues come out ascending, as the reference requires.
 #pragma once
@@ -530,59 +531,72 @@ __device__ void tridiag_vectors(int n, int kvec, double* Y, double* tf, const Ei
 
 // ------------------------------------------------------------------- 4. back-transform
 // Y[j] <- H(0) H(1) ... H(n-3) Y[j] for j < kvec, two vectors per warp held in registers.
-__device__ void back_transform(int n, int kvec, const double* __restrict__ A, double* Y, const EigenScratch& s_) {
-  const double* __restrict__ tau_ = s_.tau;
+// One warp applies the reflectors to NV vectors at a time, RT rows per lane held in registers
+// (n <= 32 RT). Per reflector the NV partial dot products are reduced together (their shuffle
+// chains overlap), so the latency of a reflector is paid once for NV vectors.
+template <int RT, int NV>
+__device__ __forceinline__ void back_transform_t(int n, int kvec, const double* __restrict__ A, double* Y,
+                                                 const double* __restrict__ tau_) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int j0 = 2 * warp; j0 < kvec; j0 += 2 * kWarps) {
-    const bool two = j0 + 1 < kvec;
-    double* y0 = Y + (size_t)j0 * n;
-    double* y1 = Y + (size_t)(two ? j0 + 1 : j0) * n;
-    double z0[kRowT], z1[kRowT];
+  for (int j0 = NV * warp; j0 < kvec; j0 += NV * kWarps) {
+    double z[NV][RT];
 #pragma unroll
-    for (int t = 0; t < kRowT; ++t) {
-      const int r = lane + 32 * t;
-      z0[t] = r < n ? y0[r] : 0.0;
-      z1[t] = r < n ? y1[r] : 0.0;
+    for (int v = 0; v < NV; ++v) {
+      const double* y = Y + (size_t)(j0 + v < kvec ? j0 + v : j0) * n;
+#pragma unroll
+      for (int t = 0; t < RT; ++t) {
+        const int r = lane + 32 * t;
+        z[v][t] = r < n ? y[r] : 0.0;
+      }
     }
     for (int i = n - 3; i >= 0; --i) {
       const double tau = tau_[i];
       if (tau == 0.0) continue;
-      double a0 = 0.0, a1 = 0.0;
+      double vr[RT];
 #pragma unroll
-      for (int t = 0; t < kRowT; ++t) {
+      for (int t = 0; t < RT; ++t) {
         const int r = lane + 32 * t;
-        if (r > i && r < n) {
-          const double vr = r == i + 1 ? 1.0 : A[tri(r) + i];
-          a0 = fma(vr, z0[t], a0);
-          a1 = fma(vr, z1[t], a1);
-        }
+        vr[t] = (r > i && r < n) ? (r == i + 1 ? 1.0 : A[tri(r) + i]) : 0.0;
       }
-      for (int o = 16; o > 0; o >>= 1) {
-        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-      }
-      a0 *= tau;
-      a1 *= tau;
+      double a[NV];
 #pragma unroll
-      for (int t = 0; t < kRowT; ++t) {
-        const int r = lane + 32 * t;
-        if (r > i && r < n) {
-          const double vr = r == i + 1 ? 1.0 : A[tri(r) + i];
-          z0[t] -= a0 * vr;
-          z1[t] -= a1 * vr;
-        }
+      for (int v = 0; v < NV; ++v) {
+        double acc = 0.0;
+#pragma unroll
+        for (int t = 0; t < RT; ++t) acc = fma(vr[t], z[v][t], acc);
+        a[v] = acc;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) a[v] += __shfl_xor_sync(0xffffffffu, a[v], o);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const double s = a[v] * tau;
+#pragma unroll
+        for (int t = 0; t < RT; ++t) z[v][t] = fma(-s, vr[t], z[v][t]);
       }
     }
 #pragma unroll
-    for (int t = 0; t < kRowT; ++t) {
-      const int r = lane + 32 * t;
-      if (r < n) {
-        y0[r] = z0[t];
-        if (two) y1[r] = z1[t];
+    for (int v = 0; v < NV; ++v) {
+      if (j0 + v >= kvec) break;
+      double* y = Y + (size_t)(j0 + v) * n;
+#pragma unroll
+      for (int t = 0; t < RT; ++t) {
+        const int r = lane + 32 * t;
+        if (r < n) y[r] = z[v][t];
       }
     }
   }
   __syncthreads();
+}
+
+// The reflectors of column i (v_{i+1} = 1, v_r = A(r, i) below) applied from the last to the
+// first. Smaller matrices take more vectors per warp (the same registers either way).
+__device__ void back_transform(int n, int kvec, const double* __restrict__ A, double* Y, const EigenScratch& s_) {
+  if (n <= 64) back_transform_t<2, 8>(n, kvec, A, Y, s_.tau);
+  else if (n <= 128) back_transform_t<4, 4>(n, kvec, A, Y, s_.tau);
+  else back_transform_t<kRowT, 2>(n, kvec, A, Y, s_.tau);
 }
 
 // All eigenvalues of the saved tridiagonal (d, e) -- used once at the end for the MO energies.
