@@ -297,6 +297,18 @@ int pm3gpu_split_gemm(pm3gpu_ctx* ctx, int m, int n, int k, const double* a, int
  * most max_rows rows and returns the total number of rows. */
 int pm3gpu_last_large_trace(pm3gpu_ctx* ctx, double* rows, int max_rows);
 
+/* Batched launch (no counterpart in the reference): with on = 1, CTAs left without work near the
+ * end of a batch take the beta spin of unaccelerated unrestricted jobs still running (the
+ * reference's UHF loop without DIIS, src/scf.rs:1319-1496): from the next iteration on, the two
+ * CTAs build F_alpha and F_beta, diagonalise and form the two spin densities side by side and
+ * exchange energy parts and density changes each iteration (bounded waits). It shortens the tail
+ * of a batch (long unrestricted stability rungs, radicals) when one batch runs at a time; with
+ * batches overlapping, the idle SMs are better left to the next batch. Same results up to the
+ * summation order of the electronic energy. Default off. */
+int pm3gpu_set_tail_helpers(pm3gpu_ctx* ctx, int on);
+/* Number of jobs of the last call that ran their iterations on two CTAs. */
+int pm3gpu_last_paired_jobs(pm3gpu_ctx* ctx);
+
 /* Checks of every eigensolve of the whole-GPU path (no counterpart in the reference, whose
  * eigensolver is faer's, src/linalg.rs:221-263). Each eigensolve orthonormalises the occupied
  * vectors X by Newton-Schulz steps until max |X^T X - I| < 1e-13 (at most 5 steps; a defect still

@@ -93,7 +93,9 @@ struct pm3gpu_ctx {
   std::string err;
   ElemDev h_elem[kMaxZ];
   PairDev h_pairs;
-  DevBuf elem, pairs, z, xyz, jobs, out, charges, dens, grads, eps, work, queue, rq, gmols, aooff;
+  DevBuf elem, pairs, z, xyz, jobs, out, charges, dens, grads, eps, work, queue, rq, gmols, aooff, help;
+  bool tail_helpers = false;  // idle CTAs take the beta spin of unaccelerated unrestricted jobs
+  int paired = 0;              // jobs of the last call that ran on two CTAs
   int sms = 0, smem_optin = 0, smem_per_sm = 0;
   double timings[6] = {0, 0, 0, 0, 0, 0};
   int launches = 0;
@@ -579,6 +581,7 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   CUDA_TRY(c, c->dens.ensure(8 * std::max<size_t>(tot.dens, 1)));
   CUDA_TRY(c, c->eps.ensure(8 * std::max<size_t>(tot.eps, 1)));
   CUDA_TRY(c, c->queue.ensure(64));
+  if (c->tail_helpers) CUDA_TRY(c, c->help.ensure(sizeof(HelpRec) * (size_t)grid));
   CUDA_TRY(c, cudaMemcpyAsync(c->jobs.p, jobs.data(), sizeof(JobDesc) * nj, cudaMemcpyHostToDevice, c->stream));
   if (nr)
     CUDA_TRY(c, cudaMemcpyAsync(c->jobs.as<JobDesc>() + nj, rjobs.data(), sizeof(JobDesc) * nr, cudaMemcpyHostToDevice,
@@ -586,6 +589,7 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   if (dens_in && !dens_in->empty())
     CUDA_TRY(c, cudaMemcpyAsync(c->dens.p, dens_in->data(), 8 * dens_in->size(), cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaMemsetAsync(c->queue.p, 0, 64, c->stream));
+  if (c->tail_helpers) CUDA_TRY(c, cudaMemsetAsync(c->help.p, 0, sizeof(HelpRec) * (size_t)grid, c->stream));
   CUDA_TRY(c, cudaMemsetAsync(c->rq.p, 0, 2 * sizeof(int) * std::max(nr, 1), c->stream));
   if (nr) CUDA_TRY(c, cudaMemsetAsync(c->out.as<JobOut>() + nj, 0xff, sizeof(JobOut) * nr, c->stream));
   KernelArgs a{};
@@ -612,6 +616,7 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   a.wcap = wcap;
   a.queue = c->queue.as<int>();
   a.prof = nullptr;
+  a.help = c->tail_helpers ? c->help.as<HelpRec>() : nullptr;
   if (c->profile) {
     CUDA_TRY(c, c->prof.ensure(sizeof(unsigned long long) * kPhases));
     CUDA_TRY(c, cudaMemsetAsync(c->prof.p, 0, sizeof(unsigned long long) * kPhases, c->stream));
@@ -623,7 +628,7 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   c->launches += 1;
   CUDA_TRY(c, cudaGetLastError());
   CUDA_TRY(c, cudaEventRecord(c->kev[1], c->stream));
-  int qh[4] = {0, 0, 0, 0};
+  int qh[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   CUDA_TRY(c, cudaMemcpyAsync(qh, c->queue.p, sizeof(qh), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaMemcpyAsync(R.out.data(), c->out.p, sizeof(JobOut) * nj, cudaMemcpyDeviceToHost, c->stream));
   if (nr)
@@ -641,7 +646,8 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
     CUDA_TRY(c, cudaMemcpyAsync(R.eps.data(), c->eps.p, 8 * tot.eps, cudaMemcpyDeviceToHost, c->stream));
   }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  if (qh[3]) return fail(c, PM3GPU_CUDA_ERROR, "stability-search queue handshake timed out on the device");
+  if (qh[3]) return fail(c, PM3GPU_CUDA_ERROR, "a bounded wait of the batched SCF kernel ran out on the device");
+  c->paired += qh[6];
   if (c->profile) {
     unsigned long long ph[kPhases];
     CUDA_TRY(c, cudaMemcpy(ph, c->prof.p, sizeof(ph), cudaMemcpyDeviceToHost));
@@ -997,6 +1003,7 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
               pm3gpu_result* results, double* charges, double* gradients, double* density, double* mo_energies,
               double* all_dens = nullptr, const size_t* all_dens_off = nullptr) {
   c->launches = 0;
+  c->paired = 0;
   c->timings[3] = 0.0;
   c->timings[5] = 0.0;
   c->h2d = c->d2h = 0;
@@ -1376,7 +1383,7 @@ void pm3gpu_context_destroy(pm3gpu_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (DevBuf* b : {&c->elem, &c->pairs, &c->z, &c->xyz, &c->jobs, &c->out, &c->charges, &c->dens, &c->grads, &c->eps,
-                    &c->work, &c->queue, &c->prof, &c->rq, &c->gmols, &c->aooff})
+                    &c->work, &c->queue, &c->prof, &c->rq, &c->gmols, &c->aooff, &c->help})
     b->release();
   for (int k = 0; k < 6; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
@@ -1893,6 +1900,15 @@ int pm3gpu_split_gemm(pm3gpu_ctx* c, int m, int n, int k, const double* a, int l
   if (flag) return fail(c, PM3GPU_CUDA_ERROR, "split-BF16 GEMM: a pipeline wait in the kernel ran out");
   return PM3GPU_OK;
 }
+
+int pm3gpu_set_tail_helpers(pm3gpu_ctx* c, int on) {
+  if (!c) return PM3GPU_INVALID_INPUT;
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->tail_helpers = on != 0;
+  return PM3GPU_OK;
+}
+
+int pm3gpu_last_paired_jobs(pm3gpu_ctx* c) { return c ? c->paired : 0; }
 
 int pm3gpu_set_large_checks(pm3gpu_ctx* c, int on) {
   if (!c) return PM3GPU_INVALID_INPUT;

@@ -7,7 +7,16 @@
 namespace pm3gpu {
 
 // ------------------------------------------------------------------------------- one job
-__device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
+// Bounded wait of one thread for *p >= want (about a second at most). False when it ran out.
+__device__ __forceinline__ bool wait_at_least(const volatile int* p, int want) {
+  for (int i = 0; i < (1 << 22); ++i) {
+    if (*p >= want) return true;
+    __nanosleep(200);
+  }
+  return false;
+}
+
+__device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out, int kind = -1, int jidx = -1) {
   const KernelArgs& A = *c.A;
   c.job = job;
   c.out = out;
@@ -109,8 +118,40 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
   const int kvb = n < nb + 1 ? n : nb + 1;
   const int slot_mats = uhf ? 4 : 3;
 
+  // An unaccelerated unrestricted job offers its beta spin to an idle CTA: from the first
+  // iteration boundary after a helper took the offer, the helper builds F_beta, diagonalises it
+  // and forms P_beta on this CTA's workspace while this CTA does the alpha spin.
+  HelpRec* hr = (A.help && uhf && J.accel == 0 && kind >= 0) ? A.help + blockIdx.x : nullptr;
+  __shared__ int s_pair;  // 1 once the two CTAs run the iterations together
+  int gen = 0;
+  if (tid == 0) {
+    s_pair = 0;
+    if (hr) {
+      gen = (((volatile HelpRec*)hr)->sg >> 3) + 1;
+      hr->kind = kind;
+      hr->idx = jidx;
+      hr->go = -1;
+      hr->hdone = -1;
+      __threadfence();
+      atomicExch(&hr->sg, gen * 8 + 1);
+    }
+  }
+  __syncthreads();
+
   for (int iter = 0; iter < J.max_scf; ++iter) {
     iterations = iter + 1;
+    if (hr) {  // a helper that took the offer starts with this iteration
+      if (tid == 0 && !s_pair && atomicAdd(&hr->sg, 0) == gen * 8 + 2) {
+        hr->cur = c.cur;
+        hr->go = iter;
+        __threadfence();
+        // a helper that gave up waiting has set the offer to stop: then this job stays alone
+        s_pair = atomicCAS(&hr->sg, gen * 8 + 2, gen * 8 + 3) == gen * 8 + 2 ? 1 : 0;
+        if (s_pair) atomicAdd(&A.queue[6], 1);  // jobs that ran paired (reported to the host)
+      }
+      __syncthreads();
+    }
+    const bool paired = hr && s_pair;
     double* Pc = c.P[c.cur];
     double* Qc = c.Q[c.cur];
     double* Pn = c.P[1 - c.cur];
@@ -149,6 +190,15 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
       double part = 0.0;
       for (size_t k = tid; k < nn; k += kThreads) part = fma(Pc[k], c.H[k] + Fa[k], part);
       e_elec = 0.5 * block_sum(part, c.red);
+      mark(c, kPhFock);
+    } else if (paired) {  // alpha here; the helper builds F_beta and returns its energy part
+      double* Pt = c.Vb + nn;
+      for (size_t k = tid; k < nn; k += kThreads) Pt[k] = Pc[k] + Qc[k];
+      __syncthreads();
+      build_fock(c, Pt, Pc, nullptr, Fa, nullptr);
+      double part = 0.0;
+      for (size_t k = tid; k < nn; k += kThreads) part += Pt[k] * c.H[k] + Pc[k] * Fa[k];
+      e_elec = block_sum(part, c.red);  // completed with the helper's part below
       mark(c, kPhFock);
     } else {
       double* Pt = c.Vb + nn;  // scratch right after Vb (slot reserves it)
@@ -243,7 +293,7 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
       const double* __restrict__ coef = c.coef;
       const double* __restrict__ hist = c.hist;
       const double shift = J.shift;
-      for (int spin = 0; spin < (uhf ? 2 : 1); ++spin) {
+      for (int spin = 0; spin < (uhf && !paired ? 2 : 1); ++spin) {
         const double* Pproj = spin == 0 ? Pc : Qc;
         const double* Fnew = spin == 0 ? Fa : Fb;
         for (int k = tid; k < nt; k += kThreads) {
@@ -277,15 +327,38 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
         }
       }
     }
+    if (paired) {  // the helper's beta spin of this iteration: energy part and density change
+      if (tid == 0) {
+        const bool ok = wait_at_least(&((volatile HelpRec*)hr)->hdone, iter);
+        if (!ok) atomicExch(&A.queue[3], 1);  // reported by the host as a device error
+        __threadfence();
+        c.misc[0] = ok ? ((volatile HelpRec*)hr)->part_b[iter & 1] : NAN;
+        c.misc[1] = ok ? ((volatile HelpRec*)hr)->sq_b[iter & 1] : NAN;
+      }
+      __syncthreads();
+      e_elec = 0.5 * (e_elec + c.misc[0]);
+      sq_b = c.misc[1];
+      __syncthreads();
+    }
     const double dp = uhf ? sqrt(sq_a / (double)nn) + sqrt(sq_b / (double)nn) : sqrt(sq_a / (double)nn);
     const double de = fabs(e_elec - e_old);
     last_change = dp;
     e_old = e_elec;
     c.cur = 1 - c.cur;
+    const bool done = (iter > 0 && de < J.e_tol && dp < J.p_tol) || !(dp == dp);
+    if (paired && tid == 0 && !done && iter + 1 < J.max_scf) {  // the helper may run the next iteration
+      hr->cur = c.cur;
+      __threadfence();
+      atomicExch(&hr->go, iter + 1);
+    }
     if (iter > 0 && de < J.e_tol && dp < J.p_tol) {
       converged = true;
       break;
     }
+    if (!(dp == dp)) break;  // only after a failed pairing wait (NaN), which the host reports
+  }
+  if (hr && tid == 0) {  // close the offer: stop the helper, or withdraw an offer not yet taken
+    if (atomicCAS(&hr->sg, gen * 8 + 1, gen * 8) != gen * 8 + 1) atomicExch(&hr->sg, gen * 8 + 4);
   }
 
   // ------------------------------------------------------- closing energy at the final density
@@ -371,7 +444,128 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out) {
   __syncthreads();
 }
 
+// Workspace pointers of the slot starting at `slot` (layout of slot_doubles).
+__device__ __forceinline__ void slot_ptrs(Ctx& c, double* slot, int nmax) {
+  const size_t nn = (size_t)nmax * nmax;
+  c.H = slot;
+  c.P[0] = slot + nn;
+  c.P[1] = slot + 2 * nn;
+  c.Q[0] = slot + 3 * nn;
+  c.Q[1] = slot + 4 * nn;
+  c.F = slot + 5 * nn;
+  c.G = slot + 6 * nn;
+  c.Vt = slot + 7 * nn;
+  c.Vb = slot + 8 * nn;  // followed by one nn of scratch (total density)
+  c.Ag = slot + 10 * nn;
+  c.tf = slot + 11 * nn;     // 6 nn: eigenvector scratch
+  c.hist = slot + 17 * nn;   // 32 nn: accelerator history
+  c.tri_a = slot + 49 * nn;
+  c.tri_b = c.tri_a + 4 * nmax;  // per spin: saved tridiagonal (2n), eigenvalues (n), their change (n)
+  c.W = c.tri_b + 4 * nmax;
+}
+
+// The beta spin of CTA L's unrestricted job (offer generation `mygen`, already taken by this
+// CTA), iteration by iteration on L's workspace: F_beta = H + J(P_t) - K(P_beta), its eigensolve
+// (warm-started from L's saved beta eigenvalues) and the new P_beta, then the energy part and the
+// squared density change for L, which decides convergence. Own shared memory and own scratch
+// (packed eigen input, eigenvector scratch, total density) stay with this CTA. Every wait is
+// bounded; a wait that runs out raises the launch's error flag.
+__device__ __noinline__ void help_job(Ctx& c, int L, int mygen) {
+  const KernelArgs& A = *c.A;
+  HelpRec* hr = A.help + L;
+  volatile HelpRec* vr = hr;
+  const int tid = threadIdx.x;
+  __shared__ int s_h[2];
+  c.tmark = clock64();
+  if (tid == 0) {
+    int st = 0;
+    for (int i = 0; i < (1 << 22) && !st; ++i) {
+      const int v = vr->sg;
+      if ((v >> 3) != mygen || (v & 7) == 4) st = 4;
+      else if ((v & 7) == 3) st = 3;
+      else __nanosleep(200);
+    }
+    if (!st && atomicCAS(&hr->sg, mygen * 8 + 2, mygen * 8 + 4) != mygen * 8 + 2)  // gave up: unless activated
+      st = (vr->sg == mygen * 8 + 3) ? 3 : 4;
+    __threadfence();
+    s_h[0] = st == 3 ? vr->go : -1;
+  }
+  __syncthreads();
+  int iter = s_h[0];
+  __syncthreads();
+  if (iter < 0) return;
+  const JobDesc* tab = vr->kind == 0 ? A.jobs : A.rjobs;
+  c.job = tab[vr->idx];
+  const JobDesc& J = c.job;
+  c.n = J.nao;
+  c.N = J.natom;
+  const int n = c.n, nb = J.n_beta;
+  const size_t nn = (size_t)n * n;
+  setup_job(c);
+  double* own_vb = c.Vb;
+  double* own_vt = c.Vt;
+  double* own_ag = c.Ag;
+  double* own_tf = c.tf;
+  slot_ptrs(c, A.work + (size_t)L * A.slot, A.nmax);  // L's matrices
+  c.Vb = own_vb;
+  c.Vt = own_vt;
+  c.Ag = own_ag;
+  c.tf = own_tf;
+  double* Pt = own_vb + nn;
+  double* eps_b = c.tri_b + 2 * n;
+  const int kvb = n < nb + 1 ? n : nb + 1;
+  for (;; ++iter) {
+    if (tid == 0) {
+      int ok = -1;
+      for (int i = 0; i < (1 << 22) && ok < 0; ++i) {
+        if (vr->go >= iter) ok = 1;
+        else {
+          const int v = vr->sg;
+          if ((v >> 3) != mygen || (v & 7) == 4) ok = 0;
+          else __nanosleep(200);
+        }
+      }
+      if (ok < 0) {
+        atomicExch(&A.queue[3], 1);
+        ok = 0;
+      }
+      __threadfence();
+      s_h[0] = ok;
+      s_h[1] = vr->cur;
+    }
+    __syncthreads();
+    const int ok = s_h[0], cur = s_h[1];
+    __syncthreads();
+    if (!ok) break;
+    const double* Pc = c.P[cur];
+    double* Qc = c.Q[cur];
+    double* Qn = c.Q[1 - cur];
+    for (size_t k = tid; k < nn; k += kThreads) Pt[k] = Pc[k] + Qc[k];
+    __syncthreads();
+    build_fock(c, Pt, Qc, nullptr, c.G, nullptr);
+    double part = 0.0;
+    for (size_t k = tid; k < nn; k += kThreads) part += Qc[k] * c.G[k];
+    part = block_sum(part, c.red);
+    mark(c, kPhFock);
+    double* Ap = pack_input(c, c.G, Qc, J.shift);
+    eigensolve(c, Ap, kvb, nb, c.Vb, eps_b, c.tri_b, iter > 0, c.tri_b + 3 * n);
+    const double sq = density(c, c.Vb, nb, 1.0, Qc, Qn, J.damping);
+    mark(c, kPhDensity);
+    if (tid == 0) {
+      hr->part_b[iter & 1] = part;
+      hr->sq_b[iter & 1] = sq;
+      __threadfence();
+      atomicExch(&hr->hdone, iter);
+    }
+    __syncthreads();
+  }
+  slot_ptrs(c, A.work + (size_t)blockIdx.x * A.slot, A.nmax);  // back to this CTA's own slot
+}
+
 // ----------------------------------------------------------------------- the kernel
+// CTAs that may stay, once the first passes are all taken, for stability rungs still to come.
+constexpr int kMaxWaiters = 32;
+
 __global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_job;
@@ -419,37 +613,21 @@ __global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args)
   c.tile = up;
   c.Asm = up;
 
-  const size_t nn = (size_t)args.nmax * args.nmax;
-  double* slot = args.work + (size_t)blockIdx.x * args.slot;
-  c.H = slot;
-  c.P[0] = slot + nn;
-  c.P[1] = slot + 2 * nn;
-  c.Q[0] = slot + 3 * nn;
-  c.Q[1] = slot + 4 * nn;
-  c.F = slot + 5 * nn;
-  c.G = slot + 6 * nn;
-  c.Vt = slot + 7 * nn;
-  c.Vb = slot + 8 * nn;  // followed by one nn of scratch (total density)
-  c.Ag = slot + 10 * nn;
-  c.tf = slot + 11 * nn;     // 6 nn: eigenvector scratch
-  c.hist = slot + 17 * nn;   // 32 nn: accelerator history
-  c.tri_a = slot + 49 * nn;
-  c.tri_b = c.tri_a + 4 * args.nmax;  // per spin: saved tridiagonal (2n), eigenvalues (n), their change (n)
-  c.W = c.tri_b + 4 * args.nmax;
+  slot_ptrs(c, args.work + (size_t)blockIdx.x * args.slot, args.nmax);
 
   __shared__ unsigned long long s_ph[kPhases];
   c.ph = s_ph;
   if (threadIdx.x < kPhases) s_ph[threadIdx.x] = 0ULL;
   __syncthreads();
-  __shared__ int s_kind;
+  __shared__ int s_kind, s_hgen;
   int* q = args.queue;
   for (;;) {
     if (threadIdx.x == 0) {
       // Rung jobs first (they are the long ones and only exist once a first pass asked for
       // them), else the next first-pass job. Every wait here is bounded; a handshake that
       // times out raises the error flag instead of hanging.
-      int kind = -1, idx = -1;
-      bool first_done = false;
+      int kind = -1, idx = -1, hgen = 0;
+      bool first_done = false, waiting = false;
       for (int guard = 0; guard < (1 << 20); ++guard) {
         const int h = atomicAdd(&q[2], 0), t = atomicAdd(&q[1], 0);
         if (h < t) {
@@ -480,17 +658,56 @@ __global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args)
           first_done = true;
           continue;
         }
-        break;
+        // No job to take. While first passes are still running they may queue stability rungs
+        // (q[4] counts finished first passes); up to kMaxWaiters CTAs stay for them, sleeping
+        // between polls, so that late rungs run side by side instead of one after another on the
+        // CTA that queued them. The rest exit and free their SM for other work. Bounded by the
+        // guard: a CTA that waits too long exits (its rungs still run on the queuing CTA).
+        bool offers = false;  // an unrestricted job offering its beta spin: take it
+        if (args.help) {
+          for (int L = 0; L < (int)gridDim.x && kind < 0; ++L) {
+            if (L == (int)blockIdx.x) continue;
+            const int v = ((volatile HelpRec*)args.help)[L].sg;
+            if ((v & 7) != 1) continue;
+            offers = true;
+            if (atomicCAS(&args.help[L].sg, v, (v & ~7) | 2) == v) {
+              kind = 2;
+              idx = L;
+              hgen = v >> 3;
+            }
+          }
+          if (kind >= 0) break;
+        }
+        if (!offers && atomicAdd(&q[4], 0) >= args.njobs) break;
+        if (!waiting) {
+          if (atomicAdd(&q[5], 1) >= kMaxWaiters) {
+            atomicSub(&q[5], 1);
+            break;
+          }
+          waiting = true;
+        }
+        __nanosleep(2000);
       }
+      if (waiting) atomicSub(&q[5], 1);
       s_kind = kind;
       s_job = idx;
+      s_hgen = hgen;
     }
     __syncthreads();
-    const int kind = s_kind, jid = s_job;
+    const int kind = s_kind, jid = s_job, hg = s_hgen;
     __syncthreads();
     if (kind < 0) break;
-    if (kind == 0) run_job(c, args.jobs[jid], args.out + jid);
-    else run_job(c, args.rjobs[jid], args.rout + jid);
+    if (kind == 2) {
+      help_job(c, jid, hg);
+    } else if (kind == 0) {
+      run_job(c, args.jobs[jid], args.out + jid, 0, jid);
+      if (threadIdx.x == 0) {  // after its rungs (if any) are queued
+        __threadfence();
+        atomicAdd(&q[4], 1);
+      }
+    } else {
+      run_job(c, args.rjobs[jid], args.rout + jid, 1, jid);
+    }
   }
   if (args.prof && threadIdx.x < kPhases) atomicAdd(&args.prof[threadIdx.x], s_ph[threadIdx.x]);
 }

@@ -95,9 +95,25 @@ struct KernelArgs {
   long long slot;        // doubles per slot
   int nmax;              // largest nao of the launch (slot dimension)
   long long wcap;        // doubles reserved for the pair table
-  int* queue;            // [0] next first-pass job, [1] rung queue tail, [2] rung queue head, [3] error
+  int* queue;            // [0] next first-pass job, [1] rung queue tail, [2] rung queue head, [3] error,
+                         // [4] finished first passes, [5] CTAs waiting for late work, [6] jobs paired
   unsigned long long* prof;  // [kPhases] SM cycles per phase, summed over CTAs (null = off)
   SmemLayout sm;
+  struct HelpRec* help;  // [grid] per CTA: its unrestricted job's offer of the beta spin (null = off)
+};
+
+// One CTA's offer of the beta spin of its unrestricted job to an idle CTA (a "helper"). `sg`
+// packs a generation (bits 3..) and a state (bits 0-2): 0 idle, 1 open, 2 taken by a helper,
+// 3 active (the two CTAs run the iterations from `go` on together), 4 stop. Each new offer takes a
+// new generation, so a helper of an older offer never acts on a newer one.
+struct HelpRec {
+  int sg;
+  int kind, idx;   // the job: 0 first-pass table, 1 rung table
+  int go;          // iteration the helper may run next (the leader published its densities for it)
+  int cur;         // current density buffer of iteration `go`
+  int hdone;       // last iteration the helper has finished
+  int pad[2];
+  double part_b[2], sq_b[2];  // helper's energy part sum P_beta F_beta and squared density change, by iteration parity
 };
 
 // ---------------------------------------------------------------------------- helpers
@@ -289,7 +305,9 @@ __device__ double build_core(Ctx& c) {
 // every array stays in registers. W is the pair's (PA x PB) row-major integral block.
 // kJ = false leaves out the two-centre Coulomb sums into jacc (the whole-GPU path adds them per
 // atom in a fixed order instead of with atomics).
-template <int NA, int NB, bool UHF, bool kJ = true>
+// SPIN = true builds one spin's Fock matrix of an unrestricted job, F = H + J(Pt) - K(Pa) (the
+// first spin of the UHF form alone), for a job whose two spins run on two CTAs.
+template <int NA, int NB, bool UHF, bool kJ = true, bool SPIN = false>
 __device__ __forceinline__ void fock_pair(int n, int a, int b, int oa, int ob, const double* __restrict__ dpk,
                                           double* jacc, const double* __restrict__ H, const double* __restrict__ w,
                                           const double* Pt, const double* Pa, const double* Pb, double* F, double* G) {
@@ -319,8 +337,8 @@ __device__ __forceinline__ void fock_pair(int n, int a, int b, int oa, int ob, c
   // exchange: K[mu][la] = sum_{nu, si} X[nu][si] (mu nu | la si), one spin at a time
 #pragma unroll
   for (int spin = 0; spin < (UHF ? 2 : 1); ++spin) {
-    const double* X = UHF ? (spin == 0 ? Pa : Pb) : Pt;
-    const double xs = UHF ? 1.0 : 0.5;
+    const double* X = (UHF || SPIN) ? (spin == 0 ? Pa : Pb) : Pt;
+    const double xs = (UHF || SPIN) ? 1.0 : 0.5;
     double* out = spin == 0 ? F : G;
     double x[NA * NB];
 #pragma unroll
@@ -345,10 +363,12 @@ __device__ __forceinline__ void fock_pair(int n, int a, int b, int oa, int ob, c
 
 // F = H + J(Pt) - K(Ps) (fock.rs:285-332). Pt = total density; for RHF Ps = Pt/2 (pb == null),
 // for UHF two spin Focks F (from Pa) and G (from Pb) are built in one pass.
+// With Pa given and Pb null, one spin of an unrestricted job: F = H + J(Pt) - K(Pa) (G unused).
 __device__ void build_fock(Ctx& c, const double* Pt, const double* Pa, const double* Pb, double* F, double* G) {
   const KernelArgs& A = *c.A;
   const int n = c.n, N = c.N, tid = threadIdx.x;
   const bool uhf = Pb != nullptr;
+  const bool spin1 = !uhf && Pa != nullptr;
   // stage packed atomic densities (fock.rs:93-100) and zero the Coulomb accumulators
   for (int k = tid; k < N * 10; k += kThreads) {
     const int a = k / 10, p = k % 10;
@@ -384,12 +404,15 @@ __device__ void build_fock(Ctx& c, const double* Pt, const double* Pa, const dou
       const int oa = soff[a], ob = soff[b];
       if (hu && hv) {
         if (uhf) fock_pair<4, 4, true>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+        else if (spin1) fock_pair<4, 4, false, true, true>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
         else fock_pair<4, 4, false>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
       } else if (hu || hv) {
         if (uhf) fock_pair<4, 1, true>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+        else if (spin1) fock_pair<4, 1, false, true, true>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
         else fock_pair<4, 1, false>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
       } else {
         if (uhf) fock_pair<1, 1, true>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
+        else if (spin1) fock_pair<1, 1, false, true, true>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
         else fock_pair<1, 1, false>(n, a, b, oa, ob, dpk, jacc, H, w, Pt, Pa, Pb, F, G);
       }
     }
@@ -411,6 +434,8 @@ __device__ void build_fock(Ctx& c, const double* Pt, const double* Pa, const dou
         if (uhf) {
           ka = fma(Pa[ix], exch, ka);
           kb = fma(Pb[ix], exch, kb);
+        } else if (spin1) {
+          ka = fma(Pa[ix], exch, ka);
         } else {
           ka = fma(0.5 * Pt[ix], exch, ka);
         }

@@ -97,7 +97,8 @@ EXPORTS = [
     "pm3gpu_tuning_choice",
     "pm3gpu_guess_train", "pm3gpu_guess_set_params", "pm3gpu_guess_get_params", "pm3gpu_guess_predict",
     "pm3gpu_standard_parameters", "pm3gpu_set_parameters", "pm3gpu_guess_gradients",
-    "pm3gpu_set_large_checks", "pm3gpu_last_large_checks", "pm3gpu_split_gemm",
+    "pm3gpu_set_large_checks", "pm3gpu_last_large_checks", "pm3gpu_split_gemm", "pm3gpu_set_tail_helpers",
+    "pm3gpu_last_paired_jobs",
 ]
 
 _lib = None
@@ -148,6 +149,8 @@ def load() -> ctypes.CDLL:
     L.pm3gpu_tuning_choice.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.pm3gpu_last_large_trace.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     L.pm3gpu_set_large_checks.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.pm3gpu_set_tail_helpers.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.pm3gpu_last_paired_jobs.argtypes = [ctypes.c_void_p]
     L.pm3gpu_split_gemm.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D,
                                     ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     L.pm3gpu_last_large_checks.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
