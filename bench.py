@@ -781,6 +781,9 @@ def main():
     ap.add_argument("--tuned-train", type=int, default=8192,
                     help="tuned arm: molecules (same generator, another seed) whose converged densities train the "
                          "learned initial density before timing")
+    ap.add_argument("--tail-helpers", action="store_true",
+                    help="batched workloads: idle CTAs take the beta spin of unaccelerated unrestricted jobs "
+                         "(pm3gpu_set_tail_helpers) in every arm")
     ap.add_argument("--no-large", dest="large", action="store_false",
                     help="organics workload: skip the 6000-atom record (2000-water cluster, FP64 and mixed s/SCF, "
                          "first-iteration parity against the CPU oracle, CPU time extrapolated)")
@@ -868,6 +871,8 @@ def main():
         out = []
         for _ in range(max(1, n)):
             c = _lib.Context(local)
+            if args.tail_helpers and lib.pm3gpu_set_tail_helpers(c.ptr, 1) != 0:
+                raise RuntimeError(c.last_error())
             if setup:
                 setup(c)
             st = torch.cuda.Stream(dev)
@@ -1016,7 +1021,8 @@ def main():
                    "submission": (f"slot k submits its first batch k x {1e3 * plain['stagger']:.0f} ms into the timed "
                                   "region (one batch time / slots), then back to back")
                    if args.inflight > 1 else "one batch at a time",
-                   "converged_fraction": conv / (n_mol * args.steps * world)},
+                   "converged_fraction": conv / (n_mol * args.steps * world),
+                   "tail_helpers": bool(args.tail_helpers)},
         "e2e": {"value": e2e, "unit": "SCF/s", "h2d_bytes_per_step": plain["h2d"], "d2h_bytes_per_step": plain["d2h"]},
         "gpu_launches": plain["launches"],
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
