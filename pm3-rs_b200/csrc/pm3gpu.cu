@@ -466,6 +466,9 @@ long long pair_table_doubles(const pm3gpu_ctx* c, const int32_t* z, int natom) {
   return (s * s - s2) / 2;
 }
 
+// Static shared memory of scf_batch_kernel (set when a context is created).
+int g_scf_static_smem = 1024;
+
 // Shared-memory carve-up of one launch. The packed eigen input lives in shared memory for
 // bases up to `nsm` (global memory above). When `naos` is given, the layout is shrunk to let
 // two CTAs share an SM as long as at least 90% of the launch's jobs still fit in shared memory.
@@ -493,7 +496,7 @@ SmemLayout make_layout(int amax, int nmax, int optin, int smem_per_sm = 0, const
   };
   int nsm = fit(optin);
   if (smem_per_sm > 0 && ctas != 1 && (ctas == 2 || (naos && !naos->empty()))) {
-    const int budget2 = smem_per_sm / 2 - 1024 - 512;  // per-CTA reservation and static shared memory
+    const int budget2 = smem_per_sm / 2 - 1024 - g_scf_static_smem;  // per-CTA reservation, static shared memory
     const int nsm2 = fit(budget2);
     if (nsm2 < nsm && off + fixed_union * 8 <= budget2) {
       if (ctas == 2) {
@@ -1354,11 +1357,15 @@ int pm3gpu_context_create(int device, pm3gpu_ctx** out) {
   cudaDeviceProp prop;
   if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) return bail(e);
   c->sms = prop.multiProcessorCount;
-  c->smem_optin = (int)prop.sharedMemPerBlockOptin;
-  c->smem_per_sm = (int)prop.sharedMemPerMultiprocessor;
   // The dynamic shared-memory limit is an attribute of the kernel for the whole process, not of
-  // one context: it is raised once to the device's opt-in maximum, so that concurrent contexts
-  // never lower it under one another's launches (each launch asks for its own layout's bytes).
+  // one context: it is raised once to the most the device allows beside the kernel's static shared
+  // memory, so that concurrent contexts never lower it under one another's launches (each launch
+  // asks for its own layout's bytes, which make_layout keeps within the same budget).
+  cudaFuncAttributes fa{};
+  if ((e = cudaFuncGetAttributes(&fa, scf_batch_kernel)) != cudaSuccess) return bail(e);
+  c->smem_optin = (int)prop.sharedMemPerBlockOptin - (int)fa.sharedSizeBytes;
+  g_scf_static_smem = std::max(512, (int)fa.sharedSizeBytes);
+  c->smem_per_sm = (int)prop.sharedMemPerMultiprocessor;
   if ((e = cudaFuncSetAttribute(scf_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, c->smem_optin)) !=
       cudaSuccess)
     return bail(e);
