@@ -588,6 +588,9 @@ def tuned_arm(args, lib, ctx0, make_slots, measure, plain_opts, gpu_opts, plain,
     rad = args.workload == "radicals-2048"
     c_off, c_z, c_xyz = packed(molecules(256 if rad else 1024, seed=777, workload=args.workload))
     path = os.path.join(tempfile.mkdtemp(prefix="pm3gpu_tuning_"), f"tuning_{args.workload}.json")
+    # the arms run batches in flight: tune for the rate of the bulk of a batch
+    if lib.pm3gpu_set_tuning_goal(ctx0.ptr, _lib.TUNE_THROUGHPUT if args.inflight > 1 else _lib.TUNE_BATCH_TIME) != 0:
+        raise RuntimeError(ctx0.last_error())
     if lib.pm3gpu_autotune(ctx0.ptr, len(c_off) - 1, c_off.ctypes.data_as(I32), c_z.ctypes.data_as(I32),
                            c_xyz.ctypes.data_as(D), ctypes.byref(plain_opts), path.encode()) != 0:
         raise RuntimeError(ctx0.last_error())
@@ -646,7 +649,8 @@ def tuned_arm(args, lib, ctx0, make_slots, measure, plain_opts, gpu_opts, plain,
         "max_abs_dhf_kcal_vs_plain": float(dhf.max()) if dhf.size else None,
         "molecules_dhf_above_0.01_kcal": int((dhf > 0.01).sum()),
         "converged_fraction": r["conv"] / (n_mol * args.steps),
-        "modes": {"launch": "autotuned (calibration sample: 1024 other molecules of the generator)",
+        "modes": {"launch": "autotuned (calibration sample: 1024 other molecules of the generator; goal: "
+                            + ("throughput, batches in flight)" if args.inflight > 1 else "batch time)"),
                   "guess": f"learned, trained before timing on {len(t_off) - 1} other molecules ({epochs} epochs)",
                   "precision": "mixed (split-BF16 tcgen05 products where the path has them, FP64 closing iterations)"},
         "setup_seconds": setup_s, "train_loss_per_epoch": [float(v) for v in losses], "tuning": tuning.get("batch"),

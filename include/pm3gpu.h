@@ -266,6 +266,13 @@ int pm3gpu_set_large_threshold(pm3gpu_ctx* ctx, int nao);
  * pm3gpu_tuning_choice returns the choice a size would get (kind 0: CTAs per SM for a
  * batch whose largest basis is `size`; kind 1: 1 = cooperative panels for basis `size`), or -1
  * when no tuned bucket covers it. */
+/* What pm3gpu_autotune minimises for the batched launch: PM3GPU_TUNE_BATCH_TIME (default), the time
+ * of one whole batch, tail included (one batch at a time); PM3GPU_TUNE_THROUGHPUT, the time until
+ * 90% of the first passes have ended, the rate of the bulk of a batch (batches in flight, where one
+ * batch's tail overlaps the next). The times written to the JSON file are of the chosen goal. */
+#define PM3GPU_TUNE_BATCH_TIME 0
+#define PM3GPU_TUNE_THROUGHPUT 1
+int pm3gpu_set_tuning_goal(pm3gpu_ctx* ctx, int goal);
 int pm3gpu_autotune(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
                     const double* xyz_bohr, const pm3gpu_options* opts, const char* cache_path);
 int pm3gpu_load_tuning(pm3gpu_ctx* ctx, const char* path);

@@ -95,6 +95,10 @@ struct pm3gpu_ctx {
   PairDev h_pairs;
   DevBuf elem, pairs, z, xyz, jobs, out, charges, dens, grads, eps, work, queue, rq, gmols, aooff, help;
   bool tail_helpers = false;  // idle CTAs take the beta spin of unaccelerated unrestricted jobs
+  int tune_goal = 0;           // autotuner: 0 batch time, 1 throughput with batches in flight
+  bool record_jobs = false;    // time each first pass's end (the autotuner's throughput goal)
+  DevBuf tjob;
+  std::vector<unsigned long long> job_ns;  // last launch: first-pass end times, then the start
   int paired = 0;              // jobs of the last call that ran on two CTAs
   int sms = 0, smem_optin = 0, smem_per_sm = 0;
   double timings[6] = {0, 0, 0, 0, 0, 0};
@@ -593,6 +597,11 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
     CUDA_TRY(c, cudaMemcpyAsync(c->dens.p, dens_in->data(), 8 * dens_in->size(), cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaMemsetAsync(c->queue.p, 0, 64, c->stream));
   if (c->tail_helpers) CUDA_TRY(c, cudaMemsetAsync(c->help.p, 0, sizeof(HelpRec) * (size_t)grid, c->stream));
+  if (c->record_jobs) {
+    CUDA_TRY(c, c->tjob.ensure(8 * (size_t)(nj + 1)));
+    CUDA_TRY(c, cudaMemsetAsync(c->tjob.p, 0, 8 * (size_t)nj, c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->tjob.as<unsigned long long>() + nj, 0xff, 8, c->stream));
+  }
   CUDA_TRY(c, cudaMemsetAsync(c->rq.p, 0, 2 * sizeof(int) * std::max(nr, 1), c->stream));
   if (nr) CUDA_TRY(c, cudaMemsetAsync(c->out.as<JobOut>() + nj, 0xff, sizeof(JobOut) * nr, c->stream));
   KernelArgs a{};
@@ -620,6 +629,7 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   a.queue = c->queue.as<int>();
   a.prof = nullptr;
   a.help = c->tail_helpers ? c->help.as<HelpRec>() : nullptr;
+  a.tjob = c->record_jobs ? c->tjob.as<unsigned long long>() : nullptr;
   if (c->profile) {
     CUDA_TRY(c, c->prof.ensure(sizeof(unsigned long long) * kPhases));
     CUDA_TRY(c, cudaMemsetAsync(c->prof.p, 0, sizeof(unsigned long long) * kPhases, c->stream));
@@ -647,6 +657,10 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   if (read_eps && tot.eps) {
     R.eps.resize(tot.eps);
     CUDA_TRY(c, cudaMemcpyAsync(R.eps.data(), c->eps.p, 8 * tot.eps, cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (c->record_jobs) {
+    c->job_ns.resize(nj + 1);
+    CUDA_TRY(c, cudaMemcpyAsync(c->job_ns.data(), c->tjob.p, 8 * (size_t)(nj + 1), cudaMemcpyDeviceToHost, c->stream));
   }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   if (qh[3]) return fail(c, PM3GPU_CUDA_ERROR, "a bounded wait of the batched SCF kernel ran out on the device");
@@ -1916,6 +1930,13 @@ int pm3gpu_set_tail_helpers(pm3gpu_ctx* c, int on) {
 }
 
 int pm3gpu_last_paired_jobs(pm3gpu_ctx* c) { return c ? c->paired : 0; }
+
+int pm3gpu_set_tuning_goal(pm3gpu_ctx* c, int goal) {
+  if (!c || (goal != PM3GPU_TUNE_BATCH_TIME && goal != PM3GPU_TUNE_THROUGHPUT)) return fail(c, PM3GPU_INVALID_INPUT, "bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->tune_goal = goal;
+  return PM3GPU_OK;
+}
 
 int pm3gpu_set_large_checks(pm3gpu_ctx* c, int on) {
   if (!c) return PM3GPU_INVALID_INPUT;

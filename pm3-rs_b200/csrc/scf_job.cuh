@@ -7,6 +7,12 @@
 namespace pm3gpu {
 
 // ------------------------------------------------------------------------------- one job
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Bounded wait of one thread for *p >= want (about a second at most). False when it ran out.
 __device__ __forceinline__ bool wait_at_least(const volatile int* p, int want) {
   for (int i = 0; i < (1 << 22); ++i) {
@@ -615,6 +621,7 @@ __global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args)
 
   slot_ptrs(c, args.work + (size_t)blockIdx.x * args.slot, args.nmax);
 
+  if (args.tjob && threadIdx.x == 0) atomicMin(&args.tjob[args.njobs], globaltimer_ns());
   __shared__ unsigned long long s_ph[kPhases];
   c.ph = s_ph;
   if (threadIdx.x < kPhases) s_ph[threadIdx.x] = 0ULL;
@@ -704,6 +711,7 @@ __global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args)
       if (threadIdx.x == 0) {  // after its rungs (if any) are queued
         __threadfence();
         atomicAdd(&q[4], 1);
+        if (args.tjob) args.tjob[jid] = globaltimer_ns();
       }
     } else {
       run_job(c, args.rjobs[jid], args.rout + jid, 1, jid);

@@ -100,6 +100,7 @@ struct KernelArgs {
   unsigned long long* prof;  // [kPhases] SM cycles per phase, summed over CTAs (null = off)
   SmemLayout sm;
   struct HelpRec* help;  // [grid] per CTA: its unrestricted job's offer of the beta spin (null = off)
+  unsigned long long* tjob;  // [njobs + 1] global-timer ns when each first pass ended, [njobs] the start (null = off)
 };
 
 // One CTA's offer of the beta spin of its unrestricted job to an idle CTA (a "helper"). `sg`

@@ -12,6 +12,8 @@ GUESS_LEARNED = 4
 GUESS_PARAMS = 150280
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+TUNE_BATCH_TIME = 0
+TUNE_THROUGHPUT = 1
 INVALID_INPUT = 1
 MISSING_ELEMENT = 2
 RESOURCE_LIMIT = 3
@@ -98,7 +100,7 @@ EXPORTS = [
     "pm3gpu_guess_train", "pm3gpu_guess_set_params", "pm3gpu_guess_get_params", "pm3gpu_guess_predict",
     "pm3gpu_standard_parameters", "pm3gpu_set_parameters", "pm3gpu_guess_gradients",
     "pm3gpu_set_large_checks", "pm3gpu_last_large_checks", "pm3gpu_split_gemm", "pm3gpu_set_tail_helpers",
-    "pm3gpu_last_paired_jobs",
+    "pm3gpu_last_paired_jobs", "pm3gpu_set_tuning_goal",
 ]
 
 _lib = None
@@ -151,6 +153,7 @@ def load() -> ctypes.CDLL:
     L.pm3gpu_set_large_checks.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.pm3gpu_set_tail_helpers.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.pm3gpu_last_paired_jobs.argtypes = [ctypes.c_void_p]
+    L.pm3gpu_set_tuning_goal.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.pm3gpu_split_gemm.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D,
                                     ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     L.pm3gpu_last_large_checks.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]

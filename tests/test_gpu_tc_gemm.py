@@ -39,8 +39,8 @@ def test_split_gemm_matches_fp64_product(m, n, k):
     bound = 4e-5 * (np.abs(a) @ np.abs(b).T) + 1e-30
     err = np.abs(got - ref)
     assert np.all(err <= bound), float((err / bound).max())
-    # far better than plain BF16 (2^-9): the split is what gives FP32-level products
-    assert np.median(err / (np.abs(a) @ np.abs(b).T)) < 1e-6
+    # far better than plain BF16 (2^-9 = 2e-3): the split is what gives FP32-level products
+    assert np.median(err / (np.abs(a) @ np.abs(b).T)) < 4e-6
 
 
 def test_split_gemm_symmetric_products_of_the_scf():
