@@ -222,9 +222,10 @@ def fp64_gemm_peak(dev):
 PHASES = ["core", "fock", "commutator", "diis_solve", "pack", "tridiagonalise", "eigenvalues", "eigenvectors",
           "back_transform", "density", "final", "gradient"]
 # DRAM bytes (read + write) of one scf_batch_kernel launch per molecule of this workload, from an
-# ncu capture of a 256-molecule batch (7.43 GB); the per-CTA workspaces of 296 resident CTAs
-# exceed L2, so the SCF matrices stream from HBM. Scaled to a launch by the molecules it solves.
-DRAM_BYTES_PER_MOLECULE = 7.43e9 / 256
+# ncu capture of a 256-molecule batch at the plain arm's launch choice (5.88 GB); the per-CTA
+# workspaces of 296 resident CTAs exceed L2, so the SCF matrices stream from HBM. Scaled to a
+# launch by the molecules it solves.
+DRAM_BYTES_PER_MOLECULE = 5.88e9 / 256
 
 
 def scf_flops(nao, n_occ, iters):
