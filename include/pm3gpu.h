@@ -229,7 +229,8 @@ int pm3gpu_fock(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const double* xy
 /* Phase timings of the last call (milliseconds, CUDA events): [0] upload, [1] the batched launch
  * (first passes and stability rungs of the per-CTA molecules), [2] selection, whole-GPU molecules
  * and gradients, [3] the SCF passes of the whole-GPU molecules alone (first pass and stability
- * rungs, no gradient), [4] total, [5] time inside the batched SCF kernel.
+ * rungs, no gradient), [4] total, [5] time inside the batched SCF kernel, [6] the learned-guess
+ * inference (features, network, assembly) before the batched launch.
  * Returns the count written. */
 int pm3gpu_last_timings(pm3gpu_ctx* ctx, double* ms, int max_entries);
 

@@ -101,11 +101,12 @@ struct pm3gpu_ctx {
   std::vector<unsigned long long> job_ns;  // last launch: first-pass end times, then the start
   int paired = 0;              // jobs of the last call that ran on two CTAs
   int sms = 0, smem_optin = 0, smem_per_sm = 0;
-  double timings[6] = {0, 0, 0, 0, 0, 0};
+  double timings[7] = {0, 0, 0, 0, 0, 0, 0};
   int launches = 0;
   long long h2d = 0, d2h = 0;  // bytes moved by the last call
   cudaEvent_t ev[6] = {};
   cudaEvent_t kev[2] = {};
+  cudaEvent_t gev[2] = {};  // around the learned-guess inference of a batch (timings[6])
   bool profile = false;
   DevBuf prof;
   double phase_cycles[kPhases] = {};
@@ -1023,6 +1024,8 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
   c->paired = 0;
   c->timings[3] = 0.0;
   c->timings[5] = 0.0;
+  c->timings[6] = 0.0;
+  bool guess_timed = false;
   c->h2d = c->d2h = 0;
   for (int k = 0; k < kPhases; ++k) c->phase_cycles[k] = 0.0;
   cudaEventRecord(c->ev[0], c->stream);
@@ -1100,10 +1103,13 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
       }
     }
     if (!lmol.empty()) {
+      CUDA_TRY(c, cudaEventRecord(c->gev[0], c->stream));
       GuessRows G;
       guess_rows(c, la0, lna, h_z, total_atoms, G);
       const int rg = guess_infer(c, G, dz, dxyz, total_atoms);
       if (rg != PM3GPU_OK) return rg;
+      CUDA_TRY(c, cudaEventRecord(c->gev[1], c->stream));
+      guess_timed = true;
       for (size_t k = 0; k < lmol.size(); ++k) jobs[plans[lmol[k]].first_job].guess_off = G.mols[k].dens_off;
     }
   }
@@ -1119,6 +1125,11 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
   LaunchOut R;
   int rc = launch_jobs(c, sorted, rjobs, zs, dz, dxyz, tot, want.density, want.eps, R);
   if (rc != PM3GPU_OK) return rc;
+  if (guess_timed) {  // the launch has synchronised the stream
+    float gms = 0.f;
+    CUDA_TRY(c, cudaEventElapsedTime(&gms, c->gev[0], c->gev[1]));
+    c->timings[6] = gms;
+  }
   cudaEventRecord(c->ev[2], c->stream);
 
   // ---------------------------------------------------------------- selection + epilogue
@@ -1367,7 +1378,8 @@ int pm3gpu_context_create(int device, pm3gpu_ctx** out) {
   for (int k = 0; k < 6; ++k)
     if ((e = cudaEventCreate(&c->ev[k])) != cudaSuccess) return bail(e);
   for (int k = 0; k < 2; ++k)
-    if ((e = cudaEventCreate(&c->kev[k])) != cudaSuccess) return bail(e);
+    if ((e = cudaEventCreate(&c->kev[k])) != cudaSuccess || (e = cudaEventCreate(&c->gev[k])) != cudaSuccess)
+      return bail(e);
   cudaDeviceProp prop;
   if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) return bail(e);
   c->sms = prop.multiProcessorCount;
@@ -1408,8 +1420,10 @@ void pm3gpu_context_destroy(pm3gpu_ctx* c) {
     b->release();
   for (int k = 0; k < 6; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
-  for (int k = 0; k < 2; ++k)
+  for (int k = 0; k < 2; ++k) {
     if (c->kev[k]) cudaEventDestroy(c->kev[k]);
+    if (c->gev[k]) cudaEventDestroy(c->gev[k]);
+  }
   if (c->lbuf) {
     c->lbuf->release();
     delete c->lbuf;
@@ -1582,7 +1596,7 @@ int pm3gpu_fock(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz,
 
 int pm3gpu_last_timings(pm3gpu_ctx* c, double* ms, int max_entries) {
   if (!c || !ms) return 0;
-  const int k = std::min(max_entries, 6);
+  const int k = std::min(max_entries, 7);
   for (int i = 0; i < k; ++i) ms[i] = c->timings[i];
   return k;
 }

@@ -532,58 +532,83 @@ __host__ __device__ bool cdiis_coeffs(int m, const double* gram, double* x) {
 // lane k owns weight c_k and its gradient component; the Euclidean projection onto the simplex
 // sorts the trial point (descending, ties by index, as a stable insertion sort does) and every
 // lane runs the reference's serial cumulative-sum scan over the sorted values, so the weights are
-// the ones the serial loop produces. `sm` is shared scratch of kMaxDepth * (kMaxDepth + 1) doubles.
+// the ones the serial loop produces. `sm` is shared scratch of kMaxDepth * (2 kMaxDepth + 1) doubles.
 __device__ void adiis_coeffs_warp(int m, const double* mg, double* out, double* sm) {
+  constexpr int K = kMaxDepth;
   const int k = threadIdx.x & 31;
   const int last = m - 1;
-  const double mnn = mg[last * kMaxDepth + last];
-  double* S = sm;                       // [kMaxDepth][kMaxDepth]
-  double* d = sm + kMaxDepth * kMaxDepth;  // [kMaxDepth]
+  const double mnn = mg[last * K + last];
+  double* S = sm;           // [K][K]
+  double* T = sm + K * K;   // [K][K] S + S^T, the gradient's matrix (same sums as the reference's)
+  double* d = T + K * K;    // [K]
   if (k < m) {
-    d[k] = mg[k * kMaxDepth + last] - mnn;
-    for (int j = 0; j < m; ++j)
-      S[k * kMaxDepth + j] = mg[k * kMaxDepth + j] - mg[k * kMaxDepth + last] - mg[last * kMaxDepth + j] + mnn;
+    d[k] = mg[k * K + last] - mnn;
+    for (int j = 0; j < m; ++j) S[k * K + j] = mg[k * K + j] - mg[k * K + last] - mg[last * K + j] + mnn;
   }
+  __syncwarp();
+  if (k < m)
+    for (int j = 0; j < m; ++j) T[k * K + j] = S[k * K + j] + S[j * K + k];
   __syncwarp();
   double L = 1.0e-12;
   for (int i = 0; i < m; ++i) {
     double row = 0.0;
-    for (int j = 0; j < m; ++j) row += fabs(S[i * kMaxDepth + j] + S[j * kMaxDepth + i]);
+    for (int j = 0; j < m; ++j) row += fabs(T[i * K + j]);
     L = fmax(L, row);
   }
   const double lr = 1.0 / L;
-  double ck = k == last ? 1.0 : 0.0;
+  // Every lane runs the whole iteration on the full state in registers (the lanes agree), so the
+  // loop needs no shuffles: gradient, trial point, its stable descending order, the reference's
+  // cumulative-sum scan for the simplex projection, and the change.
+  double c[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) c[j] = j == last ? 1.0 : 0.0;
   for (int it = 0; it < 400; ++it) {
-    double tr = 0.0;
-    if (k < m) {
-      double g = 2.0 * d[k];
-      for (int j = 0; j < m; ++j) g += (S[k * kMaxDepth + j] + S[j * kMaxDepth + k]) * __shfl_sync(0xffffffffu, ck, j);
-      tr = ck - lr * g;
-    } else {
-      for (int j = 0; j < m; ++j) (void)__shfl_sync(0xffffffffu, ck, j);
+    double t[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      double g = 2.0 * d[q < m ? q : 0];
+#pragma unroll
+      for (int j = 0; j < K; ++j)
+        if (j < m) g += T[q * K + j] * c[j];
+      t[q] = q < m ? c[q] - lr * g : 0.0;
     }
-    // rank of tr_k in descending order (ties: lower index first)
-    int rank = 0;
-    for (int j = 0; j < m; ++j) {
-      const double tj = __shfl_sync(0xffffffffu, tr, j);
-      rank += (tj > tr || (tj == tr && j < k)) ? 1 : 0;
+    // the trial point sorted descending by a 19-comparator network on a copy (unused entries
+    // -inf, so they sort last); ties give equal values in either order, so the cumulative sums,
+    // and with them the projection, are those of the reference's stable sort
+    double u[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) u[q] = q < m ? t[q] : -INFINITY;
+    constexpr int kNet[19][2] = {{0, 2}, {1, 3}, {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}, {0, 1}, {2, 3},
+                                 {4, 5}, {6, 7}, {2, 4}, {3, 5}, {1, 4}, {3, 6}, {1, 2}, {3, 4}, {5, 6}};
+#pragma unroll
+    for (int e = 0; e < 19; ++e) {
+      const double a = u[kNet[e][0]], b = u[kNet[e][1]];
+      u[kNet[e][0]] = fmax(a, b);
+      u[kNet[e][1]] = fmin(a, b);
     }
     double css = 0.0, theta = 0.0;
-    for (int p = 0; p < m; ++p) {
-      const unsigned who = __ballot_sync(0xffffffffu, k < m && rank == p);
-      const double up = __shfl_sync(0xffffffffu, tr, __ffs(who) - 1);
-      css += up;
-      const double t = (css - 1.0) / (double)(p + 1);
-      if (up - t > 0.0) theta = t;
+#pragma unroll
+    for (int p = 0; p < K; ++p) {
+      if (p >= m) break;
+      css += u[p];
+      const double tt = (css - 1.0) / (double)(p + 1);
+      if (u[p] - tt > 0.0) theta = tt;
     }
-    const double pk = k < m ? fmax(tr - theta, 0.0) : 0.0;
-    const double dk = k < m ? fabs(pk - ck) : 0.0;
     double delta = 0.0;
-    for (int i = 0; i < m; ++i) delta += __shfl_sync(0xffffffffu, dk, i);
-    ck = pk;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      if (q >= m) break;
+      const double pq = fmax(t[q] - theta, 0.0);
+      delta += fabs(pq - c[q]);
+      c[q] = pq;
+    }
     if (delta < 1.0e-12) break;
   }
-  if (k < m) out[k] = ck;
+  if (k < m) {
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+      if (q == k) out[k] = c[q];
+  }
   __syncwarp();
 }
 
