@@ -305,8 +305,9 @@ int pm3gpu_split_gemm(pm3gpu_ctx* ctx, int m, int n, int k, const double* a, int
  * most max_rows rows and returns the total number of rows. */
 int pm3gpu_last_large_trace(pm3gpu_ctx* ctx, double* rows, int max_rows);
 
-/* Batched launch (no counterpart in the reference): with on = 1, CTAs left without work near the
- * end of a batch take the beta spin of unaccelerated unrestricted jobs still running (the
+/* Batched launch (no counterpart in the reference): with on = 1, up to 32 CTAs left without work
+ * near the end of a batch stay for stability rungs queued late and take the beta spin of
+ * unaccelerated unrestricted jobs still running (the
  * reference's UHF loop without DIIS, src/scf.rs:1319-1496): from the next iteration on, the two
  * CTAs build F_alpha and F_beta, diagonalise and form the two spin densities side by side and
  * exchange energy parts and density changes each iteration (bounded waits). It shortens the tail

@@ -55,6 +55,25 @@ __device__ __forceinline__ double block_sum_alt(double v, double* red, int& pari
   return t;
 }
 
+// row[c] -= v_row w_c + w_row v_c for c in [c0, c1] (w_c = p_c + a2 v_c), four at a time.
+__device__ __forceinline__ void update_row(double* __restrict__ row, int c0, int c1, double vr, double wr, double a2,
+                                           const double* __restrict__ v, const double* __restrict__ p) {
+  int c = c0;
+  for (; c + 3 <= c1; c += 4) {
+    const double v0 = v[c], v1 = v[c + 1], v2 = v[c + 2], v3 = v[c + 3];
+    const double w0 = p[c] + a2 * v0, w1 = p[c + 1] + a2 * v1, w2 = p[c + 2] + a2 * v2, w3 = p[c + 3] + a2 * v3;
+    const double a0 = row[c], a1 = row[c + 1], a2_ = row[c + 2], a3 = row[c + 3];
+    row[c] = a0 - (vr * w0 + wr * v0);
+    row[c + 1] = a1 - (vr * w1 + wr * v1);
+    row[c + 2] = a2_ - (vr * w2 + wr * v2);
+    row[c + 3] = a3 - (vr * w3 + wr * v3);
+  }
+  for (; c <= c1; ++c) {
+    const double vc = v[c], wc = p[c] + a2 * vc;
+    row[c] -= vr * wc + wr * vc;
+  }
+}
+
 // Householder reduction, one thread per row (n <= kThreads): thread r owns row r of the packed
 // lower triangle for the matrix-vector product (its row segment plus the column below it) and
 // for the rank-2 update of its row segment, and contributes its element of the next column to
@@ -125,29 +144,31 @@ __device__ void tridiagonalize(int n, double* __restrict__ A, const EigenScratch
       s.p[r] = y;
     }
     const double a2 = -0.5 * tau * block_sum_alt(mine ? y * vr : 0.0, s.red, parity);
-    // A22 -= v w^T + w v^T on row r (w = p + a2 v), keeping the next column's norm part
+    // A22 -= v w^T + w v^T (w = p + a2 v) on the row segments c in (i, r], keeping the next
+    // column's norm part. Row r has r - i elements, so the segments are balanced in pairs: the
+    // thread of a short row (length l < H, H half the longest plus one) also takes the first
+    // H - l elements of the complementary long row n + i - r (length L + 1 - l, L = n - i - 1),
+    // whose own thread then starts after them; every thread does about H elements.
     double part = 0.0;
     if (mine) {
+      const int L = n - i - 1, H = (L + 2) / 2;
+      const int len = r - i, mate = n + i - r, len_mate = n - r;
+      // own row: skip the head that the short row's thread takes
+      const int c0 = (len >= H && len_mate < H && mate != r) ? i + 1 + (H - len_mate) : i + 1;
       const double wr = y + a2 * vr;
-      double* row = A + tr;
-      int c = i + 1;
-      for (; c + 3 <= r; c += 4) {
-        const double v0 = s.v[c], v1 = s.v[c + 1], v2 = s.v[c + 2], v3 = s.v[c + 3];
-        const double w0 = s.p[c] + a2 * v0, w1 = s.p[c + 1] + a2 * v1, w2 = s.p[c + 2] + a2 * v2,
-                     w3 = s.p[c + 3] + a2 * v3;
-        const double a0 = row[c], a1 = row[c + 1], a2_ = row[c + 2], a3 = row[c + 3];
-        row[c] = a0 - (vr * w0 + wr * v0);
-        row[c + 1] = a1 - (vr * w1 + wr * v1);
-        row[c + 2] = a2_ - (vr * w2 + wr * v2);
-        row[c + 3] = a3 - (vr * w3 + wr * v3);
-      }
-      for (; c <= r; ++c) {
-        const double vc = s.v[c], wc = s.p[c] + a2 * vc;
-        row[c] -= vr * wc + wr * vc;
-      }
-      if (r >= i + 3) {
-        const double x = row[i + 1];
+      update_row(A + tr, c0, r, vr, wr, a2, s.v, s.p);
+      if (c0 == i + 1 && r >= i + 3) {
+        const double x = A[tr + i + 1];
         part = x * x;
+      }
+      if (len < H && mate != r) {  // head of the complementary long row
+        const int tm = tri(mate);
+        const double vm = s.v[mate], wm = s.p[mate] + a2 * vm;
+        update_row(A + tm, i + 1, i + H - len, vm, wm, a2, s.v, s.p);
+        if (mate >= i + 3) {
+          const double x = A[tm + i + 1];
+          part += x * x;
+        }
       }
     }
     xn2 = block_sum_alt(part, s.red, parity);
@@ -375,9 +396,10 @@ __device__ void tridiag_vectors(int n, int kvec, double* Y, double* tf, const Ei
   const double win = 1.0e-11 * fmax(tnorm, 1.0);
   for (int j = tid; j < kvec; j += kThreads) {
     const double lam = s.lam[j];
-    // which unreduced block holds this eigenvalue (degenerate copies go to successive blocks)
-    int pos = j - sturm(s.d, s.e2, 0, n - 1, lam - win, pivmin);
-    int b = -1, sub = 0;
+    // which unreduced block holds this eigenvalue (degenerate copies go to successive blocks);
+    // an unsplit T (the usual case) has one block, and the three Sturm counts are not needed
+    int pos = nb == 1 ? 0 : j - sturm(s.d, s.e2, 0, n - 1, lam - win, pivmin);
+    int b = nb == 1 ? 0 : -1, sub = 0;
     for (int q = 0; q < nb && b < 0; ++q) {
       const int lo = s.blk[q], hi = s.blk[q + 1] - 1;
       const int c = sturm(s.d, s.e2, lo, hi, lam + win, pivmin) - sturm(s.d, s.e2, lo, hi, lam - win, pivmin);

@@ -630,6 +630,9 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   a.queue = c->queue.as<int>();
   a.prof = nullptr;
   a.help = c->tail_helpers ? c->help.as<HelpRec>() : nullptr;
+  // With tail helpers, up to 32 idle CTAs stay for late stability rungs and unrestricted jobs to
+  // help; otherwise idle CTAs exit and free their SM for the next batch in flight.
+  a.max_waiters = c->tail_helpers ? 32 : 0;
   a.tjob = c->record_jobs ? c->tjob.as<unsigned long long>() : nullptr;
   if (c->profile) {
     CUDA_TRY(c, c->prof.ensure(sizeof(unsigned long long) * kPhases));

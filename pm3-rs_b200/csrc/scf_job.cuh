@@ -569,8 +569,6 @@ __device__ __noinline__ void help_job(Ctx& c, int L, int mygen) {
 }
 
 // ----------------------------------------------------------------------- the kernel
-// CTAs that may stay, once the first passes are all taken, for stability rungs still to come.
-constexpr int kMaxWaiters = 32;
 
 __global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -666,7 +664,7 @@ __global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args)
           continue;
         }
         // No job to take. While first passes are still running they may queue stability rungs
-        // (q[4] counts finished first passes); up to kMaxWaiters CTAs stay for them, sleeping
+        // (q[4] counts finished first passes); up to max_waiters CTAs stay for them, sleeping
         // between polls, so that late rungs run side by side instead of one after another on the
         // CTA that queued them. The rest exit and free their SM for other work. Bounded by the
         // guard: a CTA that waits too long exits (its rungs still run on the queuing CTA).
@@ -687,7 +685,8 @@ __global__ void __launch_bounds__(kThreads, 2) scf_batch_kernel(KernelArgs args)
         }
         if (!offers && atomicAdd(&q[4], 0) >= args.njobs) break;
         if (!waiting) {
-          if (atomicAdd(&q[5], 1) >= kMaxWaiters) {
+          if (args.max_waiters <= 0) break;
+          if (atomicAdd(&q[5], 1) >= args.max_waiters) {
             atomicSub(&q[5], 1);
             break;
           }

@@ -101,6 +101,7 @@ struct KernelArgs {
   SmemLayout sm;
   struct HelpRec* help;  // [grid] per CTA: its unrestricted job's offer of the beta spin (null = off)
   unsigned long long* tjob;  // [njobs + 1] global-timer ns when each first pass ended, [njobs] the start (null = off)
+  int max_waiters;       // CTAs that may stay, once the first passes are all taken, for work still to come
 };
 
 // One CTA's offer of the beta spin of its unrestricted job to an idle CTA (a "helper"). `sg`
