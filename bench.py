@@ -10,11 +10,12 @@ own 4096 molecules (seed offset by rank): weak scaling, no data-path collective.
 
 `value`: inputs (atom numbers and coordinates) already resident in HBM, CUDA-event time on the
 device. `e2e`: the same through the host C ABI (pm3gpu_batch) from pinned host buffers,
-host<->device copies inside the timed region. By default three batches are in flight (three
+host<->device copies inside the timed region. By default four batches are in flight (four
 contexts, each with its own stream and host thread) and the device time spans all K steps; L2 is
 flushed (a 512 MiB write) before them and the per-CTA workspaces exceed L2. With `--inflight 1`
-each step is timed alone with a flush between steps. Before timing, the autotuner calibrates the
-launch choice on another sample of the same generator (`--no-autotune` skips it).
+each step is timed alone with a flush between steps. The headline (plain) arm uses the built-in
+launch choice and the reference's defaults; the tuned arm beside it calibrates the launch choice
+on another sample of the same generator and adds the learned guess and mixed precision.
 `--impl reference` times the reference algorithm's CPU implementation (the C++ oracle that
 restates pm3-rs, linked to SciPy's OpenBLAS) on the host cores instead.
 """
@@ -772,7 +773,7 @@ def main():
     ap.add_argument("--epochs", type=int, default=6, help="learned-guess workload: training epochs")
     ap.add_argument("--waters", type=int, default=2000,
                     help="water-2000 workload: number of waters (the cluster uses the first sites of a 13 x 13 x 12 grid)")
-    ap.add_argument("--inflight", type=int, default=3,
+    ap.add_argument("--inflight", type=int, default=4,
                     help="batched workloads: batches in flight (contexts/streams/host threads); 1 times the batches "
                          "one after another")
     ap.add_argument("--save-guess", default=None,

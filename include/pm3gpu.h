@@ -248,6 +248,11 @@ int pm3gpu_last_transfer_bytes(pm3gpu_ctx* ctx, long long* h2d, long long* d2h);
 /* Number of this library's kernels launched by the last call. */
 int pm3gpu_last_kernel_launches(pm3gpu_ctx* ctx);
 
+/* Shape of the last batched SCF launch (no counterpart in the reference): CTAs resident per SM and
+ * the largest basis size whose packed eigen matrix stays in shared memory; larger molecules of that
+ * launch keep it in global memory until its trailing part fits. */
+int pm3gpu_last_launch_layout(pm3gpu_ctx* ctx, int* ctas_per_sm, int* smem_matrix_n);
+
 /* Molecules with at least `nao` basis functions are solved one at a time on the whole GPU
  * (grid-wide integral and Fock kernels, blocked eigensolver, cuBLAS DGEMM for the dense
  * products) instead of one CTA each. Default and maximum 257: every molecule beyond one CTA's

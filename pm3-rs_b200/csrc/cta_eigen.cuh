@@ -2,8 +2,8 @@
 // `self_adjoint_eigen` (pm3-rs src/linalg.rs:221-263) on the SCF path:
 //   1. Householder reduction to tridiagonal form, the matrix held as a packed lower triangle
 //      (row-major: element (r, c), r >= c, at r(r+1)/2 + c) in shared memory (or global memory
-//      when it does not fit), one thread per row. Reflectors stay in the strictly-lower part
-//      of column i.
+//      when it does not fit), a power-of-two group of threads per remaining row. Reflectors stay
+//      in the strictly-lower part of column i.
 //   2. Eigenvalues of the tridiagonal T by Sturm-count multisection, a group of lanes per
 //      eigenvalue, started from the previous SCF iteration's eigenvalues when given.
 //   3. Eigenvectors of T by twisted (N_r D_r N_r^T) factorisation, one thread per vector,
@@ -55,40 +55,26 @@ __device__ __forceinline__ double block_sum_alt(double v, double* red, int& pari
   return t;
 }
 
-// row[c] -= v_row w_c + w_row v_c for c in [c0, c1] (w_c = p_c + a2 v_c), four at a time.
-__device__ __forceinline__ void update_row(double* __restrict__ row, int c0, int c1, double vr, double wr, double a2,
-                                           const double* __restrict__ v, const double* __restrict__ p) {
-  int c = c0;
-  for (; c + 3 <= c1; c += 4) {
-    const double v0 = v[c], v1 = v[c + 1], v2 = v[c + 2], v3 = v[c + 3];
-    const double w0 = p[c] + a2 * v0, w1 = p[c + 1] + a2 * v1, w2 = p[c + 2] + a2 * v2, w3 = p[c + 3] + a2 * v3;
-    const double a0 = row[c], a1 = row[c + 1], a2_ = row[c + 2], a3 = row[c + 3];
-    row[c] = a0 - (vr * w0 + wr * v0);
-    row[c + 1] = a1 - (vr * w1 + wr * v1);
-    row[c + 2] = a2_ - (vr * w2 + wr * v2);
-    row[c + 3] = a3 - (vr * w3 + wr * v3);
-  }
-  for (; c <= c1; ++c) {
-    const double vc = v[c], wc = p[c] + a2 * vc;
-    row[c] -= vr * wc + wr * vc;
-  }
-}
-
-// Householder reduction, one thread per row (n <= kThreads): thread r owns row r of the packed
-// lower triangle for the matrix-vector product (its row segment plus the column below it) and
-// for the rank-2 update of its row segment, and contributes its element of the next column to
-// the next reflector's norm. Three barriers per column.
-__device__ void tridiagonalize(int n, double* __restrict__ A, const EigenScratch& s_) {
+// Householder reduction (n <= kThreads). For column i, the m = n - i - 1 trailing rows get T
+// threads each (T the largest power of two with T m <= kThreads, at most a warp), so that late
+// columns, with few rows left, still keep the CTA busy. The T threads of row r split the
+// matrix-vector product (its row segment c <= r, then the column below it) and the rank-2
+// update of its row segment by interleaved columns, and combine the product by shuffles; the
+// first of them contributes its element of the next column to the next reflector's norm.
+// Three barriers per column. This sweep reduces columns [0, i_stop) of the n x n matrix and, with
+// `close`, writes the last diagonal and off-diagonal entries; d, e, tau are indexed from the
+// matrix's first row.
+__device__ void householder_columns(int n, double* __restrict__ A, double* v, double* p, double* red, double* tau_out,
+                                    double* e_out, double* d_out, int i_stop, bool close) {
   // scratch pointers in registers: the stores below go through generic pointers, which
-  // would otherwise force the struct to be re-read after every store
+  // would otherwise force them to be re-read after every store
   struct {
     double *v, *p, *red, *tau, *e, *d;
-  } s = {s_.v, s_.p, s_.red, s_.tau, s_.e, s_.d};
-  const int r = threadIdx.x;
+  } s = {v, p, red, tau_out, e_out, d_out};
+  const int t = threadIdx.x;
   int parity = 0;
-  const int tr = r < n ? tri(r) : 0;
-  double xn2 = block_sum_alt(r >= 2 && r < n ? A[tr] * A[tr] : 0.0, s.red, parity);
-  for (int i = 0; i + 2 < n; ++i) {
+  double xn2 = block_sum_alt(t >= 2 && t < n ? A[tri(t)] * A[tri(t)] : 0.0, s.red, parity);
+  for (int i = 0; i < i_stop; ++i) {
     const double alpha = A[tri(i + 1) + i];
     double beta = alpha, tau = 0.0, scal = 0.0;
     if (xn2 > 0.0) {
@@ -96,84 +82,84 @@ __device__ void tridiagonalize(int n, double* __restrict__ A, const EigenScratch
       tau = (beta - alpha) / beta;
       scal = 1.0 / (alpha - beta);
     }
-    if (r == 0) {
+    if (t == 0) {
       s.tau[i] = tau;
       s.e[i] = beta;
       s.d[i] = A[tri(i) + i];
     }
     if (xn2 == 0.0) {  // column already reduced (uniform): only the next norm is needed
-      xn2 = block_sum_alt(r >= i + 3 && r < n ? A[tr + i + 1] * A[tr + i + 1] : 0.0, s.red, parity);
+      xn2 = block_sum_alt(t >= i + 3 && t < n ? A[tri(t) + i + 1] * A[tri(t) + i + 1] : 0.0, s.red, parity);
       continue;
     }
-    const bool mine = r > i && r < n;
-    double vr = 0.0;
-    if (mine) {
-      vr = 1.0;
-      if (r > i + 1) {
-        vr = A[tr + i] * scal;
-        A[tr + i] = vr;
+    if (t > i && t < n) {  // reflector: one thread per row
+      double vr = 1.0;
+      if (t > i + 1) {
+        vr = A[tri(t) + i] * scal;
+        A[tri(t) + i] = vr;
       }
-      s.v[r] = vr;
+      s.v[t] = vr;
     }
     __syncthreads();
-    // y_r = sum_c A(r, c) v_c over c > i: row segment (c <= r), then the column below r;
-    // four independent accumulators keep several shared-memory loads in flight
+    const int m = n - i - 1;
+    const int lg = min(5, 31 - __clz(kThreads / m));
+    const int T = 1 << lg, k = t & (T - 1), r = i + 1 + (t >> lg);
+    const bool mine = r < n;
+    const int tr = mine ? tri(r) : 0;
+    // y_r = sum_{c > i} A(r, c) v_c; four independent accumulators per thread
     double y = 0.0;
     if (mine) {
       double y0 = 0.0, y1 = 0.0, y2 = 0.0, y3 = 0.0;
       const double* row = A + tr;
-      int c = i + 1;
-      for (; c + 3 <= r; c += 4) {
+      int c = i + 1 + k;
+      for (; c + 3 * T <= r; c += 4 * T) {
         y0 = fma(row[c], s.v[c], y0);
-        y1 = fma(row[c + 1], s.v[c + 1], y1);
-        y2 = fma(row[c + 2], s.v[c + 2], y2);
-        y3 = fma(row[c + 3], s.v[c + 3], y3);
+        y1 = fma(row[c + T], s.v[c + T], y1);
+        y2 = fma(row[c + 2 * T], s.v[c + 2 * T], y2);
+        y3 = fma(row[c + 3 * T], s.v[c + 3 * T], y3);
       }
-      for (; c <= r; ++c) y0 = fma(row[c], s.v[c], y0);
-      int q = r + 1, idx = tri(r + 1) + r;
-      for (; q + 3 < n; q += 4) {
-        const int i1 = idx + q + 1, i2 = i1 + q + 2, i3 = i2 + q + 3;
-        y0 = fma(A[idx], s.v[q], y0);
-        y1 = fma(A[i1], s.v[q + 1], y1);
-        y2 = fma(A[i2], s.v[q + 2], y2);
-        y3 = fma(A[i3], s.v[q + 3], y3);
-        idx = i3 + q + 4;
+      for (; c <= r; c += T) y0 = fma(row[c], s.v[c], y0);
+      for (; c + 3 * T < n; c += 4 * T) {
+        y0 = fma(A[tri(c) + r], s.v[c], y0);
+        y1 = fma(A[tri(c + T) + r], s.v[c + T], y1);
+        y2 = fma(A[tri(c + 2 * T) + r], s.v[c + 2 * T], y2);
+        y3 = fma(A[tri(c + 3 * T) + r], s.v[c + 3 * T], y3);
       }
-      for (; q < n; idx += q + 1, ++q) y1 = fma(A[idx], s.v[q], y1);
-      y = tau * ((y0 + y1) + (y2 + y3));
-      s.p[r] = y;
+      for (; c < n; c += T) y1 = fma(A[tri(c) + r], s.v[c], y1);
+      y = (y0 + y1) + (y2 + y3);
     }
-    const double a2 = -0.5 * tau * block_sum_alt(mine ? y * vr : 0.0, s.red, parity);
-    // A22 -= v w^T + w v^T (w = p + a2 v) on the row segments c in (i, r], keeping the next
-    // column's norm part. Row r has r - i elements, so the segments are balanced in pairs: the
-    // thread of a short row (length l < H, H half the longest plus one) also takes the first
-    // H - l elements of the complementary long row n + i - r (length L + 1 - l, L = n - i - 1),
-    // whose own thread then starts after them; every thread does about H elements.
+    for (int o = T >> 1; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+    y *= tau;
+    const double vr = mine ? s.v[r] : 0.0;
+    if (mine && k == 0) s.p[r] = y;
+    const double a2 = -0.5 * tau * block_sum_alt(mine && k == 0 ? y * vr : 0.0, s.red, parity);
+    // A22 -= v w^T + w v^T (w = p + a2 v) on the row segments, keeping the next column's norm part
     double part = 0.0;
     if (mine) {
-      const int L = n - i - 1, H = (L + 2) / 2;
-      const int len = r - i, mate = n + i - r, len_mate = n - r;
-      // own row: skip the head that the short row's thread takes
-      const int c0 = (len >= H && len_mate < H && mate != r) ? i + 1 + (H - len_mate) : i + 1;
       const double wr = y + a2 * vr;
-      update_row(A + tr, c0, r, vr, wr, a2, s.v, s.p);
-      if (c0 == i + 1 && r >= i + 3) {
-        const double x = A[tr + i + 1];
-        part = x * x;
+      double* row = A + tr;
+      int c = i + 1 + k;
+      for (; c + 3 * T <= r; c += 4 * T) {
+        const double v0 = s.v[c], v1 = s.v[c + T], v2 = s.v[c + 2 * T], v3 = s.v[c + 3 * T];
+        const double w0 = s.p[c] + a2 * v0, w1 = s.p[c + T] + a2 * v1, w2 = s.p[c + 2 * T] + a2 * v2,
+                     w3 = s.p[c + 3 * T] + a2 * v3;
+        const double a0 = row[c], a1 = row[c + T], a2_ = row[c + 2 * T], a3 = row[c + 3 * T];
+        row[c] = a0 - (vr * w0 + wr * v0);
+        row[c + T] = a1 - (vr * w1 + wr * v1);
+        row[c + 2 * T] = a2_ - (vr * w2 + wr * v2);
+        row[c + 3 * T] = a3 - (vr * w3 + wr * v3);
       }
-      if (len < H && mate != r) {  // head of the complementary long row
-        const int tm = tri(mate);
-        const double vm = s.v[mate], wm = s.p[mate] + a2 * vm;
-        update_row(A + tm, i + 1, i + H - len, vm, wm, a2, s.v, s.p);
-        if (mate >= i + 3) {
-          const double x = A[tm + i + 1];
-          part += x * x;
-        }
+      for (; c <= r; c += T) {
+        const double vc = s.v[c], wc = s.p[c] + a2 * vc;
+        row[c] -= vr * wc + wr * vc;
+      }
+      if (k == 0 && r >= i + 3) {
+        const double x = row[i + 1];
+        part = x * x;
       }
     }
     xn2 = block_sum_alt(part, s.red, parity);
   }
-  if (r == 0) {
+  if (close && t == 0) {
     if (n >= 2) {
       s.d[n - 2] = A[tri(n - 2) + n - 2];
       s.e[n - 2] = A[tri(n - 1) + n - 2];
@@ -181,6 +167,36 @@ __device__ void tridiagonalize(int n, double* __restrict__ A, const EigenScratch
     }
     s.d[n - 1] = A[tri(n - 1) + n - 1];
     s.e[n - 1] = 0.0;
+  }
+  __syncthreads();
+}
+
+// Householder reduction of the packed n x n matrix A (shared or global memory). When A is in
+// global memory and `sm` (sm_cap doubles of shared memory, free during the eigensolve) is given,
+// the first columns are reduced in place until the trailing triangle fits in `sm`; the rest of
+// the reduction runs there (every access of a trailing column is then a shared-memory access) and
+// the trailing triangle, with its reflectors, is copied back for the back-transformation.
+__device__ void tridiagonalize(int n, double* __restrict__ A, const EigenScratch& s, double* sm = nullptr,
+                               int sm_cap = 0) {
+  int nl = n;
+  if (sm != nullptr)
+    while (nl > 0 && tri(nl) > sm_cap) --nl;
+  const int i0 = n - nl;
+  if (sm == nullptr || i0 == 0 || nl < 3) {
+    householder_columns(n, A, s.v, s.p, s.red, s.tau, s.e, s.d, n - 2, true);
+    return;
+  }
+  householder_columns(n, A, s.v, s.p, s.red, s.tau, s.e, s.d, i0, false);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  for (int r = w; r < nl; r += kWarps) {
+    const double* src = A + tri(r + i0) + i0;
+    for (int c = l; c <= r; c += 32) sm[tri(r) + c] = src[c];
+  }
+  __syncthreads();
+  householder_columns(nl, sm, s.v, s.p, s.red, s.tau + i0, s.e + i0, s.d + i0, nl - 2, true);
+  for (int r = w; r < nl; r += kWarps) {
+    double* dst = A + tri(r + i0) + i0;
+    for (int c = l; c <= r; c += 32) dst[c] = sm[tri(r) + c];
   }
   __syncthreads();
 }

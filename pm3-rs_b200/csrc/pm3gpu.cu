@@ -103,6 +103,7 @@ struct pm3gpu_ctx {
   int sms = 0, smem_optin = 0, smem_per_sm = 0;
   double timings[7] = {0, 0, 0, 0, 0, 0, 0};
   int launches = 0;
+  int last_ctas = 0, last_nsm = 0;  // last batched launch: CTAs per SM, largest basis with its eigen matrix in shared memory
   long long h2d = 0, d2h = 0;  // bytes moved by the last call
   cudaEvent_t ev[6] = {};
   cudaEvent_t kev[2] = {};
@@ -574,6 +575,8 @@ int launch_jobs(pm3gpu_ctx* c, const std::vector<JobDesc>& jobs, const std::vect
   int per_sm = 0;
   CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scf_batch_kernel, kThreads, L.bytes));
   if (per_sm < 1) return fail(c, PM3GPU_RESOURCE_LIMIT, "SCF kernel does not fit on an SM");
+  c->last_ctas = per_sm;
+  c->last_nsm = L.nsm;
   const long long slot = slot_doubles(nmax, wcap);
   size_t free_b = 0, total_b = 0;
   CUDA_TRY(c, cudaMemGetInfo(&free_b, &total_b));
@@ -1605,6 +1608,13 @@ int pm3gpu_last_timings(pm3gpu_ctx* c, double* ms, int max_entries) {
 }
 
 int pm3gpu_last_kernel_launches(pm3gpu_ctx* c) { return c ? c->launches : 0; }
+
+int pm3gpu_last_launch_layout(pm3gpu_ctx* c, int* ctas_per_sm, int* smem_matrix_n) {
+  if (!c) return PM3GPU_INVALID_INPUT;
+  if (ctas_per_sm) *ctas_per_sm = c->last_ctas;
+  if (smem_matrix_n) *smem_matrix_n = c->last_nsm;
+  return PM3GPU_OK;
+}
 
 int pm3gpu_last_large_phase_ms(pm3gpu_ctx* c, double* ms, int max_entries) {
   if (!c || !ms) return 0;

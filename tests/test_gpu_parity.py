@@ -170,6 +170,32 @@ def test_generated_radicals_batch_matches_oracle():
         assert np.abs(res.charges_of(m) - ref["charges"]).max() < Q_TOL
 
 
+def test_large_molecules_in_a_two_cta_batch_match_oracle():
+    """Molecules larger than the shared-memory eigen matrix of a two-CTA-per-SM launch: 30 small
+    organics keep the launch at two CTAs per SM (over 90% of the batch fits), so the water
+    clusters of 26, 34 and 42 molecules (n = 156, 204, 252) keep their packed matrix in global
+    memory and finish the Householder reduction in shared memory once the trailing triangle fits
+    (after 1 to ~110 columns, depending on n). Every molecule against the oracle."""
+    small = workloads.organic_batch(30, 5, 15, seed=77)
+    waters = [workloads.water_cluster(26), workloads.water_cluster(34), workloads.water_cluster(42, grid=(4, 4, 3))]
+    mols = small + waters
+    offs, z, xyz = workloads.pack(mols)
+    o = native.options(p_tol=1e-8)
+    ctx = _lib.Context()
+    try:
+        res = native.batch(offs, z, xyz * A2B, o, context=ctx)
+        ctas, nsm = ctypes.c_int(), ctypes.c_int()
+        assert ctx.lib.pm3gpu_last_launch_layout(ctx.ptr, ctypes.byref(ctas), ctypes.byref(nsm)) == _lib.OK
+    finally:
+        ctx.close()
+    assert ctas.value == 2 and nsm.value < 156, (ctas.value, nsm.value)
+    for m, (zz, xx) in enumerate(mols):
+        ref = O.single_point(zz, xx * A2B, p_tol=1e-8)
+        assert res.status[m] == 0
+        assert abs(res.heat_of_formation_kcal[m] - ref["heat_of_formation_kcal"]) < HOF_TOL, m
+        assert np.abs(res.charges_of(m) - ref["charges"]).max() < Q_TOL, m
+
+
 def test_water_cluster_34_matches_oracle():
     z, xyz = workloads.water_cluster(34)
     ref = O.single_point(z, xyz * A2B, p_tol=1e-8)
