@@ -254,8 +254,8 @@ int pm3gpu_last_kernel_launches(pm3gpu_ctx* ctx);
 int pm3gpu_last_launch_layout(pm3gpu_ctx* ctx, int* ctas_per_sm, int* smem_matrix_n);
 
 /* Molecules with at least `nao` basis functions are solved one at a time on the whole GPU
- * (grid-wide integral and Fock kernels, blocked eigensolver, cuBLAS DGEMM for the dense
- * products) instead of one CTA each. Default and maximum 257: every molecule beyond one CTA's
+ * (grid-wide integral and Fock kernels, blocked eigensolver, the library's FP64 tensor-core GEMM for
+ * the dense products) instead of one CTA each. Default and maximum 257: every molecule beyond one CTA's
  * 256 basis functions. Lower values send smaller molecules to that path too (one molecule at a
  * time, all SMs on it). Same run_pm3 semantics either way (no reference counterpart: the
  * reference has one CPU path). */
@@ -294,6 +294,14 @@ int pm3gpu_tuning_choice(pm3gpu_ctx* ctx, int kind, int size);
 #define PM3GPU_PRECISION_FP64 0
 #define PM3GPU_PRECISION_MIXED 1
 int pm3gpu_set_precision(pm3gpu_ctx* ctx, int mode);
+
+/* The whole-GPU path's FP64 product by itself (no counterpart in the reference, whose dense
+ * products are faer's): C = alpha op(A) op(B) + beta C with the column-major BLAS dgemm contract
+ * (op = transpose when trans_a / trans_b is nonzero; A, B, C host arrays with leading dimensions
+ * lda, ldb, ldc), computed by the library's FP64 tensor-core (DMMA) GEMM with the tile shape and
+ * K split the path would use for these sizes. C is read when beta != 0 and overwritten. */
+int pm3gpu_dgemm(pm3gpu_ctx* ctx, int trans_a, int trans_b, int m, int n, int k, double alpha, const double* a, int lda,
+                 const double* b, int ldb, double beta, double* c, int ldc);
 
 /* The mixed mode's split-BF16 product by itself (no counterpart in the reference): out (m x n,
  * row-major FP32) = A B^T for A (m x k, leading dimension lda) and B (n x k, ldb), row-major FP64

@@ -19,7 +19,7 @@ NVCC_FLAGS = [
     "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC", "-shared",
     "-diag-suppress", "550",
-    "-lcublas", "-Xlinker", "-rpath=/usr/local/cuda/lib64",
+    "-Xlinker", "-rpath=/usr/local/cuda/lib64",
 ]
 
 

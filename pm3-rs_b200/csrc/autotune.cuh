@@ -101,8 +101,7 @@ int tune_large_part(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t
     const int b = tune_bucket(kTuneLargeBuckets, nao);
     if (std::find(done.begin(), done.end(), b) != done.end()) continue;
     done.push_back(b);
-    if (!c->blas) BLAS_TRY(c, cublasCreate(&c->blas));
-    BLAS_TRY(c, cublasSetStream(c->blas, c->stream));
+    CUDA_TRY(c, dgemm_ready(c->device));
     if (!c->lbuf) c->lbuf = new LargeBufs();
     CUDA_TRY(c, c->z.ensure(4 * (size_t)na));
     CUDA_TRY(c, c->xyz.ensure(24 * (size_t)na));

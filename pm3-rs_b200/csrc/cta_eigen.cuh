@@ -64,7 +64,7 @@ __device__ __forceinline__ double block_sum_alt(double v, double* red, int& pari
 // Three barriers per column. This sweep reduces columns [0, i_stop) of the n x n matrix and, with
 // `close`, writes the last diagonal and off-diagonal entries; d, e, tau are indexed from the
 // matrix's first row.
-__device__ void householder_columns(int n, double* __restrict__ A, double* v, double* p, double* red, double* tau_out,
+__device__ __forceinline__ void householder_columns(int n, double* __restrict__ A, double* v, double* p, double* red, double* tau_out,
                                     double* e_out, double* d_out, int i_stop, bool close) {
   // scratch pointers in registers: the stores below go through generic pointers, which
   // would otherwise force them to be re-read after every store
@@ -171,34 +171,9 @@ __device__ void householder_columns(int n, double* __restrict__ A, double* v, do
   __syncthreads();
 }
 
-// Householder reduction of the packed n x n matrix A (shared or global memory). When A is in
-// global memory and `sm` (sm_cap doubles of shared memory, free during the eigensolve) is given,
-// the first columns are reduced in place until the trailing triangle fits in `sm`; the rest of
-// the reduction runs there (every access of a trailing column is then a shared-memory access) and
-// the trailing triangle, with its reflectors, is copied back for the back-transformation.
-__device__ void tridiagonalize(int n, double* __restrict__ A, const EigenScratch& s, double* sm = nullptr,
-                               int sm_cap = 0) {
-  int nl = n;
-  if (sm != nullptr)
-    while (nl > 0 && tri(nl) > sm_cap) --nl;
-  const int i0 = n - nl;
-  if (sm == nullptr || i0 == 0 || nl < 3) {
-    householder_columns(n, A, s.v, s.p, s.red, s.tau, s.e, s.d, n - 2, true);
-    return;
-  }
-  householder_columns(n, A, s.v, s.p, s.red, s.tau, s.e, s.d, i0, false);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  for (int r = w; r < nl; r += kWarps) {
-    const double* src = A + tri(r + i0) + i0;
-    for (int c = l; c <= r; c += 32) sm[tri(r) + c] = src[c];
-  }
-  __syncthreads();
-  householder_columns(nl, sm, s.v, s.p, s.red, s.tau + i0, s.e + i0, s.d + i0, nl - 2, true);
-  for (int r = w; r < nl; r += kWarps) {
-    double* dst = A + tri(r + i0) + i0;
-    for (int c = l; c <= r; c += 32) dst[c] = sm[tri(r) + c];
-  }
-  __syncthreads();
+// Householder reduction of the packed n x n matrix A (shared or global memory).
+__device__ void tridiagonalize(int n, double* __restrict__ A, const EigenScratch& s) {
+  householder_columns(n, A, s.v, s.p, s.red, s.tau, s.e, s.d, n - 2, true);
 }
 
 // ------------------------------------------------------------- 2. split + eigenvalues

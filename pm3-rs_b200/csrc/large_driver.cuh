@@ -1,9 +1,11 @@
 // Host driver of the whole-GPU path for one large molecule: the run_job SCF loop (scf.rs:1179-1496)
-// with the work spread over the device (large_scf.cuh kernels, cuBLAS DGEMM for the dense
-// products). Included by pm3gpu.cu inside its private namespace, after the context definition.
+// with the work spread over the device (large_scf.cuh kernels, the DMMA DGEMM of dgemm.cuh for
+// the dense products). Included by pm3gpu.cu inside its private namespace, after the context
+// definition.
 //
-// Matrices are row-major n x n FP64. cuBLAS sees a row-major matrix as its column-major
-// transpose; every call below is written in that view (comments give the row-major product).
+// Matrices are row-major n x n FP64. The GEMM follows the column-major BLAS contract, which sees a
+// row-major matrix as its transpose; every call below is written in that view (comments give the
+// row-major product).
 //
 // Eigensolver for large n: blocked Householder tridiagonalisation (one cooperative launch per
 // panel + one rank-64 DGEMM trailing update; five launches per column replayed from a CUDA graph
@@ -16,7 +18,6 @@
 // rotation within the cluster, and the polar step fixes their orthogonality without leaving the
 // cluster's invariant subspace, which is all the density P = w C_occ C_occ^T depends on.
 
-constexpr size_t kBlasWorkspace = 64u << 20;  // cuBLAS workspace, set before graph capture
 // Mixed mode hands over to FP64 once the RMS density change is below max(100 p_tol, this floor),
 // or when it stops falling. The split-BF16 density noise is ~2e-8 RMS at n = 12000 (water
 // clusters); the switch keeps it a few tenths of a percent of the residuals that the DIIS history
@@ -38,7 +39,7 @@ struct TriGraph {
 
 struct LargeBufs {
   TriGraph tg;
-  DevBuf blas_ws;
+  DevBuf gwork;  // split-K workspace of the DGEMMs
   DevBuf ao, sprow, sroff;
   DevBuf H, W, hacc, dpk, jacc, part, part2, scal;
   DevBuf P[2], Q[2], Pt, F, G, hist, A;
@@ -57,7 +58,7 @@ struct LargeBufs {
                       &Dp, &Lp, &Um, &Gm, &Mm, &Tm, &Z1, &Z2, &blocks, &Gk, &mh[0], &mh[1], &ml[0], &ml[1], &c32, &gsync, &vw, &wv, &Fchk, &tcerr})
       b->release();
     tcerr_zeroed = false;
-    blas_ws.release();
+    gwork.release();
     tg.reset();
   }
 };
@@ -76,10 +77,10 @@ enum LargePhase : int {
   kLgCore = 0, kLgFock, kLgDiis, kLgTridiag, kLgEigval, kLgEigvec, kLgBack, kLgOrth, kLgDensity, kLgPhases
 };
 
-#define BLAS_TRY(ctx, call)                                                                        \
-  do {                                                                                             \
-    cublasStatus_t s_ = (call);                                                                    \
-    if (s_ != CUBLAS_STATUS_SUCCESS) return fail((ctx), PM3GPU_CUDA_ERROR, std::string(#call ": cuBLAS status ") + std::to_string((int)s_)); \
+#define GEMM_TRY(call)                 \
+  do {                                 \
+    const int rc_ = (call);            \
+    if (rc_ != PM3GPU_OK) return rc_;  \
   } while (0)
 
 inline int grid_for(size_t work, int per_block = large::kBlock, int cap = large::kRedBlocks) {
@@ -578,7 +579,20 @@ class LargeSolver {
     CUDA_TRY(c_, cudaMemcpyAsync(dst, src, 8 * nn_, cudaMemcpyDeviceToDevice, c_->stream));
     return PM3GPU_OK;
   }
-  cublasHandle_t blas() { return c_->blas; }
+  // C = alpha op(A) op(B) + beta C (column-major) on the context's stream, by the hand-written
+  // DMMA GEMM (dgemm.cuh); launches are added to *count (the context's counter by default). The
+  // split-K workspace grows only for shapes that split, none of which runs under graph capture
+  // (the captured multi-launch reduction's rank-2b updates have K = 2b).
+  int gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A, int lda, const double* B, int ldb,
+           double beta, double* C, int ldc, int* count = nullptr) {
+    const dg::Plan p = dg::plan(m, n, k, c_->sms);
+    if (p.work_doubles > 0) CUDA_TRY(c_, B_.gwork.ensure(8 * p.work_doubles));
+    const int r = dg::gemm(c_->stream, c_->sms, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                           B_.gwork.as<double>());
+    if (r < 0) return fail(c_, PM3GPU_CUDA_ERROR, std::string("DGEMM launch: ") + cudaGetErrorString(cudaGetLastError()));
+    *(count ? count : &c_->launches) += r;
+    return PM3GPU_OK;
+  }
 
   int finish(double* out) {
     large::finish_sum<<<1, large::kBlock, 0, c_->stream>>>(B_.part.as<double>(), large::kRedBlocks, B_.scal.as<double>());
@@ -620,7 +634,7 @@ class LargeSolver {
     CUDA_TRY(c_, cudaGetLastError());
     return PM3GPU_OK;
   }
-  // E = F P - P F (scf.rs:1039-1054): row-major F P is cuBLAS's column-major P F.
+  // E = F P - P F (scf.rs:1039-1054): row-major F P is the column-major product P F.
   // Mixed mode (lowp) takes the product from split-BF16 tensor-core GEMMs with FP32 accumulation.
   int commutator(const double* F, const double* P, double* E, bool lowp = false) {
     if (lowp) {  // C = F P^T = F P (P symmetric), both operands K-major rows
@@ -632,7 +646,7 @@ class LargeSolver {
       return combine_transpose(E, 1.0, -1.0);
     }
     const double one = 1.0, zero = 0.0;
-    BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, n_, n_, n_, &one, P, n_, F, n_, &zero, E, n_));
+    GEMM_TRY(gemm(false, false, n_, n_, n_, one, P, n_, F, n_, zero, E, n_));
     large::antisym_kernel<<<grid_for(nn_), large::kBlock, 0, c_->stream>>>(E, n_);
     ++c_->launches;
     return PM3GPU_OK;
@@ -651,8 +665,7 @@ class LargeSolver {
       return combine_transpose(P, 0.5 * w, 0.5 * w);
     }
     const double zero = 0.0;
-    BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, n_, n_, k, &w, B_.X.as<double>(), ld,
-                             B_.X.as<double>(), ld, &zero, P, n_));
+    GEMM_TRY(gemm(true, false, n_, n_, k, w, B_.X.as<double>(), ld, B_.X.as<double>(), ld, zero, P, n_));
     return PM3GPU_OK;
   }
 
@@ -718,8 +731,6 @@ class LargeSolver {
     for (int k = 0; hit && k < TriGraph::kKeys; ++k) hit = g.key[k] == key[k];
     if (!hit) {
       g.reset();
-      CUDA_TRY(c_, B_.blas_ws.ensure(kBlasWorkspace));
-      BLAS_TRY(c_, cublasSetWorkspace(blas(), B_.blas_ws.p, kBlasWorkspace));
       if (cudaStreamBeginCapture(c_->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         (void)cudaGetLastError();
         int launches = 0;
@@ -812,13 +823,10 @@ class LargeSolver {
           const double* Xq = X + (size_t)q * large::kCoopLd;
           const double* Yq = Y + (size_t)q * large::kCoopLd;
           if (b == large::kPanel) {
-            BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, 2 * b, &mone, Yq, large::kCoopLd, Xq,
-                                     large::kCoopLd, &one, C, n));
+            GEMM_TRY(gemm(true, false, m, m, 2 * b, mone, Yq, large::kCoopLd, Xq, large::kCoopLd, one, C, n, &launches));
           } else {  // last, narrower panel: columns b.. of X and Y are not part of it
-            BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Yq, large::kCoopLd, Xq,
-                                     large::kCoopLd, &one, C, n));
-            BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Yq + large::kPanel, large::kCoopLd,
-                                     Xq + large::kPanel, large::kCoopLd, &one, C, n));
+            GEMM_TRY(gemm(true, false, m, m, b, mone, Yq, large::kCoopLd, Xq, large::kCoopLd, one, C, n, &launches));
+            GEMM_TRY(gemm(true, false, m, m, b, mone, Yq + large::kPanel, large::kCoopLd, Xq + large::kPanel, large::kCoopLd, one, C, n, &launches));
           }
         }
         continue;
@@ -852,10 +860,8 @@ class LargeSolver {
         double* C = A + (size_t)q * n + q;
         const double* Vq = V + (size_t)q * large::kPanel;
         const double* Wq = W + (size_t)q * large::kPanel;
-        BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Wq, large::kPanel, Vq, large::kPanel,
-                                 &one, C, n));
-        BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_T, CUBLAS_OP_N, m, m, b, &mone, Vq, large::kPanel, Wq, large::kPanel,
-                                 &one, C, n));
+        GEMM_TRY(gemm(true, false, m, m, b, mone, Wq, large::kPanel, Vq, large::kPanel, one, C, n, &launches));
+        GEMM_TRY(gemm(true, false, m, m, b, mone, Vq, large::kPanel, Wq, large::kPanel, one, C, n, &launches));
       }
     }
     large::tail_kernel<<<1, 1, 0, c_->stream>>>(A, n, d, e, tau);
@@ -1001,19 +1007,15 @@ class LargeSolver {
       const double* Vr = V + (size_t)r0 * large::kPanel;
       double* Xr = X + (size_t)r0 * K;
       // G = V^T V (b x b); column-major: Vc Vc^T
-      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_T, b, b, m, &one, Vr, large::kPanel, Vr, large::kPanel,
-                               &zero, B_.Gm.as<double>(), b));
+      GEMM_TRY(gemm(false, true, b, b, m, one, Vr, large::kPanel, Vr, large::kPanel, zero, B_.Gm.as<double>(), b));
       large::wy_t_kernel<<<1, 1, 0, c_->stream>>>(B_.Gm.as<double>(), tau, p, b, B_.Tm.as<double>());
       ++c_->launches;
       // Z = V^T X  -> column-major Zc = Xc Vc^T (K x b)
-      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_T, (int)K, b, m, &one, Xr, (int)K, Vr, large::kPanel,
-                               &zero, B_.Z1.as<double>(), (int)K));
+      GEMM_TRY(gemm(false, true, (int)K, b, m, one, Xr, (int)K, Vr, large::kPanel, zero, B_.Z1.as<double>(), (int)K));
       // Z2 = T Z -> Z2c = Zc T^T, T row-major = column-major T^T
-      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, (int)K, b, b, &one, B_.Z1.as<double>(), (int)K,
-                               B_.Tm.as<double>(), large::kPanel, &zero, B_.Z2.as<double>(), (int)K));
+      GEMM_TRY(gemm(false, false, (int)K, b, b, one, B_.Z1.as<double>(), (int)K, B_.Tm.as<double>(), large::kPanel, zero, B_.Z2.as<double>(), (int)K));
       // X -= V Z2 -> Xc -= Z2c Vc
-      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, (int)K, m, b, &mone, B_.Z2.as<double>(), (int)K, Vr,
-                               large::kPanel, &one, Xr, (int)K));
+      GEMM_TRY(gemm(false, false, (int)K, m, b, mone, B_.Z2.as<double>(), (int)K, Vr, large::kPanel, one, Xr, (int)K));
     }
     tick(kLgBack);
     // ---- 5. orthonormalise: X <- X (3I - X^T X) / 2 until max |X^T X - I| < 1e-13; at most
@@ -1025,8 +1027,7 @@ class LargeSolver {
     last_ns_steps_ = 0;
     last_defect_ = INFINITY;
     for (int step = 0; step <= kNsSteps; ++step) {
-      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_T, (int)K, (int)K, n, &one, X, (int)K, X, (int)K, &zero,
-                               Gk, (int)K));
+      GEMM_TRY(gemm(false, true, (int)K, (int)K, n, one, X, (int)K, X, (int)K, zero, Gk, (int)K));
       large::orth_defect_kernel<<<large::kRedBlocks, large::kBlock, 0, c_->stream>>>(Gk, (int)K, B_.part.as<double>());
       ++c_->launches;
       std::vector<double> mx(large::kRedBlocks);
@@ -1049,8 +1050,7 @@ class LargeSolver {
       large::ns_matrix_kernel<<<grid_for(K * K), large::kBlock, 0, c_->stream>>>(Gk, B_.Mm.as<double>(), (int)K);
       ++c_->launches;
       // X M (row-major) -> column-major M Xc (M symmetric)
-      BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, (int)K, n, (int)K, &one, B_.Mm.as<double>(), (int)K, X,
-                               (int)K, &zero, B_.Xt.as<double>(), (int)K));
+      GEMM_TRY(gemm(false, false, (int)K, n, (int)K, one, B_.Mm.as<double>(), (int)K, X, (int)K, zero, B_.Xt.as<double>(), (int)K));
       std::swap(B_.X, B_.Xt);
       X = B_.X.as<double>();
     }
@@ -1065,8 +1065,7 @@ class LargeSolver {
     const double one = 1.0, zero = 0.0;
     CUDA_TRY(c_, B_.Xt.ensure(8 * (size_t)n * k));
     // row-major Y = F X  ->  column-major Yc = Xc F (F symmetric)
-    BLAS_TRY(c_, cublasDgemm(blas(), CUBLAS_OP_N, CUBLAS_OP_N, k, n, n, &one, B_.X.as<double>(), k, F, n, &zero,
-                             B_.Xt.as<double>(), k));
+    GEMM_TRY(gemm(false, false, k, n, n, one, B_.X.as<double>(), k, F, n, zero, B_.Xt.as<double>(), k));
     large::eig_residual_kernel<<<large::kRedBlocks, large::kBlock, 0, c_->stream>>>(
         B_.Xt.as<double>(), B_.X.as<double>(), B_.lam.as<double>(), n, k, B_.part.as<double>());
     ++c_->launches;

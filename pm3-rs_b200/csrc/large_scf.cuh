@@ -3,7 +3,7 @@
 // build run one thread per atom pair (src/hamiltonian.rs:191-344, src/fock.rs:93-332), the sums
 // into each atom's diagonal block one warp per atom in a fixed order (no atomics: repeated solves
 // agree bit for bit); the dense products (commutator, density, the eigensolver's trailing updates
-// and back-transformation) are cuBLAS DGEMMs issued by the host driver; the multi-launch
+// and back-transformation) are DMMA DGEMMs (dgemm.cuh) issued by the host driver; the multi-launch
 // Householder panel (the cooperative one is panel_coop.cuh), the Sturm multisection, the
 // twisted-factorisation eigenvectors, the compact-WY factors and all reductions are here.
 #pragma once

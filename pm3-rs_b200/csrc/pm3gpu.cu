@@ -1,6 +1,5 @@
 // Host side of the pm3gpu C ABI: context, job planning, launches and the stability-search
 // driver of run_pm3 (pm3-rs src/scf.rs:450-848).
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -15,6 +14,7 @@
 #include <vector>
 
 #include "../../include/pm3gpu.h"
+#include "dgemm.cuh"
 #include "gradient_kernel.cuh"
 #include "large_scf.cuh"
 #include "panel_coop.cuh"
@@ -112,7 +112,6 @@ struct pm3gpu_ctx {
   DevBuf prof;
   double phase_cycles[kPhases] = {};
   // whole-GPU path for large molecules
-  cublasHandle_t blas = nullptr;
   int large_min = kMaxN + 1;  // molecules with at least this many basis functions
   LargeBufs* lbuf = nullptr;
   DevBuf lsel;                // densities of the selected state (P_tot | P_alpha | P_beta)
@@ -128,7 +127,7 @@ struct pm3gpu_ctx {
   int precision = PM3GPU_PRECISION_FP64;  // arithmetic of the whole-GPU path's dense products
   bool coop_panels = true;    // Householder panels as cooperative launches (PM3GPU_COOP_PANELS=0: off)
   std::vector<double> ltrace;  // per-iteration record of the last whole-GPU solve (5 per row)
-  DevBuf tcbuf[7];             // pm3gpu_split_gemm: A, B (FP64), A hi / lo, B hi / lo, C; tcerr
+  DevBuf tcbuf[7];             // pm3gpu_split_gemm: A, B (FP64), A hi / lo, B hi / lo, C; tcerr (pm3gpu_dgemm: A, B, C, split-K work)
   bool large_checks = false;   // whole-GPU path: eigen residual of every eigensolve (one more DGEMM)
   std::vector<double> lchecks;  // per-eigensolve checks of the last whole-GPU solve (6 per row)
   // learned initial density: FP32 master parameters, BF16 copy, Adam moments, gradients
@@ -723,6 +722,20 @@ int launch_gradients(pm3gpu_ctx* c, const std::vector<GradMol>& mols, const std:
   return PM3GPU_OK;
 }
 
+// The DGEMM kernels' shared-memory attribute, set once per device on the first whole-GPU solve or
+// pm3gpu_dgemm call (the batched path never launches them). The device must be current.
+cudaError_t dgemm_ready(int device) {
+  static std::mutex mu;
+  static std::vector<char> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (device < 0) return cudaErrorInvalidDevice;
+  if ((int)done.size() <= device) done.resize(device + 1, 0);
+  if (done[device]) return cudaSuccess;
+  const cudaError_t e = dg::set_attributes();
+  if (e == cudaSuccess) done[device] = 1;
+  return e;
+}
+
 #include "large_driver.cuh"
 
 // run_pm3 (scf.rs:450-848) for one molecule on the whole-GPU path: the first pass, the
@@ -734,8 +747,7 @@ int run_large(pm3gpu_ctx* c, const MolPlan& p, const int32_t* hz, const int32_t*
   for (double& t : c->large_ms) t = 0.0;
   c->ltrace.clear();
   c->lchecks.clear();
-  if (!c->blas) BLAS_TRY(c, cublasCreate(&c->blas));
-  BLAS_TRY(c, cublasSetStream(c->blas, c->stream));
+  CUDA_TRY(c, dgemm_ready(c->device));
   if (!c->lbuf) c->lbuf = new LargeBufs();
   LargeSolver S(c, *c->lbuf);
   double ecc = 0.0;
@@ -1440,7 +1452,6 @@ void pm3gpu_context_destroy(pm3gpu_ctx* c) {
                     &c->gZ[0], &c->gZ[1], &c->gZ[2], &c->gH[0], &c->gH[1], &c->gH[2], &c->gdH, &c->gdZ, &c->gT, &c->gM,
                     &c->gidx, &c->gXb, &c->gTb, &c->gMb, &c->gdY, &c->gpart, &c->gguess, &c->gdens})
     b->release();
-  if (c->blas) cublasDestroy(c->blas);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
 }
@@ -1946,6 +1957,37 @@ int pm3gpu_split_gemm(pm3gpu_ctx* c, int m, int n, int k, const double* a, int l
   CUDA_TRY(c, cudaMemcpyAsync(&flag, derr, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   if (flag) return fail(c, PM3GPU_CUDA_ERROR, "split-BF16 GEMM: a pipeline wait in the kernel ran out");
+  return PM3GPU_OK;
+}
+
+int pm3gpu_dgemm(pm3gpu_ctx* c, int trans_a, int trans_b, int m, int n, int k, double alpha, const double* a, int lda,
+                 const double* b, int ldb, double beta, double* cm, int ldc) {
+  if (!c || m < 1 || n < 1 || k < 0 || !a || !b || !cm) return fail(c, PM3GPU_INVALID_INPUT, "bad argument");
+  const long long ra = trans_a ? k : m, ca = trans_a ? m : k;  // stored shapes, column-major
+  const long long rb = trans_b ? n : k, cb = trans_b ? k : n;
+  if (lda < std::max<long long>(1, ra) || ldb < std::max<long long>(1, rb) || ldc < m)
+    return fail(c, PM3GPU_INVALID_INPUT, "leading dimension below the row count");
+  std::lock_guard<std::mutex> lk(c->mu);
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  c->err.clear();
+  CUDA_TRY(c, dgemm_ready(c->device));
+  const size_t na = (size_t)lda * std::max<long long>(ca, 1), nb = (size_t)ldb * std::max<long long>(cb, 1),
+               nc = (size_t)ldc * n;
+  const dg::Plan pl = dg::plan(m, n, k, c->sms);
+  DevBuf* B = c->tcbuf;
+  CUDA_TRY(c, B[0].ensure(8 * na));
+  CUDA_TRY(c, B[1].ensure(8 * nb));
+  CUDA_TRY(c, B[2].ensure(8 * nc));
+  CUDA_TRY(c, B[3].ensure(8 * std::max<size_t>(pl.work_doubles, 1)));
+  CUDA_TRY(c, cudaMemcpyAsync(B[0].p, a, 8 * na, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(B[1].p, b, 8 * nb, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(B[2].p, cm, 8 * nc, cudaMemcpyHostToDevice, c->stream));
+  const int r = dg::gemm(c->stream, c->sms, trans_a != 0, trans_b != 0, m, n, k, alpha, B[0].as<double>(), lda,
+                         B[1].as<double>(), ldb, beta, B[2].as<double>(), ldc, B[3].as<double>());
+  if (r < 0) return fail(c, PM3GPU_CUDA_ERROR, std::string("DGEMM launch: ") + cudaGetErrorString(cudaGetLastError()));
+  c->launches = r;
+  CUDA_TRY(c, cudaMemcpyAsync(cm, B[2].p, 8 * nc, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return PM3GPU_OK;
 }
 

@@ -640,8 +640,7 @@ __device__ void eigensolve(Ctx& c, double* Ap, int kval, int kvec, double* Y, do
                            bool warm = false, double* dlam = nullptr) {
   const int n = c.n;
   mark(c, kPhPack);
-  // a matrix in global memory finishes its reduction in the shared-memory union (idle here)
-  tridiagonalize(n, Ap, c.es, Ap == c.Asm ? nullptr : c.Asm, tri(c.A->sm.nsm));
+  tridiagonalize(n, Ap, c.es);
   if (tri_save && threadIdx.x == 0)
     for (int i = 0; i < n; ++i) {
       tri_save[i] = c.es.d[i];

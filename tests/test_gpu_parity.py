@@ -173,9 +173,8 @@ def test_generated_radicals_batch_matches_oracle():
 def test_large_molecules_in_a_two_cta_batch_match_oracle():
     """Molecules larger than the shared-memory eigen matrix of a two-CTA-per-SM launch: 30 small
     organics keep the launch at two CTAs per SM (over 90% of the batch fits), so the water
-    clusters of 26, 34 and 42 molecules (n = 156, 204, 252) keep their packed matrix in global
-    memory and finish the Householder reduction in shared memory once the trailing triangle fits
-    (after 1 to ~110 columns, depending on n). Every molecule against the oracle."""
+    clusters of 26, 34 and 42 molecules (n = 156, 204, 252) run their eigensolver on a packed
+    matrix in global memory. Every molecule against the oracle."""
     small = workloads.organic_batch(30, 5, 15, seed=77)
     waters = [workloads.water_cluster(26), workloads.water_cluster(34), workloads.water_cluster(42, grid=(4, 4, 3))]
     mols = small + waters
