@@ -379,6 +379,14 @@ __global__ void adam_kernel(float* p, const float* gr, float* m, float* v, int n
     pb[k] = __float2bfloat16(q);
   }
 }
+// Wt (out x in) = W^T for a row-major (in x out) weight: the K-major B operand of the tcgen05 layers.
+__global__ void transpose_w_kernel(const __nv_bfloat16* __restrict__ W, int kin, int kout, __nv_bfloat16* __restrict__ Wt) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < kin * kout; e += gridDim.x * blockDim.x) {
+    const int n = e / kin, k = e % kin;
+    Wt[e] = W[(size_t)k * kout + n];
+  }
+}
+
 __global__ void to_bf16_kernel(const float* p, int n, __nv_bfloat16* pb) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) pb[k] = __float2bfloat16(p[k]);
 }

@@ -135,6 +135,8 @@ struct pm3gpu_ctx {
   long long adam_steps = 0;
   DevBuf gp, gpb, gm, gv, gg;
   DevBuf gqmols, gatom, gao, gcoord, gX, gY, gZ[3], gH[3], gdH, gdZ, gT, gM, gidx, gXb, gTb, gMb, gdY, gpart, gguess, gdens;
+  DevBuf gwt, gerr;  // inference: transposed hidden weights (tcgen05 B operands), kernel error flag
+  int* h_gerr = nullptr;  // pinned copy of gerr, read after the stream's next synchronisation
 };
 
 namespace {
@@ -964,6 +966,55 @@ int mlp_forward(pm3gpu_ctx* c, const __nv_bfloat16* X, long long rows, float* Y)
   return PM3GPU_OK;
 }
 
+// Inference on `rows` feature rows: the three hidden layers on the tcgen05 layer kernel
+// (tc::launch_mlp_layer, bias + SiLU in its epilogue), the output layer fused into the last one's
+// epilogue; Y = rows x kOut FP32. The rounding points are mlp_forward's (FP32 pre-activations, BF16
+// activations); training keeps mlp_forward, whose pre-activations the backward pass needs.
+int mlp_infer(pm3gpu_ctx* c, const __nv_bfloat16* X, long long rows, float* Y) {
+  using namespace guess;
+  if (rows <= 0) return PM3GPU_OK;
+  if (rows > (1LL << 30)) return fail(c, PM3GPU_RESOURCE_LIMIT, "learned guess: too many feature rows in one call");
+  const __nv_bfloat16* P = c->gpb.as<__nv_bfloat16>();
+  const float* pf = c->gp.as<float>();
+  CUDA_TRY(c, c->gwt.ensure(2 * (size_t)kHid * (kIn + 2 * kHid)));
+  for (int l = 0; l < 2; ++l) CUDA_TRY(c, c->gH[l].ensure(2 * (size_t)kHid * rows));
+  __nv_bfloat16* Wt1 = c->gwt.as<__nv_bfloat16>();
+  __nv_bfloat16* Wt2 = Wt1 + (size_t)kHid * kIn;
+  __nv_bfloat16* Wt3 = Wt2 + (size_t)kHid * kHid;
+  transpose_w_kernel<<<64, 256, 0, c->stream>>>(P + kW1, kIn, kHid, Wt1);
+  transpose_w_kernel<<<256, 256, 0, c->stream>>>(P + kW2, kHid, kHid, Wt2);
+  transpose_w_kernel<<<256, 256, 0, c->stream>>>(P + kW3, kHid, kHid, Wt3);
+  CUDA_TRY(c, cudaGetLastError());
+  int* err = c->gerr.as<int>();
+  __nv_bfloat16* H1 = c->gH[0].as<__nv_bfloat16>();
+  __nv_bfloat16* H2 = c->gH[1].as<__nv_bfloat16>();
+  const int M = (int)rows;
+  if (!tc::launch_mlp_layer(M, kIn, X, Wt1, pf + kB1, H1, nullptr, nullptr, nullptr, err, c->stream) ||
+      !tc::launch_mlp_layer(M, kHid, H1, Wt2, pf + kB2, H2, nullptr, nullptr, nullptr, err, c->stream) ||
+      !tc::launch_mlp_layer(M, kHid, H2, Wt3, pf + kB3, nullptr, P + kW4, pf + kB4, Y, err, c->stream))
+    return fail(c, PM3GPU_CUDA_ERROR, "learned guess: tensor map or kernel attribute of the tcgen05 layers");
+  c->launches += 6;
+  CUDA_TRY(c, cudaGetLastError());
+  return PM3GPU_OK;
+}
+
+// Inference over all rows, 2^20 at a time, without blocking the host: the kernels' error flag is
+// cleared first and copied to pinned host memory after the last layer; the caller reads it with
+// infer_failed() once the stream has been synchronised (a host wait here would hold back the next
+// launches while other work occupies the SMs).
+int mlp_infer_all(pm3gpu_ctx* c, const __nv_bfloat16* X, long long rows, float* Y) {
+  using namespace guess;
+  CUDA_TRY(c, c->gerr.ensure(sizeof(int)));
+  CUDA_TRY(c, cudaMemsetAsync(c->gerr.p, 0, sizeof(int), c->stream));
+  for (long long r0 = 0; r0 < rows; r0 += 1LL << 20) {
+    const int rc = mlp_infer(c, X + r0 * kIn, std::min<long long>(1LL << 20, rows - r0), Y + r0 * kOut);
+    if (rc != PM3GPU_OK) return rc;
+  }
+  CUDA_TRY(c, cudaMemcpyAsync(c->h_gerr, c->gerr.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  return PM3GPU_OK;
+}
+bool infer_failed(pm3gpu_ctx* c) { return *reinterpret_cast<volatile int*>(c->h_gerr) != 0; }
+
 // Forward and backward pass of the network on B rows X (BF16), targets T and masks Mk (FP32):
 // loss = inv_count * sum Mk (Y - T)^2 (its partial sums are added into *accum), gradient of
 // every parameter into c->gg (layout of the parameter vector). dY, dZ are rounded to BF16 for the
@@ -1010,12 +1061,8 @@ int guess_infer(pm3gpu_ctx* c, const GuessRows& G, const int32_t* dz, const doub
   if (rc != PM3GPU_OK) return rc;
   CUDA_TRY(c, c->gY.ensure(4 * (size_t)guess::kOut * std::max<long long>(G.rows, 1)));
   CUDA_TRY(c, c->gguess.ensure(8 * std::max<size_t>(G.dens_total, 1)));
-  const long long chunk = 1 << 20;
-  for (long long r0 = 0; r0 < G.rows; r0 += chunk) {
-    const long long nr = std::min(chunk, G.rows - r0);
-    rc = mlp_forward(c, c->gX.as<__nv_bfloat16>() + r0 * guess::kIn, nr, c->gY.as<float>() + r0 * guess::kOut);
-    if (rc != PM3GPU_OK) return rc;
-  }
+  rc = mlp_infer_all(c, c->gX.as<__nv_bfloat16>(), G.rows, c->gY.as<float>());
+  if (rc != PM3GPU_OK) return rc;
   CUDA_TRY(c, cudaMemsetAsync(c->gguess.p, 0, 8 * G.dens_total, c->stream));
   guess::assemble_kernel<<<gblocks(G.rows), 256, 0, c->stream>>>(c->gqmols.as<guess::Mol>(), (int)G.mols.size(),
                                                                 c->elem.as<ElemDev>(), dz, dxyz, c->gao.as<int>(),
@@ -1144,6 +1191,7 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
   int rc = launch_jobs(c, sorted, rjobs, zs, dz, dxyz, tot, want.density, want.eps, R);
   if (rc != PM3GPU_OK) return rc;
   if (guess_timed) {  // the launch has synchronised the stream
+    if (infer_failed(c)) return fail(c, PM3GPU_CUDA_ERROR, "learned guess: a pipeline wait in the tcgen05 layer kernel ran out");
     float gms = 0.f;
     CUDA_TRY(c, cudaEventElapsedTime(&gms, c->gev[0], c->gev[1]));
     c->timings[6] = gms;
@@ -1385,6 +1433,8 @@ int pm3gpu_context_create(int device, pm3gpu_ctx** out) {
   pm3gpu_ctx* c = new pm3gpu_ctx();
   c->device = device;
   auto bail = [&](cudaError_t e) {
+    if (c->h_gerr) cudaFreeHost(c->h_gerr);
+    if (c->own) cudaStreamDestroy(c->own);
     delete c;
     (void)e;
     return PM3GPU_CUDA_ERROR;
@@ -1413,6 +1463,9 @@ int pm3gpu_context_create(int device, pm3gpu_ctx** out) {
   if ((e = cudaFuncSetAttribute(scf_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, c->smem_optin)) !=
       cudaSuccess)
     return bail(e);
+  if ((e = cudaHostAlloc(reinterpret_cast<void**>(&c->h_gerr), sizeof(int), cudaHostAllocDefault)) != cudaSuccess)
+    return bail(e);
+  *c->h_gerr = 0;
   derive_elements(c->h_elem, &c->h_pairs);
   noalloc_forget(device);
   {
@@ -1450,8 +1503,9 @@ void pm3gpu_context_destroy(pm3gpu_ctx* c) {
   for (DevBuf& b : c->tcbuf) b.release();
   for (DevBuf* b : {&c->gp, &c->gpb, &c->gm, &c->gv, &c->gg, &c->gqmols, &c->gatom, &c->gao, &c->gcoord, &c->gX, &c->gY,
                     &c->gZ[0], &c->gZ[1], &c->gZ[2], &c->gH[0], &c->gH[1], &c->gH[2], &c->gdH, &c->gdZ, &c->gT, &c->gM,
-                    &c->gidx, &c->gXb, &c->gTb, &c->gMb, &c->gdY, &c->gpart, &c->gguess, &c->gdens})
+                    &c->gidx, &c->gXb, &c->gTb, &c->gMb, &c->gdY, &c->gpart, &c->gguess, &c->gdens, &c->gwt, &c->gerr})
     b->release();
+  if (c->h_gerr) cudaFreeHost(c->h_gerr);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
 }
@@ -1688,7 +1742,7 @@ int pm3gpu_guess_predict(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const in
   int rc = guess_features(c, G, c->z.as<int32_t>(), c->xyz.as<double>(), total_atoms);
   if (rc != PM3GPU_OK) return rc;
   CUDA_TRY(c, c->gY.ensure(4 * (size_t)kOut * std::max<long long>(G.rows, 1)));
-  rc = mlp_forward(c, c->gX.as<__nv_bfloat16>(), G.rows, c->gY.as<float>());
+  rc = mlp_infer_all(c, c->gX.as<__nv_bfloat16>(), G.rows, c->gY.as<float>());
   if (rc != PM3GPU_OK) return rc;
   if (outputs)
     CUDA_TRY(c, cudaMemcpyAsync(outputs, c->gY.p, 4 * (size_t)kOut * G.rows, cudaMemcpyDeviceToHost, c->stream));
@@ -1698,6 +1752,7 @@ int pm3gpu_guess_predict(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const in
     CUDA_TRY(c, cudaMemcpyAsync(xb.data(), c->gX.p, 2 * xb.size(), cudaMemcpyDeviceToHost, c->stream));
   }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (infer_failed(c)) return fail(c, PM3GPU_CUDA_ERROR, "learned guess: a pipeline wait in the tcgen05 layer kernel ran out");
   for (size_t k = 0; k < xb.size(); ++k) features[k] = __bfloat162float(xb[k]);
   return PM3GPU_OK;
 }

@@ -32,6 +32,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
+#include <vector>
 
 namespace pm3gpu {
 namespace tc {
@@ -269,6 +271,163 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// ------------------------------------------------------------------ MLP layers
+// One hidden layer of the learned-guess network on the same machinery (no counterpart in the
+// reference): H = silu(A W^T + b) with A (M x K, K = 64 or 256) and W^T (256 x K) K-major BF16, one
+// product per K slice, FP32 accumulator in tensor memory, bias + SiLU + BF16 rounding in the
+// epilogue (the rounding points of the mma.sync path: FP32 pre-activation, BF16 activation). With
+// HEAD the epilogue also applies the 256 x 8 output layer to the BF16 activations of its row
+// (Y = H W4 + b4, FP32), so the last hidden activations never leave the SM. Stage = A tile
+// (128 x 64) + W tile (256 x 64), 48 KB; two stages, two CTAs per SM.
+constexpr uint32_t kMlpStage = kTileA + kTileB;
+constexpr uint32_t kMlpSmem = kStages * kMlpStage + 1024 + 128;
+
+template <bool HEAD>
+__global__ void __launch_bounds__(kThreads, 2)
+    mlp_layer_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mW, int M, int K,
+                     const float* __restrict__ bias, __nv_bfloat16* __restrict__ H, const __nv_bfloat16* __restrict__ W4,
+                     const float* __restrict__ b4, float* __restrict__ Y, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  const uint32_t bar0 = base + kStages * kMlpStage;
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 16u + 8u * s; };
+  const uint32_t accum_bar = bar0 + 32u;
+  unsigned char* gen = smem_raw + (base - raw);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gen + kStages * kMlpStage + 40);
+  volatile int* fail = reinterpret_cast<volatile int*>(gen + kStages * kMlpStage + 44);
+  int* issued_p = reinterpret_cast<int*>(gen + kStages * kMlpStage + 48);
+
+  __shared__ int skip;
+  if (threadIdx.x == 0) skip = *reinterpret_cast<volatile int*>(err);
+  __syncthreads();
+  if (skip) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * kBM;
+  const int nkb = (K + kBK - 1) / kBK;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 32) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(accum_bar, 1);
+    *fail = 0;
+    *issued_p = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {  // ---- TMA producer
+    int issued = 0;
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb & 1;
+      if (kb >= kStages && !mbar_wait(empty_bar(s), ((kb >> 1) - 1) & 1, fail)) {
+        *fail = 1;
+        break;
+      }
+      const uint32_t st = base + s * kMlpStage;
+      mbar_expect_tx(full_bar(s), kMlpStage);
+      tma_load_2d(st, &mA, kb * kBK, m0, full_bar(s));
+      tma_load_2d(st + kTileA, &mW, kb * kBK, 0, full_bar(s));
+      issued = kb + 1;
+    }
+    *issued_p = issued;
+  } else if (warp == 1 && lane == 0) {  // ---- MMA issuer
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb & 1;
+      if (!mbar_wait(full_bar(s), (kb >> 1) & 1, fail)) {
+        *fail = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t st = base + s * kMlpStage;
+#pragma unroll
+      for (int k = 0; k < kBK / 16; ++k)
+        umma_f16(tmem, sw128_desc(st + 32u * k), sw128_desc(st + kTileA + 32u * k), (kb | k) != 0);
+      umma_commit(empty_bar(s));
+    }
+    umma_commit(accum_bar);
+  }
+  __syncwarp();
+
+  int never = 0;
+  const bool done = mbar_wait(accum_bar, 0, &never);
+  if (!done && threadIdx.x == 0) *fail = 1;
+  __syncthreads();
+  const bool ok = !*fail;
+  tc_fence_after();
+  if (ok && nkb > 0) {
+    const int row = warp * 32 + lane;
+    const int gm = m0 + row;
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    float y[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll 1
+    for (int c0 = 0; c0 < kBN; c0 += 32) {
+      uint32_t r[32];
+      tmem_ld32(lane_base + (uint32_t)c0, r);
+      float h[32];  // BF16-rounded activations of columns c0 .. c0 + 31
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const float z = __uint_as_float(r[j]) + __ldg(bias + c0 + j);
+        h[j] = __bfloat162float(__float2bfloat16(z / (1.0f + __expf(-z))));
+      }
+      if (!HEAD) {
+        if (gm < M) {  // 64 bytes of the row: four 16-byte stores of packed pairs
+          uint4* dst = reinterpret_cast<uint4*>(H + (size_t)gm * kBN + c0);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            uint32_t w[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const __nv_bfloat162 b2 = __floats2bfloat162_rn(h[8 * q + 2 * e], h[8 * q + 2 * e + 1]);
+              w[e] = (uint32_t)__bfloat16_as_ushort(b2.x) | ((uint32_t)__bfloat16_as_ushort(b2.y) << 16);
+            }
+            dst[q] = make_uint4(w[0], w[1], w[2], w[3]);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const __nv_bfloat16* w = W4 + (size_t)(c0 + j) * 8;
+#pragma unroll
+          for (int o = 0; o < 8; ++o) y[o] = fmaf(h[j], __bfloat162float(w[o]), y[o]);
+        }
+      }
+    }
+    if (HEAD && gm < M) {
+      float4* dst = reinterpret_cast<float4*>(Y + (size_t)gm * 8);
+      dst[0] = make_float4(y[0] + b4[0], y[1] + b4[1], y[2] + b4[2], y[3] + b4[3]);
+      dst[1] = make_float4(y[4] + b4[4], y[5] + b4[5], y[6] + b4[6], y[7] + b4[7]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (*fail) {
+      const int issued = *issued_p;
+      for (int kb = (issued > kStages ? issued - kStages : 0); kb < issued; ++kb)
+        (void)mbar_wait(full_bar(kb & 1), (kb >> 1) & 1, &never);
+      atomicExch(err, 1);
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
 // ------------------------------------------------------------------ host side
 // cuTensorMapEncodeTiled from the driver (through the runtime's entry-point query: no link
 // dependency on libcuda), resolved once per process.
@@ -298,6 +457,22 @@ inline bool map_kmajor(CUtensorMap* m, const void* base, int rows, int k, int ld
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// A kernel's dynamic shared-memory limit, raised once per device and kernel (`tag` < 32): the
+// attribute is per device, and setting it again on every launch is not free (with other streams
+// busy the call can wait for their work, which would hold back this stream's next launches).
+inline bool smem_attr_once(const void* kernel, int bytes, int tag) {
+  static std::mutex mu;
+  static std::vector<uint32_t> done;  // per device: bit `tag` set once the attribute is in place
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return false;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)done.size() <= dev) done.resize(dev + 1, 0u);
+  if (done[dev] & (1u << tag)) return true;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) return false;
+  done[dev] |= 1u << tag;
+  return true;
+}
+
 // C (M x N, row-major FP32, ldc) = A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T with A (M x K, lda) and
 // B (N x K, ldb) K-major BF16 on `stream`; err (device int) is set if a wait in the kernel ran
 // out. Returns false when a tensor map cannot be made (bad alignment or no driver entry point).
@@ -308,11 +483,31 @@ inline bool launch_split_gemm(int M, int N, int K, const __nv_bfloat16* Ahi, con
   if (!map_kmajor(&a_hi, Ahi, M, K, lda, kBM) || !map_kmajor(&a_lo, Alo, M, K, lda, kBM) ||
       !map_kmajor(&b_hi, Bhi, N, K, ldb, kBN) || !map_kmajor(&b_lo, Blo, N, K, ldb, kBN))
     return false;
-  static const cudaError_t attr =
-      cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
-  if (attr != cudaSuccess) return false;
+  if (!smem_attr_once((const void*)split_gemm_kernel, (int)kSmemBytes, 0)) return false;
   const dim3 grid((unsigned)((N + kBN - 1) / kBN), (unsigned)((M + kBM - 1) / kBM));
   split_gemm_kernel<<<grid, kThreads, kSmemBytes, stream>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, C, ldc, err);
+  return true;
+}
+
+// One learned-guess layer: A (M x K, ld K) and Wt (256 x K, ld K) K-major BF16, bias (256 FP32).
+// Without W4: H (M x 256 BF16, row-major) = silu(A Wt^T + bias). With W4 (256 x 8 BF16, in x out)
+// and b4 (8 FP32): Y (M x 8 FP32) = bf16(silu(A Wt^T + bias)) W4 + b4. Returns false when a
+// tensor map or the kernel attribute cannot be set.
+inline bool launch_mlp_layer(int M, int K, const __nv_bfloat16* A, const __nv_bfloat16* Wt, const float* bias,
+                             __nv_bfloat16* H, const __nv_bfloat16* W4, const float* b4, float* Y, int* err,
+                             cudaStream_t stream) {
+  if (M < 1 || (K != 64 && K != 256)) return false;
+  CUtensorMap ma, mw;
+  if (!map_kmajor(&ma, A, M, K, K, kBM) || !map_kmajor(&mw, Wt, kBN, K, K, kBN)) return false;
+  const dim3 grid((unsigned)((M + kBM - 1) / kBM));
+  if (W4) {
+    if (!smem_attr_once((const void*)mlp_layer_kernel<true>, (int)kMlpSmem, 2)) return false;
+    mlp_layer_kernel<true><<<grid, kThreads, kMlpSmem, stream>>>(ma, mw, M, K, bias, nullptr, W4, b4, Y, err);
+  } else {
+    if (!smem_attr_once((const void*)mlp_layer_kernel<false>, (int)kMlpSmem, 1)) return false;
+    mlp_layer_kernel<false><<<grid, kThreads, kMlpSmem, stream>>>(ma, mw, M, K, bias, H, nullptr, nullptr, nullptr,
+                                                                  err);
+  }
   return true;
 }
 
