@@ -61,10 +61,32 @@ __device__ __forceinline__ void block_sums(double (&v)[K], double* red, double* 
   __syncthreads();
 }
 
+// This thread's 4 + 4 elements of the 64 x 16 chunks of op(A) and op(B) at k0 (the layout of
+// cta_gemm's shared tiles), zero outside the matrices.
+template <bool TA, bool TB>
+__device__ __forceinline__ void cta_gemm_fetch(double (&pa)[4], double (&pb)[4], int k0, int i0, int j0, int m, int n,
+                                               int k, const double* __restrict__ A, int lda,
+                                               const double* __restrict__ B, int ldb) {
+  constexpr int BM = 64, BN = 64, BK = 16;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int e = threadIdx.x + q * kThreads;
+    int ii, kk;
+    if (TA) { ii = e % BM; kk = e / BM; } else { kk = e % BK; ii = e / BK; }
+    const int gi = i0 + ii, gk = k0 + kk;
+    pa[q] = (gi < m && gk < k) ? (TA ? A[(size_t)gk * lda + gi] : A[(size_t)gi * lda + gk]) : 0.0;
+    int jj;
+    if (TB) { kk = e % BK; jj = e / BK; } else { jj = e % BN; kk = e / BN; }
+    const int gj = j0 + jj, gk2 = k0 + kk;
+    pb[q] = (gj < n && gk2 < k) ? (TB ? B[(size_t)gj * ldb + gk2] : B[(size_t)gk2 * ldb + gj]) : 0.0;
+  }
+}
+
 // C (m x n) = alpha * op(A) * op(B) with op(A) m x k, op(B) k x n; A, B row-major in global
 // memory. TA: A stored as k x m (use its transpose). Each output element goes through
-// `epi(i, j, value)`. Tiles of 64 x 64, k-chunks of 16, 4 x 4 outputs per thread; `tile`
-// needs 2 * 64 * 17 doubles of shared memory. If `lower_only`, only tiles touching the lower
+// `epi(i, j, value)`. Tiles of 64 x 64, k-chunks of 16 (the next chunk's loads in flight while the
+// current one is multiplied), 4 x 4 outputs per thread; `tile` needs 2 * 64 * 17 doubles of shared
+// memory. If `lower_only`, only tiles touching the lower
 // triangle (i >= j) are computed (for symmetric results).
 template <bool TA, bool TB, class Epi>
 __device__ void cta_gemm(int m, int n, int k, double alpha, const double* __restrict__ A, int lda,
@@ -83,26 +105,24 @@ __device__ void cta_gemm(int m, int n, int k, double alpha, const double* __rest
     for (int a = 0; a < 4; ++a)
 #pragma unroll
       for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    // the next k-chunk's elements are loaded into registers while the current one is multiplied
+    // (each thread holds 4 of op(A) and 4 of op(B): 64 x 16 / 256 threads)
+    double pa[4], pb[4];
+    cta_gemm_fetch<TA, TB>(pa, pb, 0, i0, j0, m, n, k, A, lda, B, ldb);
     for (int k0 = 0; k0 < k; k0 += BK) {
-      __syncthreads();
-      // load op(A)[i0..i0+64, k0..k0+16] into As[kk][ii]
-      for (int e = threadIdx.x; e < BM * BK; e += kThreads) {
+      __syncthreads();  // the previous chunk's products have read As, Bs
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int e = threadIdx.x + q * kThreads;
         int ii, kk;
         if (TA) { ii = e % BM; kk = e / BM; } else { kk = e % BK; ii = e / BK; }
-        const int gi = i0 + ii, gk = k0 + kk;
-        double v = 0.0;
-        if (gi < m && gk < k) v = TA ? A[(size_t)gk * lda + gi] : A[(size_t)gi * lda + gk];
-        As[kk * (BM + 1) + ii] = v;
-      }
-      for (int e = threadIdx.x; e < BK * BN; e += kThreads) {
-        int jj, kk;
+        As[kk * (BM + 1) + ii] = pa[q];
+        int jj;
         if (TB) { kk = e % BK; jj = e / BK; } else { jj = e % BN; kk = e / BN; }
-        const int gj = j0 + jj, gk = k0 + kk;
-        double v = 0.0;
-        if (gj < n && gk < k) v = TB ? B[(size_t)gj * ldb + gk] : B[(size_t)gk * ldb + gj];
-        Bs[kk * (BN + 1) + jj] = v;
+        Bs[kk * (BN + 1) + jj] = pb[q];
       }
       __syncthreads();
+      if (k0 + BK < k) cta_gemm_fetch<TA, TB>(pa, pb, k0 + BK, i0, j0, m, n, k, A, lda, B, ldb);
 #pragma unroll
       for (int kk = 0; kk < BK; ++kk) {
         double a[4], b[4];

@@ -605,9 +605,10 @@ __device__ __forceinline__ void back_transform_t(int n, int kvec, const double* 
 }
 
 // The reflectors of column i (v_{i+1} = 1, v_r = A(r, i) below) applied from the last to the
-// first. Smaller matrices take more vectors per warp (the same registers either way).
+// first. Up to n = 64 each lane holds 2 rows and a warp 4 vectors (the n/2 or so occupied vectors
+// then keep all eight warps busy, which measured faster than 8 vectors on four warps).
 __device__ void back_transform(int n, int kvec, const double* __restrict__ A, double* Y, const EigenScratch& s_) {
-  if (n <= 64) back_transform_t<2, 8>(n, kvec, A, Y, s_.tau);
+  if (n <= 64) back_transform_t<2, 4>(n, kvec, A, Y, s_.tau);
   else if (n <= 128) back_transform_t<4, 4>(n, kvec, A, Y, s_.tau);
   else back_transform_t<kRowT, 2>(n, kvec, A, Y, s_.tau);
 }

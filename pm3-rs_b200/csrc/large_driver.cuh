@@ -40,6 +40,7 @@ struct TriGraph {
 struct LargeBufs {
   TriGraph tg;
   DevBuf gwork;  // split-K workspace of the DGEMMs
+  DevBuf Vw;     // back-transformation block V (n x kWy)
   DevBuf ao, sprow, sroff;
   DevBuf H, W, hacc, dpk, jacc, part, part2, scal;
   DevBuf P[2], Q[2], Pt, F, G, hist, A;
@@ -59,6 +60,7 @@ struct LargeBufs {
       b->release();
     tcerr_zeroed = false;
     gwork.release();
+    Vw.release();
     tg.reset();
   }
 };
@@ -993,29 +995,32 @@ class LargeSolver {
     ++c_->launches;
     CUDA_TRY(c_, cudaGetLastError());
     tick(kLgEigvec);
-    // ---- 4. back-transformation X <- Q X, panels from the last to the first
-    CUDA_TRY(c_, B_.Gm.ensure(8 * (size_t)large::kPanel * large::kPanel));
-    CUDA_TRY(c_, B_.Tm.ensure(8 * (size_t)large::kPanel * large::kPanel));
-    CUDA_TRY(c_, B_.Z1.ensure(8 * K * large::kPanel));
-    CUDA_TRY(c_, B_.Z2.ensure(8 * K * large::kPanel));
-    const int np = n - 2 > 0 ? (n - 2 + large::kPanel - 1) / large::kPanel : 0;
-    for (int pi = np - 1; pi >= 0; --pi) {
-      const int p = pi * large::kPanel, b = std::min(large::kPanel, n - 2 - p);
-      large::panel_v_kernel<<<grid_for((size_t)n * large::kPanel), large::kBlock, 0, c_->stream>>>(A, n, p, b, V);
+    // ---- 4. back-transformation X <- Q X, blocks of kWy reflectors from the last to the first
+    CUDA_TRY(c_, B_.Gm.ensure(8 * (size_t)large::kWy * large::kWy));
+    CUDA_TRY(c_, B_.Tm.ensure(8 * (size_t)large::kWy * large::kWy));
+    CUDA_TRY(c_, B_.Z1.ensure(8 * K * large::kWy));
+    CUDA_TRY(c_, B_.Z2.ensure(8 * K * large::kWy));
+    CUDA_TRY(c_, B_.Vw.ensure(8 * (size_t)n * large::kWy));
+    double* Vw = B_.Vw.as<double>();
+    const int nbk = n - 2 > 0 ? (n - 2 + large::kWy - 1) / large::kWy : 0;
+    for (int bi = nbk - 1; bi >= 0; --bi) {
+      const int p = bi * large::kWy, b = std::min(large::kWy, n - 2 - p);
+      large::block_v_kernel<<<grid_for((size_t)n * large::kWy), large::kBlock, 0, c_->stream>>>(A, n, p, b, Vw);
       ++c_->launches;
       const int r0 = p + 1, m = n - r0;
-      const double* Vr = V + (size_t)r0 * large::kPanel;
+      const double* Vr = Vw + (size_t)r0 * large::kWy;
       double* Xr = X + (size_t)r0 * K;
       // G = V^T V (b x b); column-major: Vc Vc^T
-      GEMM_TRY(gemm(false, true, b, b, m, one, Vr, large::kPanel, Vr, large::kPanel, zero, B_.Gm.as<double>(), b));
-      large::wy_t_kernel<<<1, 1, 0, c_->stream>>>(B_.Gm.as<double>(), tau, p, b, B_.Tm.as<double>());
+      GEMM_TRY(gemm(false, true, b, b, m, one, Vr, large::kWy, Vr, large::kWy, zero, B_.Gm.as<double>(), b));
+      large::wy_t_block_kernel<<<1, large::kWy, 0, c_->stream>>>(B_.Gm.as<double>(), tau, p, b, B_.Tm.as<double>());
       ++c_->launches;
       // Z = V^T X  -> column-major Zc = Xc Vc^T (K x b)
-      GEMM_TRY(gemm(false, true, (int)K, b, m, one, Xr, (int)K, Vr, large::kPanel, zero, B_.Z1.as<double>(), (int)K));
+      GEMM_TRY(gemm(false, true, (int)K, b, m, one, Xr, (int)K, Vr, large::kWy, zero, B_.Z1.as<double>(), (int)K));
       // Z2 = T Z -> Z2c = Zc T^T, T row-major = column-major T^T
-      GEMM_TRY(gemm(false, false, (int)K, b, b, one, B_.Z1.as<double>(), (int)K, B_.Tm.as<double>(), large::kPanel, zero, B_.Z2.as<double>(), (int)K));
+      GEMM_TRY(gemm(false, false, (int)K, b, b, one, B_.Z1.as<double>(), (int)K, B_.Tm.as<double>(), large::kWy, zero,
+                    B_.Z2.as<double>(), (int)K));
       // X -= V Z2 -> Xc -= Z2c Vc
-      GEMM_TRY(gemm(false, false, (int)K, m, b, mone, B_.Z2.as<double>(), (int)K, Vr, large::kPanel, one, Xr, (int)K));
+      GEMM_TRY(gemm(false, false, (int)K, m, b, mone, B_.Z2.as<double>(), (int)K, Vr, large::kWy, one, Xr, (int)K));
     }
     tick(kLgBack);
     // ---- 5. orthonormalise: X <- X (3I - X^T X) / 2 until max |X^T X - I| < 1e-13; at most

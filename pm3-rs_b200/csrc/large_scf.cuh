@@ -670,29 +670,41 @@ __global__ void tail_kernel(const double* A, int n, double* d, double* e, double
   d[n - 1] = A[(size_t)(n - 1) * n + n - 1];
   e[n - 1] = 0.0;
 }
-// V of the panel [p, p+b) rebuilt from the reflectors stored in rows p .. p+b-1
-__global__ void __launch_bounds__(kBlock) panel_v_kernel(const double* A, int n, int p, int b, double* V) {
-  for (size_t q = blockIdx.x * (size_t)kBlock + threadIdx.x; q < (size_t)n * kPanel; q += (size_t)gridDim.x * kBlock) {
-    const int r = (int)(q / kPanel), k = (int)(q % kPanel);
+// Back-transformation blocks: kWy reflectors (four panels) per compact-WY block, so that its
+// products are GEMMs 128 wide instead of 32.
+constexpr int kWy = 4 * kPanel;
+// V (n x kWy, row-major) of the reflectors [p, p + b): column k is reflector p + k (zero above row
+// p + k + 1, one there, A's stored entries below); columns b .. kWy - 1 zero.
+__global__ void __launch_bounds__(kBlock) block_v_kernel(const double* A, int n, int p, int b, double* V) {
+  for (size_t q = blockIdx.x * (size_t)kBlock + threadIdx.x; q < (size_t)n * kWy; q += (size_t)gridDim.x * kBlock) {
+    const int r = (int)(q / kWy), k = (int)(q % kWy);
     const int i = p + k;
     double v = 0.0;
     if (k < b) v = r <= i ? 0.0 : (r == i + 1 ? 1.0 : A[(size_t)i * n + r]);
     V[q] = v;
   }
 }
-// T of the compact WY form H(p) ... H(p+b-1) = I - V T V^T (forward, column-wise), from the
-// Gram G = V^T V (b x b, row-major) and tau; one thread (b <= kPanel).
-__global__ void wy_t_kernel(const double* G, const double* tau, int p, int b, double* T) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int q = 0; q < kPanel * kPanel; ++q) T[q] = 0.0;
-  for (int k = 0; k < b; ++k) {
-    const double tk = tau[p + k];
-    for (int mm = 0; mm < k; ++mm) {
-      double acc = 0.0;
-      for (int l = mm; l < k; ++l) acc = fma(T[mm * kPanel + l], G[l * b + k], acc);
-      T[mm * kPanel + k] = -tk * acc;
+// T (kWy x kWy, row-major, upper triangular) of H(p) ... H(p+b-1) = I - V T V^T from the Gram
+// G = V^T V (b x b) and tau: T[k][k] = tau_k, T[m][k] = -tau_k sum_{m <= l < k} T[m][l] G[l][k].
+// Row m depends only on its own earlier entries, so thread m forms row m alone (no barriers).
+__global__ void __launch_bounds__(kWy) wy_t_block_kernel(const double* __restrict__ G, const double* __restrict__ tau,
+                                                         int p, int b, double* __restrict__ T) {
+  const int m = threadIdx.x;
+  double* row = T + (size_t)m * kWy;
+  for (int k = 0; k < kWy; ++k) row[k] = 0.0;
+  if (m >= b) return;
+  row[m] = tau[p + m];
+  for (int k = m + 1; k < b; ++k) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int l = m;
+    for (; l + 3 < k; l += 4) {
+      a0 = fma(row[l], G[(size_t)l * b + k], a0);
+      a1 = fma(row[l + 1], G[(size_t)(l + 1) * b + k], a1);
+      a2 = fma(row[l + 2], G[(size_t)(l + 2) * b + k], a2);
+      a3 = fma(row[l + 3], G[(size_t)(l + 3) * b + k], a3);
     }
-    T[k * kPanel + k] = tk;
+    for (; l < k; ++l) a0 = fma(row[l], G[(size_t)l * b + k], a0);
+    row[k] = -tau[p + k] * ((a0 + a1) + (a2 + a3));
   }
 }
 

@@ -5,6 +5,11 @@
     python pm3-rs_b200/profile_cases.py water [--waters 1000] [--iters 2]
         one whole-GPU solve of a water cluster cut after `iters` SCF iterations: one launch of
         core_pairs_kernel (pair integrals, H_core, pair table) and a few of fock_pairs_kernel
+    python pm3-rs_b200/profile_cases.py dgemm [--n 4096] [--reps 1]
+        the FP64 DMMA GEMM C = A B (n x n, column-major) of the whole-GPU path (pm3gpu_dgemm)
+    python pm3-rs_b200/profile_cases.py mlp [--mols 512]
+        learned-guess inference on `mols` organics with a random model (pm3gpu_guess_predict):
+        three launches of the tcgen05 layer kernel over all atom and pair rows
 
 Each case prints what it ran and exits 0 on success. The profiles/ summaries name the exact command.
 """
@@ -55,16 +60,58 @@ def water(waters, iters):
     print(f"water-{waters}: n = {res.nao}, {res.iterations} iterations, E_elec {res.electronic_ev:.6f} eV")
 
 
+def dgemm(n, reps):
+    ctx = _lib.Context(0)
+    rng = np.random.default_rng(0)
+    a, b = np.asfortranarray(rng.standard_normal((n, n))), np.asfortranarray(rng.standard_normal((n, n)))
+    c = np.zeros((n, n), order="F")
+    for _ in range(reps):
+        t = time.perf_counter()
+        rc = ctx.lib.pm3gpu_dgemm(ctx.ptr, 0, 0, n, n, n, 1.0, a.ctypes.data_as(D), n, b.ctypes.data_as(D), n, 0.0,
+                                  c.ctypes.data_as(D), n)
+        if rc != 0:
+            raise RuntimeError(ctx.last_error())
+        print(f"dgemm n={n}: {1e3 * (time.perf_counter() - t):.1f} ms per call (host copies included)")
+    ref = a[:64] @ b
+    print(f"max relative error of the first 64 rows: {np.abs(c[:64] - ref).max() / np.abs(ref).max():.2e}")
+
+
+def mlp(mols):
+    ctx = _lib.Context(0)
+    rng = np.random.default_rng(3)
+    n_par = 64 * 256 + 256 + 2 * (256 * 256 + 256) + 256 * 8 + 8
+    params = (rng.standard_normal(n_par) * 0.05).astype(np.float32)
+    F32 = ctypes.POINTER(ctypes.c_float)
+    if ctx.lib.pm3gpu_guess_set_params(ctx.ptr, params.ctypes.data_as(F32), n_par) != 0:
+        raise RuntimeError(ctx.last_error())
+    offs, z, xyz = workloads.pack(workloads.organic_batch(mols, 5, 60, seed=5))
+    offs = np.ascontiguousarray(offs, np.int32)
+    z = np.ascontiguousarray(z, np.int32)
+    x = np.ascontiguousarray(xyz * A2B)
+    I32 = ctypes.POINTER(ctypes.c_int32)
+    t = time.perf_counter()
+    rc = ctx.lib.pm3gpu_guess_predict(ctx.ptr, len(offs) - 1, offs.ctypes.data_as(I32), z.ctypes.data_as(I32),
+                                      x.ctypes.data_as(D), None, None)
+    if rc != 0:
+        raise RuntimeError(ctx.last_error())
+    print(f"mlp: {mols} molecules in {1e3 * (time.perf_counter() - t):.1f} ms (features, three layer launches)")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["split-gemm", "water"])
+    ap.add_argument("case", choices=["split-gemm", "water", "dgemm", "mlp"])
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--waters", type=int, default=1000)
     ap.add_argument("--iters", type=int, default=2)
+    ap.add_argument("--mols", type=int, default=512)
     a = ap.parse_args()
     if a.case == "split-gemm":
         split_gemm(a.n, a.reps)
+    elif a.case == "dgemm":
+        dgemm(a.n, a.reps)
+    elif a.case == "mlp":
+        mlp(a.mols)
     else:
         water(a.waters, a.iters)
 

@@ -66,7 +66,10 @@ def test_batch_on_two_contexts_equals_one_batch():
         for c in ctxs:
             c.close()
     assert len(parts) == 2 and min(len(p) for p in parts) > 0
+    # the per-CTA Fock build and the gradient kernel add per-atom terms with atomics, whose order
+    # depends on scheduling: the two runs agree to rounding, not bit for bit (1e-8 eV/Bohr is
+    # 4.4e-7 kcal/mol/A, below the 1e-6 kcal/mol/A parity bar)
     assert np.array_equal(one.status, two.status)
     assert np.abs(one.heat_of_formation_kcal - two.heat_of_formation_kcal).max() < 1e-9
     assert np.abs(one.charges - two.charges).max() < 1e-9
-    assert np.abs(one.gradients - two.gradients).max() < 1e-9
+    assert np.abs(one.gradients - two.gradients).max() < 1e-8
