@@ -385,78 +385,131 @@ __device__ void tridiag_vectors(int n, int kvec, double* Y, double* tf, const Ei
   const double pivmin = s.misc[0], tnorm = s.misc[1];
   const int nb = *s.nblk;
   const double win = 1.0e-11 * fmax(tnorm, 1.0);
-  for (int j = tid; j < kvec; j += kThreads) {
+  // Two halves of the CTA work on the same vectors: warps 0-3 (half 0) form the top-down
+  // factorisation L+ D+ L+^T of T - lam, warps 4-7 (half 1) the bottom-up U- D- U-^T; both are
+  // chains of divisions, so running them side by side halves the latency per vector. Then half 0
+  // picks the twist index, and the halves fill the vector above and below it. Per-vector scratch
+  // in tf (6 n): D+, L+, U-, D- (the pivots after clamping), then [twist, block], [norm parts].
+  constexpr int kHalf = kThreads / 2;
+  const int half = tid / kHalf, hj = tid % kHalf;
+  for (int j = hj; j < kvec; j += kHalf) {
     const double lam = s.lam[j];
     // which unreduced block holds this eigenvalue (degenerate copies go to successive blocks);
     // an unsplit T (the usual case) has one block, and the three Sturm counts are not needed
     int pos = nb == 1 ? 0 : j - sturm(s.d, s.e2, 0, n - 1, lam - win, pivmin);
-    int b = nb == 1 ? 0 : -1, sub = 0;
+    int b = nb == 1 ? 0 : -1;
     for (int q = 0; q < nb && b < 0; ++q) {
       const int lo = s.blk[q], hi = s.blk[q + 1] - 1;
       const int c = sturm(s.d, s.e2, lo, hi, lam + win, pivmin) - sturm(s.d, s.e2, lo, hi, lam - win, pivmin);
-      if (pos < c) {
-        b = q;
-        sub = pos;
-      } else {
-        pos -= c;
-      }
+      if (pos < c) b = q;
+      else pos -= c;
     }
     if (b < 0) b = 0;  // inconsistent counts (not expected): block 0
-    (void)sub;
-    s.vinfo[j] = b;
+    if (half == 0) s.vinfo[j] = b;
     const int lo = s.blk[b], hi = s.blk[b + 1] - 1, m = hi - lo + 1;
     double* y = Y + (size_t)j * n;
-    for (int i = 0; i < n; ++i) y[i] = 0.0;
-    if (m == 1) {
-      y[lo] = 1.0;
-      continue;
-    }
+    for (int i = half; i < n; i += 2) y[i] = 0.0;
+    if (m == 1) continue;
     double* Dp = tf + (size_t)j * 6 * n;
     double* Lp = Dp + n;
     double* Um = Lp + n;
-    // T - lam = L+ D+ L+^T (top-down)
-    double dp = s.d[lo] - lam;
-    for (int i = 0; i < m - 1; ++i) {
+    double* Dm = Um + n;
+    if (half == 0) {  // T - lam = L+ D+ L+^T (top-down)
+      double dp = s.d[lo] - lam;
+      for (int i = 0; i < m - 1; ++i) {
+        if (fabs(dp) < pivmin) dp = dp < 0.0 ? -pivmin : pivmin;
+        Dp[i] = dp;
+        const double ei = s.e[lo + i];
+        Lp[i] = ei / dp;
+        dp = (s.d[lo + i + 1] - lam) - Lp[i] * ei;
+      }
       if (fabs(dp) < pivmin) dp = dp < 0.0 ? -pivmin : pivmin;
-      Dp[i] = dp;
-      const double ei = s.e[lo + i];
-      Lp[i] = ei / dp;
-      dp = (s.d[lo + i + 1] - lam) - Lp[i] * ei;
-    }
-    if (fabs(dp) < pivmin) dp = dp < 0.0 ? -pivmin : pivmin;
-    Dp[m - 1] = dp;
-    // T - lam = U- D- U-^T (bottom-up), twist index r minimising |gamma|
-    double dm = s.d[hi] - lam;
-    if (fabs(dm) < pivmin) dm = dm < 0.0 ? -pivmin : pivmin;
-    double best = fabs(Dp[m - 1] + dm - (s.d[hi] - lam));
-    int r = m - 1;
-    for (int i = m - 2; i >= 0; --i) {
-      const double ei = s.e[lo + i];
-      Um[i] = ei / dm;
-      dm = (s.d[lo + i] - lam) - Um[i] * ei;
+      Dp[m - 1] = dp;
+    } else {  // T - lam = U- D- U-^T (bottom-up)
+      double dm = s.d[hi] - lam;
       if (fabs(dm) < pivmin) dm = dm < 0.0 ? -pivmin : pivmin;
-      const double g = fabs(Dp[i] + dm - (s.d[lo + i] - lam));
-      if (g < best) {
-        best = g;
-        r = i;
+      Dm[m - 1] = dm;
+      for (int i = m - 2; i >= 0; --i) {
+        const double ei = s.e[lo + i];
+        Um[i] = ei / dm;
+        dm = (s.d[lo + i] - lam) - Um[i] * ei;
+        if (fabs(dm) < pivmin) dm = dm < 0.0 ? -pivmin : pivmin;
+        Dm[i] = dm;
       }
     }
-    // solve N_r D_r N_r^T y = gamma_r e_r
-    y[lo + r] = 1.0;
-    for (int i = r - 1; i >= 0; --i) {
-      double z = -Lp[i] * y[lo + i + 1];
-      if (y[lo + i + 1] == 0.0 && i + 2 < m) z = -(s.e[lo + i + 1] / s.e[lo + i]) * y[lo + i + 2];
-      y[lo + i] = z;
+  }
+  __syncthreads();
+  // twist index r minimising |gamma_i| = |D+_i + D-_i - (d_i - lam)| (the largest index among ties,
+  // as a downward scan with a strict comparison finds it)
+  if (half == 0)
+    for (int j = hj; j < kvec; j += kHalf) {
+      const double lam = s.lam[j];
+      const int b = s.vinfo[j], lo = s.blk[b], hi = s.blk[b + 1] - 1, m = hi - lo + 1;
+      if (m == 1) continue;
+      double* Dp = tf + (size_t)j * 6 * n;
+      const double* Dm = Dp + 3 * n;
+      double best = fabs(Dp[m - 1] + Dm[m - 1] - (s.d[hi] - lam));
+      int r = m - 1;
+      for (int i = m - 2; i >= 0; --i) {
+        const double g = fabs(Dp[i] + Dm[i] - (s.d[lo + i] - lam));
+        if (g < best) {
+          best = g;
+          r = i;
+        }
+      }
+      reinterpret_cast<int*>(Dp + 4 * n)[0] = r;
     }
-    for (int i = r; i < m - 1; ++i) {
-      double z = -Um[i] * y[lo + i];
-      if (y[lo + i] == 0.0 && i >= 1) z = -(s.e[lo + i - 1] / s.e[lo + i]) * y[lo + i - 1];
-      y[lo + i + 1] = z;
+  __syncthreads();
+  // solve N_r D_r N_r^T y = gamma_r e_r: half 0 the rows above r, half 1 from r down; partial norms
+  for (int j = hj; j < kvec; j += kHalf) {
+    const int b = s.vinfo[j], lo = s.blk[b], hi = s.blk[b + 1] - 1, m = hi - lo + 1;
+    double* y = Y + (size_t)j * n;
+    double* Dp = tf + (size_t)j * 6 * n;
+    if (m == 1) {
+      if (half == 0) y[lo] = 1.0;
+      continue;
     }
+    const double* Lp = Dp + n;
+    const double* Um = Lp + n;
+    const int r = reinterpret_cast<const int*>(Dp + 4 * n)[0];
     double nrm = 0.0;
-    for (int i = lo; i <= hi; ++i) nrm += y[i] * y[i];
-    nrm = 1.0 / sqrt(nrm);
-    for (int i = lo; i <= hi; ++i) y[i] *= nrm;
+    if (half == 0) {
+      double yn = 1.0, ynn = 0.0;  // y[lo + i + 1], y[lo + i + 2]
+      for (int i = r - 1; i >= 0; --i) {
+        double z = -Lp[i] * yn;
+        if (yn == 0.0 && i + 2 < m) z = -(s.e[lo + i + 1] / s.e[lo + i]) * ynn;
+        y[lo + i] = z;
+        nrm = fma(z, z, nrm);
+        ynn = yn;
+        yn = z;
+      }
+    } else {
+      y[lo + r] = 1.0;
+      nrm = 1.0;
+      double yc = 1.0, yp = 0.0;  // y[lo + i], y[lo + i - 1] (the latter read only after a zero)
+      for (int i = r; i < m - 1; ++i) {
+        double z = -Um[i] * yc;
+        if (yc == 0.0 && i >= 1) z = -(s.e[lo + i - 1] / s.e[lo + i]) * yp;
+        y[lo + i + 1] = z;
+        nrm = fma(z, z, nrm);
+        yp = yc;
+        yc = z;
+      }
+    }
+    Dp[5 * n + half] = nrm;
+  }
+  __syncthreads();
+  for (int j = hj; j < kvec; j += kHalf) {
+    const int b = s.vinfo[j], lo = s.blk[b], hi = s.blk[b + 1] - 1, m = hi - lo + 1;
+    if (m == 1) continue;
+    const double* Dp = tf + (size_t)j * 6 * n;
+    const int r = reinterpret_cast<const int*>(Dp + 4 * n)[0];
+    const double scale = 1.0 / sqrt(Dp[5 * n] + Dp[5 * n + 1]);
+    double* y = Y + (size_t)j * n;
+    if (half == 0)
+      for (int i = lo; i < lo + r; ++i) y[i] *= scale;
+    else
+      for (int i = lo + r; i <= hi; ++i) y[i] *= scale;
   }
   __syncthreads();
   // Eigenvalues of one block closer than 1e-7 ||T||: the twisted vectors are not reliable

@@ -295,32 +295,29 @@ __device__ void run_job(Ctx& c, const JobDesc& job, JobOut* out, int kind = -1, 
     double sq_a, sq_b = 0.0;
     {
       double* Ap = n <= A.sm.nsm ? c.Asm : c.Ag;
-      const int nt = n * (n + 1) / 2;
       const double* __restrict__ coef = c.coef;
       const double* __restrict__ hist = c.hist;
       const double shift = J.shift;
       for (int spin = 0; spin < (uhf && !paired ? 2 : 1); ++spin) {
         const double* Pproj = spin == 0 ? Pc : Qc;
         const double* Fnew = spin == 0 ? Fa : Fb;
-        for (int k = tid; k < nt; k += kThreads) {
-          int r = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
-          while (tri(r + 1) <= k) ++r;
-          while (tri(r) > k) --r;
-          const int col = k - tri(r);
-          const size_t ix = (size_t)r * n + col;
-          double v;
-          if (use_hist) {
-            v = 0.0;
-            for (int l = 0; l < len; ++l) {
-              const double* bl = hist + (size_t)((head + l) % depth) * slot_mats * nn;
-              v = fma(coef[l], bl[(spin == 0 ? 0 : 2 * nn) + ix], v);
+        // rows to warps, columns to lanes (coalesced reads of the history matrices)
+        for (int r = tid >> 5; r < n; r += kWarps)
+          for (int col = tid & 31; col <= r; col += 32) {
+            const size_t ix = (size_t)r * n + col;
+            double v;
+            if (use_hist) {
+              v = 0.0;
+              for (int l = 0; l < len; ++l) {
+                const double* bl = hist + (size_t)((head + l) % depth) * slot_mats * nn;
+                v = fma(coef[l], bl[(spin == 0 ? 0 : 2 * nn) + ix], v);
+              }
+            } else {
+              v = Fnew[ix];
             }
-          } else {
-            v = Fnew[ix];
+            if (uhf && shift != 0.0) v += shift * ((r == col ? 1.0 : 0.0) - Pproj[ix]);
+            Ap[tri(r) + col] = v;
           }
-          if (uhf && shift != 0.0) v += shift * ((r == col ? 1.0 : 0.0) - Pproj[ix]);
-          Ap[k] = v;
-        }
         __syncthreads();
         if (spin == 0) {
           eigensolve(c, Ap, kva, na, c.Vt, eps_a, c.tri_a, iter > 0, c.tri_a + 3 * n);

@@ -618,16 +618,13 @@ __device__ void adiis_coeffs_warp(int m, const double* mg, double* out, double* 
 __device__ double* pack_input(Ctx& c, const double* X, const double* Pproj, double shift) {
   const int n = c.n;
   double* Ap = n <= c.A->sm.nsm ? c.Asm : c.Ag;
-  const int nt = n * (n + 1) / 2;
-  for (int k = threadIdx.x; k < nt; k += kThreads) {
-    int r = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
-    while (tri(r + 1) <= k) ++r;
-    while (tri(r) > k) --r;
-    const int col = k - tri(r);
-    double v = X[(size_t)r * n + col];
-    if (shift != 0.0) v += shift * ((r == col ? 1.0 : 0.0) - Pproj[(size_t)r * n + col]);
-    Ap[k] = v;
-  }
+  // rows to warps, columns to lanes (coalesced reads)
+  for (int r = threadIdx.x >> 5; r < n; r += kWarps)
+    for (int col = threadIdx.x & 31; col <= r; col += 32) {
+      double v = X[(size_t)r * n + col];
+      if (shift != 0.0) v += shift * ((r == col ? 1.0 : 0.0) - Pproj[(size_t)r * n + col]);
+      Ap[tri(r) + col] = v;
+    }
   __syncthreads();
   return Ap;
 }
