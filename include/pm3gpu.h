@@ -206,6 +206,35 @@ int pm3gpu_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const 
                  const double* xyz_bohr, const pm3gpu_options* opts, int per_molecule_options,
                  pm3gpu_result* results, double* charges, double* gradients);
 
+/* Geometry optimisation of many molecules at once: the reference's L-BFGS
+ * (src/optimizer.rs:77-221, `optimize` / OptOptions) run per molecule, every energy and gradient
+ * from the batched SCF + gradient launch (one launch per round over every molecule's pending
+ * geometry: its start or its current line-search trial). Same algorithm and stopping rules: two-loop
+ * recursion over the last `history` steps, first step 0.1 / max|g|, uphill guard, backtracking
+ * Armijo search (c1 = 1e-4, step halved down to 1e-8; a geometry whose SCF fails is a rejected
+ * step), curvature filter s.y > 1e-10, convergence when the largest gradient component is below
+ * gtol (eV/Bohr). xyz_bohr holds the starting geometries and receives the final ones;
+ * gradients[3 * total atoms] (optional) the final gradients. out[m].status is the start
+ * geometry's run_pm3 status when that evaluation failed (the molecule is then left unchanged). */
+typedef struct {
+  int max_iter;   /* 200 */
+  double gtol;    /* 1e-3 eV/Bohr on the largest gradient component */
+  int history;    /* 8 */
+} pm3gpu_opt_options;
+typedef struct {
+  int status;                     /* PM3GPU_* of the start geometry's evaluation */
+  int converged;                  /* 1 when the largest gradient component fell below gtol */
+  int iterations;                 /* the reference's count (OptResult::iterations) */
+  int evaluations;                /* energy + gradient evaluations, line-search trials included */
+  double energy_ev;               /* total energy at the final geometry */
+  double heat_of_formation_kcal;  /* at the final geometry */
+  double max_gradient;            /* eV/Bohr, at the final geometry */
+} pm3gpu_opt_result;
+void pm3gpu_default_opt_options(pm3gpu_opt_options* opt);
+int pm3gpu_optimize_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
+                          double* xyz_bohr, const pm3gpu_options* opts, const pm3gpu_opt_options* opt,
+                          pm3gpu_opt_result* out, double* gradients);
+
 /* pm3gpu_batch with z / xyz_bohr / atom_offsets already resident in device memory
  * (device pointers); results, charges and gradients are host buffers as above. */
 int pm3gpu_batch_device_inputs(pm3gpu_ctx* ctx, int n_mol, const int32_t* d_atom_offsets,

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <mutex>
 #include <random>
 #include <string>
@@ -1330,6 +1331,8 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
   return PM3GPU_OK;
 }
 
+#include "geom_opt.cuh"
+
 #include "autotune.cuh"
 
 }  // namespace
@@ -1572,6 +1575,33 @@ int pm3gpu_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t* z
   w.grad = gradients != nullptr;
   return run_batch(c, n_mol, offs, z, xyz, nullptr, nullptr, opts ? opts : &d, opts ? per_mol : 0, w, results, charges,
                    gradients, nullptr, nullptr);
+}
+
+void pm3gpu_default_opt_options(pm3gpu_opt_options* o) {
+  if (!o) return;
+  o->max_iter = 200;
+  o->gtol = 1.0e-3;
+  o->history = 8;
+}
+
+int pm3gpu_optimize_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t* z, double* xyz,
+                          const pm3gpu_options* opts, const pm3gpu_opt_options* opt, pm3gpu_opt_result* out,
+                          double* gradients) {
+  if (!c || n_mol < 0 || !offs || !z || !xyz || !out) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  pm3gpu_opt_options o;
+  pm3gpu_default_opt_options(&o);
+  if (opt) o = *opt;
+  if (o.max_iter < 0 || o.history < 0 || !(o.gtol >= 0.0)) return fail(c, PM3GPU_INVALID_INPUT, "bad optimizer options");
+  for (int m = 0; m < n_mol; ++m)
+    if (offs[m + 1] < offs[m]) return fail(c, PM3GPU_INVALID_INPUT, "atom_offsets must be non-decreasing");
+  for (long long k = 0; k < 3LL * offs[n_mol]; ++k)
+    if (!std::isfinite(xyz[k])) return fail(c, PM3GPU_INVALID_INPUT, "non-finite coordinate");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->err.clear();
+  pm3gpu_options d;
+  pm3gpu_default_options(&d);
+  return optimize_batch(c, n_mol, offs, z, xyz, opts ? opts : &d, o, out, gradients);
 }
 
 int pm3gpu_batch_device_inputs(pm3gpu_ctx* c, int n_mol, const int32_t* d_offs, const int32_t* d_z, const double* d_xyz,

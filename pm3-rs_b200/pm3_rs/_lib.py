@@ -67,6 +67,20 @@ class Result(ctypes.Structure):
     ]
 
 
+class OptOptions(ctypes.Structure):
+    """pm3gpu_opt_options: OptOptions of pm3-rs src/optimizer.rs:15-35 (max_iter, gtol, history)."""
+    _fields_ = [("max_iter", ctypes.c_int), ("gtol", ctypes.c_double), ("history", ctypes.c_int)]
+
+
+class OptResult(ctypes.Structure):
+    """pm3gpu_opt_result: one molecule's optimisation outcome."""
+    _fields_ = [
+        ("status", ctypes.c_int), ("converged", ctypes.c_int), ("iterations", ctypes.c_int),
+        ("evaluations", ctypes.c_int), ("energy_ev", ctypes.c_double), ("heat_of_formation_kcal", ctypes.c_double),
+        ("max_gradient", ctypes.c_double),
+    ]
+
+
 class Element(ctypes.Structure):
     """pm3gpu_element: the Pm3Element fields of the s/p path (pm3-rs src/params.rs:20-92)."""
     _fields_ = [
@@ -93,7 +107,8 @@ EXPORTS = [
     "pm3gpu_context_create", "pm3gpu_context_destroy", "pm3gpu_last_error_message",
     "pm3gpu_set_stream", "pm3gpu_single_point", "pm3gpu_gradient", "pm3gpu_batch",
     "pm3gpu_batch_device_inputs", "pm3gpu_core_hamiltonian", "pm3gpu_fock", "pm3gpu_last_timings",
-    "pm3gpu_last_kernel_launches", "pm3gpu_last_launch_layout", "pm3gpu_dgemm", "pm3gpu_last_transfer_bytes", "pm3gpu_last_phase_cycles",
+    "pm3gpu_last_kernel_launches", "pm3gpu_last_launch_layout", "pm3gpu_dgemm", "pm3gpu_default_opt_options",
+    "pm3gpu_optimize_batch", "pm3gpu_last_transfer_bytes", "pm3gpu_last_phase_cycles",
     "pm3gpu_single_point_noalloc", "pm3gpu_set_large_threshold", "pm3gpu_last_large_phase_ms",
     "pm3gpu_set_precision", "pm3gpu_last_large_trace", "pm3gpu_autotune", "pm3gpu_load_tuning",
     "pm3gpu_tuning_choice",
@@ -143,6 +158,10 @@ def load() -> ctypes.CDLL:
     L.pm3gpu_fock.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _D, _D, _D, _D, _D, _D]
     L.pm3gpu_last_timings.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     L.pm3gpu_last_kernel_launches.argtypes = [ctypes.c_void_p]
+    L.pm3gpu_default_opt_options.argtypes = [ctypes.POINTER(OptOptions)]
+    L.pm3gpu_default_opt_options.restype = None
+    L.pm3gpu_optimize_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, ctypes.POINTER(Options),
+                                        ctypes.POINTER(OptOptions), ctypes.POINTER(OptResult), _D]
     L.pm3gpu_dgemm.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                ctypes.c_double, _D, ctypes.c_int, _D, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
     L.pm3gpu_last_launch_layout.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]

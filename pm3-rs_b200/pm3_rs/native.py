@@ -217,3 +217,60 @@ def batch(offsets, z, xyz_bohr, opts=None, want_gradient=False, device: int = 0,
     if rc != _lib.OK:
         raise ValueError(ctx.last_error() or f"pm3gpu status {rc}")
     return BatchResult(list(results)[:n_mol], charges, grads, offsets)
+
+
+def optimize_batch(offsets, z, xyz_bohr, opts=None, max_iter: int = 200, gtol: float = 1.0e-3, history: int = 8,
+                   want_gradient: bool = False, device: int = 0, context: _lib.Context | None = None) -> dict:
+    """Geometry optimisation of many molecules at once (pm3gpu_optimize_batch): the reference's
+    L-BFGS (src/optimizer.rs:77-221) per molecule, each round one batched SCF + gradient launch over
+    every molecule's pending geometry. Bohr in and out. Returns ``positions_bohr`` (final, packed
+    like the input), ``status``, ``converged``, ``iterations``, ``evaluations``, ``energy_ev``,
+    ``heat_of_formation_kcal``, ``max_gradient`` (eV/Bohr) per molecule, and ``gradients`` when
+    asked for."""
+    ctx = context if context is not None else _lib.default_context(device)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+    z = np.ascontiguousarray(z, dtype=np.int32)
+    x = np.ascontiguousarray(np.asarray(xyz_bohr, dtype=np.float64).reshape(-1, 3)).copy()
+    n_mol = len(offsets) - 1
+    o = opts if opts is not None else options()
+    oo = _lib.OptOptions(int(max_iter), float(gtol), int(history))
+    res = (_lib.OptResult * max(n_mol, 1))()
+    g = np.zeros_like(x) if want_gradient else None
+    rc = ctx.lib.pm3gpu_optimize_batch(ctx.ptr, n_mol, _ip(offsets), _ip(z), _dp(x), ctypes.byref(o), ctypes.byref(oo),
+                                       res, _dp(g) if g is not None else None)
+    if rc != 0:
+        raise ValueError(ctx.last_error() or f"pm3gpu status {rc}")
+    r = np.ctypeslib.as_array(res)[:n_mol]
+    out = {"positions_bohr": x, "status": r["status"].copy(), "converged": r["converged"].astype(bool),
+           "iterations": r["iterations"].copy(), "evaluations": r["evaluations"].copy(),
+           "energy_ev": r["energy_ev"].copy(), "heat_of_formation_kcal": r["heat_of_formation_kcal"].copy(),
+           "max_gradient": r["max_gradient"].copy()}
+    if g is not None:
+        out["gradients"] = g
+    return out
+
+
+def optimize(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+             reference: str = "auto", method: str = "pm3", field=None, max_steps: int = 200,
+             force_tol=None) -> dict:
+    """Geometry optimisation (src/python.rs:430-486): positions in Angstrom; ``force_tol`` in
+    eV/Angstrom (None keeps OptOptions' 1e-3 eV/Bohr). Same keys as the reference:
+    ``positions_angstrom`` / ``positions``, ``energy_hartree``, ``energy_ev``,
+    ``heat_of_formation_kcal``, ``converged``, ``iterations`` / ``steps``."""
+    _check_method(method, field)
+    z, xyz = _as_arrays(numbers, positions)
+    gtol = 1.0e-3 if force_tol is None else float(force_tol) * PM3_A0
+    r = optimize_batch([0, len(z)], z, xyz, options(charge, multiplicity, reference), max_iter=max_steps, gtol=gtol)
+    if r["status"][0] != 0:
+        raise ValueError(_lib.default_context().last_error() or f"pm3gpu status {int(r['status'][0])}")
+    coords = (r["positions_bohr"] * PM3_A0).tolist()
+    return {
+        "positions_angstrom": coords,
+        "positions": coords,
+        "energy_hartree": float(r["energy_ev"][0]) * EV_TO_HARTREE,
+        "energy_ev": float(r["energy_ev"][0]),
+        "heat_of_formation_kcal": float(r["heat_of_formation_kcal"][0]),
+        "converged": bool(r["converged"][0]),
+        "iterations": int(r["iterations"][0]),
+        "steps": int(r["iterations"][0]),
+    }
