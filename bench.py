@@ -57,6 +57,19 @@ def _oracle_worker(args):
     return n_conv
 
 
+def _oracle_opt_worker(mols):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import lbfgs_ref
+
+    n_conv = 0
+    for z, xyz in mols:
+        try:
+            n_conv += int(lbfgs_ref.optimize(z, xyz)["converged"])
+        except Exception:
+            pass
+    return n_conv
+
+
 def cpu_throughput(mols, cores, steps=1, warmup=0, opts=None):
     """Converged molecules/s of the oracle over `mols` on `cores` spawn workers (one thread each)."""
     import multiprocessing as mp
@@ -755,6 +768,74 @@ def guess_main(args, rank):
     print(json.dumps(line))
 
 
+def optimize_main(args, rank, cores):
+    """Batched geometry optimisation (pm3gpu_optimize_batch): 256 generated organics of 5-20
+    atoms from the generator's geometry (standard bond lengths and angles, not minima), the
+    reference's L-BFGS with OptOptions' defaults. A step = one batched optimisation of all of them
+    (every round one SCF + gradient launch over the pending geometries); value = converged
+    optimisations per second. Inputs and results are host arrays: the call is the public entry,
+    so `e2e` is the same measurement. CPU: the restated optimiser over the oracle on a sample."""
+    if rank != 0:
+        return
+    from pm3_rs import native, workloads
+
+    n_mol = args.n_mol or 256
+    mols = [(np.asarray(z), np.asarray(xyz) * A2B) for z, xyz in workloads.organic_batch(n_mol, 5, 20, seed=4242)]
+    offs, z, xyz = workloads.pack(mols)
+    unit = "optimisations/s"
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"  # one thread per spawned oracle process
+    os.environ["OMP_NUM_THREADS"] = "1"
+    if args.impl == "reference":
+        sample = mols[:max(cores, 16)]
+        import multiprocessing as mp
+
+        with mp.get_context("spawn").Pool(cores) as pool:
+            chunks = [sample[i::cores] for i in range(cores)]
+            t0 = time.perf_counter()
+            n = sum(pool.map(_oracle_opt_worker, chunks))
+            el = time.perf_counter() - t0
+        v = n / el
+        print(json.dumps({"impl": "reference", "metric": "converged geometry optimisations/s (batched)", "value": v,
+                          "unit": unit, "n_gpus": args.gpus, "steps": 1, "warmup": 0, "higher_is_better": True,
+                          "cpu_baseline": {"value": v, "unit": unit, "cores": cores, "kind": "port",
+                                           "sample": f"first {len(sample)} of the {n_mol} molecules"},
+                          "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+    import torch
+
+    for _ in range(max(args.warmup, 1)):
+        native.optimize_batch(offs, z, xyz)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = native.optimize_batch(offs, z, xyz)
+        times.append(time.perf_counter() - t0)
+    conv = int(r["converged"].sum())
+    t = float(np.median(times))
+    value = conv / t
+    line = {"metric": "converged geometry optimisations/s (batched)", "value": value, "unit": unit, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"optimize-{n_mol}: generated organics of 5-20 atoms from standard geometry, "
+                                   "RHF PM3, reference OptOptions (L-BFGS, gtol 1e-3 eV/Bohr, 200 iterations)",
+                       "converged": conv, "mean_iterations": float(np.mean(r["iterations"])),
+                       "mean_evaluations": float(np.mean(r["evaluations"])), "timing": "wall clock of the call"},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None}}
+    if not args.no_cpu_baseline:
+        sample = mols[:max(cores, 16)]
+        import multiprocessing as mp
+
+        with mp.get_context("spawn").Pool(cores) as pool:
+            chunks = [sample[i::cores] for i in range(cores)]
+            t0 = time.perf_counter()
+            n = sum(pool.map(_oracle_opt_worker, chunks))
+            el = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": n / el, "unit": unit, "cores": cores, "kind": "port",
+                                "sample": f"first {len(sample)} of the {n_mol} molecules, one process per core"}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -765,7 +846,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="organics-4096",
-                    choices=["organics-4096", "radicals-2048", "water-2000", "learned-guess"],
+                    choices=["organics-4096", "radicals-2048", "water-2000", "learned-guess", "optimize-256"],
                     help="organics-4096: the batched headline (default); radicals-2048: 2048 doublet radicals "
                          "of 10-80 atoms, UHF + analytic gradients; water-2000: one 6000-atom water cluster "
                          "(12000 basis functions) on the whole-GPU path, seconds per SCF")
@@ -811,6 +892,8 @@ def main():
         return water_main(args, rank)
     if args.workload == "learned-guess":
         return guess_main(args, rank)
+    if args.workload == "optimize-256":
+        return optimize_main(args, rank, cores)
     desc, oracle_opts, gpu_opts, want_grad, default_n = workload_spec(args)
     if args.n_mol is None:
         args.n_mol = default_n
