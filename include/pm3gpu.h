@@ -235,6 +235,19 @@ int pm3gpu_optimize_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offset
                           double* xyz_bohr, const pm3gpu_options* opts, const pm3gpu_opt_options* opt,
                           pm3gpu_opt_result* out, double* gradients);
 
+/* Cartesian Hessians of many molecules by central differences of the analytic gradient: the
+ * reference's numerical_hessian (src/hessian.rs:268-319). Column j of molecule m is
+ * (g(x + step e_j) - g(x - step e_j)) / (2 step) with j = 3 * atom + axis, then the matrix is averaged
+ * with its transpose. The SCF is tightened as the reference does for second derivatives
+ * (src/hessian.rs:169-175: e_tol <= 1e-12 eV, p_tol <= 1e-11, max_scf >= 500). Every displaced
+ * geometry of every molecule runs in the batched SCF + gradient launch. hessians receives each
+ * molecule's (3 n_m) x (3 n_m) row-major block in eV/Bohr^2, packed molecule after molecule;
+ * status[m] is PM3GPU_OK or the run_pm3 status of the molecule's first failing displacement (its
+ * block is then zero). step in Bohr (the reference's Python entry points use 1e-3). */
+int pm3gpu_numerical_hessian_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
+                                   const double* xyz_bohr, const pm3gpu_options* opts, double step,
+                                   double* hessians, int* status);
+
 /* pm3gpu_batch with z / xyz_bohr / atom_offsets already resident in device memory
  * (device pointers); results, charges and gradients are host buffers as above. */
 int pm3gpu_batch_device_inputs(pm3gpu_ctx* ctx, int n_mol, const int32_t* d_atom_offsets,

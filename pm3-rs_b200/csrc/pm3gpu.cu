@@ -1332,6 +1332,7 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
 }
 
 #include "geom_opt.cuh"
+#include "hessian.cuh"
 
 #include "autotune.cuh"
 
@@ -1602,6 +1603,23 @@ int pm3gpu_optimize_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const i
   pm3gpu_options d;
   pm3gpu_default_options(&d);
   return optimize_batch(c, n_mol, offs, z, xyz, opts ? opts : &d, o, out, gradients);
+}
+
+int pm3gpu_numerical_hessian_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t* z,
+                                   const double* xyz, const pm3gpu_options* opts, double step, double* hessians,
+                                   int* status) {
+  if (!c || n_mol < 0 || !offs || !z || !xyz || !hessians || !status) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  if (!(step > 0.0) || !std::isfinite(step)) return fail(c, PM3GPU_INVALID_INPUT, "step must be positive and finite");
+  for (int m = 0; m < n_mol; ++m)
+    if (offs[m + 1] < offs[m]) return fail(c, PM3GPU_INVALID_INPUT, "atom_offsets must be non-decreasing");
+  for (long long k = 0; k < 3LL * offs[n_mol]; ++k)
+    if (!std::isfinite(xyz[k])) return fail(c, PM3GPU_INVALID_INPUT, "non-finite coordinate");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->err.clear();
+  pm3gpu_options d;
+  pm3gpu_default_options(&d);
+  return hessian_batch(c, n_mol, offs, z, xyz, opts ? opts : &d, step, hessians, status);
 }
 
 int pm3gpu_batch_device_inputs(pm3gpu_ctx* c, int n_mol, const int32_t* d_offs, const int32_t* d_z, const double* d_xyz,

@@ -274,3 +274,83 @@ def optimize(numbers: Sequence[int], positions, charge: float = 0.0, multiplicit
         "iterations": int(r["iterations"][0]),
         "steps": int(r["iterations"][0]),
     }
+
+
+def numerical_hessian_batch(offsets, z, xyz_bohr, opts=None, step: float = 1.0e-3, device: int = 0,
+                            context: _lib.Context | None = None) -> dict:
+    """Cartesian Hessians of many molecules by central differences of the analytic gradient
+    (pm3gpu_numerical_hessian_batch; the reference's numerical_hessian, src/hessian.rs:268-319):
+    every displaced geometry of every molecule runs in the batched SCF + gradient launch. Bohr in;
+    returns ``hessians`` (one (3n, 3n) array per molecule, eV/Bohr^2) and ``status``."""
+    ctx = context if context is not None else _lib.default_context(device)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+    z = np.ascontiguousarray(z, dtype=np.int32)
+    x = np.ascontiguousarray(np.asarray(xyz_bohr, dtype=np.float64).reshape(-1, 3))
+    n_mol = len(offsets) - 1
+    o = opts if opts is not None else options()
+    nd = 3 * np.diff(offsets).astype(np.int64)
+    hoff = np.concatenate([[0], np.cumsum(nd * nd)])
+    flat = np.zeros(int(hoff[-1]))
+    status = np.zeros(max(n_mol, 1), dtype=np.int32)
+    rc = ctx.lib.pm3gpu_numerical_hessian_batch(ctx.ptr, n_mol, _ip(offsets), _ip(z), _dp(x), ctypes.byref(o),
+                                                float(step), _dp(flat), _ip(status))
+    if rc != 0:
+        raise ValueError(ctx.last_error() or f"pm3gpu status {rc}")
+    hs = [flat[hoff[m]:hoff[m + 1]].reshape(nd[m], nd[m]) for m in range(n_mol)]
+    return {"hessians": hs, "status": status[:n_mol].copy()}
+
+
+def numerical_hessian(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+                      reference: str = "auto", step: float = 1.0e-3) -> np.ndarray:
+    """One molecule's gradient-difference Hessian (eV/Bohr^2), positions in Angstrom, ``step`` in
+    Bohr (src/hessian.rs:268-319)."""
+    z, xyz = _as_arrays(numbers, positions)
+    r = numerical_hessian_batch([0, len(z)], z, xyz, options(charge, multiplicity, reference), step=step)
+    if r["status"][0] != 0:
+        raise ValueError(_lib.default_context().last_error() or f"pm3gpu status {int(r['status'][0])}")
+    return r["hessians"][0]
+
+
+def hessian(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+            reference: str = "auto", method: str = "pm3", field=None, cphf_max_iter=None) -> dict:
+    """Cartesian Hessian (src/python.rs:693-739): same signature and keys
+    (``hessian_hartree_per_bohr2`` row-major 3N x 3N lists, ``ndof``). Computed by central
+    differences of the analytic gradient with a 1e-3 Bohr step (the reference's numerical_hessian,
+    which its own tests hold to 5e-3 eV/Bohr^2 of the CPHF one); ``cphf_max_iter`` caps CPHF
+    iterations, which this path does not run."""
+    _check_method(method, field)
+    h = numerical_hessian(numbers, positions, charge, multiplicity, reference, 1.0e-3)
+    return {"hessian_hartree_per_bohr2": (h * EV_TO_HARTREE).tolist(), "ndof": int(h.shape[0])}
+
+
+def atomic_masses(numbers: Sequence[int]) -> list:
+    """Tabulated atomic masses (amu) of the parameter set, one per atom."""
+    elems, _ = _lib.standard_parameters()
+    table = {int(e.z): float(e.mass) for e in elems}
+    out = []
+    for zv in np.asarray(numbers).reshape(-1):
+        if int(zv) not in table:
+            raise ValueError(f"no PM3 parameters for Z={int(zv)} on pm3gpu")
+        out.append(table[int(zv)])
+    return out
+
+
+def frequencies(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+                reference: str = "auto", method: str = "pm3", field=None, cphf_max_iter=None) -> dict:
+    """Harmonic vibrational frequencies (src/python.rs:498-556): ``frequencies_cm``,
+    ``eigenvalues``, ``modes`` (mass-weighted, one row per degree of freedom), ``masses``,
+    ``n_rigid`` and ``rigid_residual_cm``, from the gradient-difference Hessian (see ``hessian``)."""
+    from . import vibrations
+
+    _check_method(method, field)
+    h = numerical_hessian(numbers, positions, charge, multiplicity, reference, 1.0e-3)
+    masses = atomic_masses(numbers)
+    vib = vibrations.vibrational_analysis(h, np.asarray(positions, dtype=np.float64).reshape(-1, 3), masses)
+    return {
+        "frequencies_cm": vib["frequencies_cm"],
+        "eigenvalues": vib["eigenvalues"],
+        "modes": vib["modes"].tolist(),
+        "masses": masses,
+        "n_rigid": vib["n_rigid"],
+        "rigid_residual_cm": vib["rigid_residual_cm"],
+    }

@@ -1,0 +1,70 @@
+"""Batched gradient-difference Hessians (pm3gpu_numerical_hessian_batch) against the CPU
+restatement of the reference's numerical_hessian (oracle/hessian_ref.py) driving the oracle's
+gradients, and the frequencies built from them against the reference's MOPAC-pinned water test
+(tests/molecules.rs:121-138).
+
+Both sides difference gradients that agree to the gradient parity bar (about 1e-9 eV/Bohr under
+the tightened SCF), divided by 2h = 2e-3 Bohr, so the Hessians agree to about 1e-6 eV/Bohr^2; the
+bar is 1e-5 eV/Bohr^2 on entries of order 1-50."""
+import numpy as np
+import pytest
+
+import hessian_ref
+from helpers import A2B, GOLDEN, parse
+from pm3_rs import native, workloads
+
+pytestmark = pytest.mark.gpu
+
+HESSIAN_ATOL = 1.0e-5  # eV/Bohr^2
+
+
+def _molecules():
+    mols = [parse(GOLDEN[k][0]) for k in ("water", "ammonia", "formaldehyde", "methane", "h2s", "hcl")]
+    for seed in (1, 4, 5):
+        z, xyz = workloads.organic(6, seed)
+        mols.append((np.asarray(z), np.asarray(xyz)))
+    return mols
+
+
+def test_batched_hessians_match_the_restated_reference():
+    mols = _molecules()
+    offs, z, xyz = workloads.pack(mols)
+    got = native.numerical_hessian_batch(offs, z, xyz * A2B)
+    for m, (zm, xm) in enumerate(mols):
+        ref = hessian_ref.numerical_hessian(zm, xm * A2B)
+        h = got["hessians"][m]
+        err = np.abs(h - ref).max()
+        print(f"mol {m} ({len(zm)} atoms): max |dH| {err:.2e} eV/Bohr^2 of max |H| {np.abs(ref).max():.1f}")
+        assert got["status"][m] == 0
+        assert h.shape == (3 * len(zm), 3 * len(zm))
+        assert np.array_equal(h, h.T)
+        assert err < HESSIAN_ATOL
+
+
+def test_frequencies_of_the_relaxed_water_match_mopac():
+    z, xyz = parse(GOLDEN["water"][0])
+    r = native.optimize(z, xyz)
+    f = native.frequencies(z, r["positions_angstrom"])
+    assert f["n_rigid"] == 6 and f["masses"] == native.atomic_masses(z)
+    v = np.array(f["frequencies_cm"])
+    assert np.count_nonzero(v == 0.0) == 6
+    for got, want in zip(np.sort(v)[-3:], [1743.46, 3868.68, 3989.81]):
+        assert abs(got - want) < 2.0, (got, want)
+    h = native.hessian(z, r["positions_angstrom"])
+    assert h["ndof"] == 9 and len(h["hessian_hartree_per_bohr2"]) == 9
+
+
+def test_a_failing_molecule_keeps_its_own_status():
+    """An element outside the path fails its own molecule only (its block stays zero); an empty
+    molecule has an empty Hessian."""
+    water = parse(GOLDEN["water"][0])
+    iron = (np.array([26, 1], np.int32), np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 1.6]]))
+    empty = (np.zeros(0, np.int32), np.zeros((0, 3)))
+    offs, z, xyz = workloads.pack([water, iron, empty, water])
+    got = native.numerical_hessian_batch(offs, z, xyz * A2B)
+    assert got["status"][0] == 0 and got["status"][3] == 0 and got["status"][2] == 0
+    assert got["status"][1] != 0 and not got["hessians"][1].any()
+    assert got["hessians"][2].shape == (0, 0)
+    assert np.abs(got["hessians"][0] - got["hessians"][3]).max() < 1.0e-6
+    with pytest.raises(ValueError):
+        native.numerical_hessian_batch(offs, z, xyz * A2B, step=0.0)
