@@ -54,6 +54,13 @@ extern "C" {
 #define PM3GPU_STABILITY_OFF 0
 #define PM3GPU_STABILITY_AUTO 1
 #define PM3GPU_STABILITY_ALWAYS 2
+/* Method variants (corrections::Variant, src/corrections/mod.rs:165-191). PM3-D3 adds the Grimme
+ * D3 dispersion energy (src/corrections/d3.rs) to total_ev and the heat of formation, and its
+ * gradient to the SCF gradient. The D3H4 family is not built: PM3GPU_UNSUPPORTED. */
+#define PM3GPU_VARIANT_PM3 0
+#define PM3GPU_VARIANT_D3 1
+#define PM3GPU_VARIANT_D3H4 2
+#define PM3GPU_VARIANT_D3H4X 3
 
 typedef struct pm3gpu_ctx pm3gpu_ctx;
 
@@ -73,6 +80,7 @@ typedef struct {
   double level_shift_ev;  /* 0 */
   double damping;         /* 0 */
   int scf_memory_mb;      /* 512: accelerator-history budget (sets the DIIS depth) */
+  int variant;            /* PM3GPU_VARIANT_* (Pm3Options::variant, src/scf.rs:184): 0 plain PM3 */
 } pm3gpu_options;
 
 /* Pm3Result scalar fields (src/scf.rs:353-396). Arrays are returned through caller buffers. */
@@ -247,6 +255,12 @@ int pm3gpu_optimize_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offset
 int pm3gpu_numerical_hessian_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
                                    const double* xyz_bohr, const pm3gpu_options* opts, double step,
                                    double* hessians, int* status);
+
+/* The D3 dispersion correction alone for many molecules (src/corrections/d3.rs:360-458): d3_set 1 =
+ * D3Params::pm3_d3, 2 = D3Params::pm3_d3h4. energies[n_mol] in eV; gradients[3 * total atoms]
+ * (optional) in eV/Bohr. Elements outside the D3 table contribute nothing, as in the reference. */
+int pm3gpu_d3_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
+                    const double* xyz_bohr, int d3_set, double* energies, double* gradients);
 
 /* pm3gpu_batch with z / xyz_bohr / atom_offsets already resident in device memory
  * (device pointers); results, charges and gradients are host buffers as above. */

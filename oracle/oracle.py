@@ -38,6 +38,7 @@ class Options(ctypes.Structure):
         ("level_shift_ev", ctypes.c_double),
         ("damping", ctypes.c_double),
         ("scf_memory_mb", ctypes.c_int),
+        ("variant", ctypes.c_int),
     ]
 
 
@@ -104,6 +105,9 @@ def lib():
     L.oracle_set_parameters.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
     L.oracle_reset_parameters.argtypes = []
     L.oracle_reset_parameters.restype = None
+    L.oracle_d3.argtypes = [ctypes.c_int, _I, _D, ctypes.c_int, _D, _D, _D]
+    L.oracle_d3_c6.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+    L.oracle_d3_c6.restype = ctypes.c_double
     try:
         import scipy.linalg.cython_blas as cb
         import scipy.linalg.cython_lapack as cl
@@ -285,3 +289,21 @@ def eigh(a):
     if lib().oracle_eigh(n, _dp(a), _dp(w), _dp(v)) != 0:
         raise OracleError(5, "eigh")
     return w, v
+
+
+def d3(z, xyz_bohr, d3_set=1, want_gradient=True):
+    """D3 dispersion (src/corrections/d3.rs) of one molecule: (energy eV, gradient eV/Bohr [n, 3]
+    or None, coordination numbers [n]). d3_set 1 = PM3-D3 parameters, 2 = the PM3-D3H4 ones."""
+    z = np.ascontiguousarray(z, dtype=np.int32)
+    xyz = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1, 3)
+    e = np.zeros(1)
+    g = np.zeros((len(z), 3)) if want_gradient else None
+    cn = np.zeros(len(z))
+    code = lib().oracle_d3(len(z), _ip(z), _dp(xyz), int(d3_set), _dp(e), _dp(g), _dp(cn))
+    if code != 0:
+        raise OracleError(code, "d3")
+    return float(e[0]), g, cn
+
+
+def d3_c6(zi, zj, cni, cnj) -> float:
+    return lib().oracle_d3_c6(int(zi), int(zj), float(cni), float(cnj))

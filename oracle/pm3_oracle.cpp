@@ -1570,6 +1570,7 @@ void oracle_default_options(oracle_options* o) {  // scf.rs:259-287
   o->level_shift_ev = 0.0;
   o->damping = 0.0;
   o->scf_memory_mb = 512;
+  o->variant = 0;
 }
 
 void oracle_set_lapack(void* dsyevd, void* dgemm) {
@@ -1723,6 +1724,10 @@ int oracle_single_point(int n_atoms, const int* z, const double* xyz_bohr, const
     set_err(errbuf, errlen, "multiplicity must be >= 1");
     return 1;
   }
+  if (O.variant != 0 && O.variant != 1) {
+    set_err(errbuf, errlen, "variant outside PM3 / PM3-D3");
+    return 1;
+  }
   if (!build_molecule(n_atoms, z, xyz_bohr, m, err)) {
     set_err(errbuf, errlen, err.msg);
     return err.code;
@@ -1818,7 +1823,10 @@ int oracle_single_point(int n_atoms, const int* z, const double* xyz_bohr, const
   double improvement = std::max(first_ev - state.electronic, 0.0);
   double core_ev = core_core_energy(m);
   double electronic = state.electronic;
-  double total = electronic + core_ev;
+  // post-SCF classical correction of the method variant (scf.rs:740-743): D3 for PM3-D3
+  double correction_ev = 0.0;
+  if (O.variant == 1) oracle_d3(n_atoms, z, xyz_bohr, 1, &correction_ev, nullptr, nullptr);
+  double total = electronic + core_ev + correction_ev;
   double e_isol = 0.0, eheat = 0.0;
   for (int i = 0; i < m.natom; ++i) {
     e_isol += m.el[i]->e_isol;
@@ -1898,6 +1906,12 @@ int oracle_single_point(int n_atoms, const int* z, const double* xyz_bohr, const
     } else {
       Mat none;
       electronic_gradient(m, state.density, none, none, false, g);
+    }
+    if (O.variant == 1) {  // add_correction_gradient (gradient.rs:324-357)
+      std::vector<double> gd(g.size(), 0.0);
+      double ed = 0.0;
+      oracle_d3(n_atoms, z, xyz_bohr, 1, &ed, gd.data(), nullptr);
+      for (size_t k = 0; k < g.size(); ++k) g[k] += gd[k];
     }
     std::memcpy(gradient, g.data(), g.size() * sizeof(double));
   }

@@ -29,6 +29,7 @@ typedef struct {
   double level_shift_ev;
   double damping;
   int scf_memory_mb;
+  int variant;       /* 0 PM3, 1 PM3-D3 (corrections::Variant, src/corrections/mod.rs:165-178) */
 } oracle_options;
 
 typedef struct {
@@ -49,6 +50,14 @@ void oracle_default_options(oracle_options* o);
 void oracle_set_lapack(void* dsyevd, void* dgemm);
 
 int oracle_nao(int n_atoms, const int* z);
+
+/* Grimme D3 dispersion of one molecule (src/corrections/d3.rs): d3_set 1 = D3Params::pm3_d3,
+ * 2 = D3Params::pm3_d3h4. energy_ev receives the energy (eV); gradient[3n] (eV/Bohr, forward-mode
+ * dual numbers as src/gradient.rs:324-357) and cn[n] (coordination numbers) are optional. */
+int oracle_d3(int n_atoms, const int* z, const double* xyz_bohr, int d3_set, double* energy_ev, double* gradient,
+              double* cn);
+/* getc6 (d3.rs:212-236) for one element pair at the given coordination numbers. */
+double oracle_d3_c6(int zi, int zj, double cni, double cnj);
 
 /* Full single point (run_pm3). charges[n_atoms] required; density[nao*nao], mo_energies[nao],
  * gradient[3*n_atoms] (eV/Bohr, closed-form Hellmann-Feynman) are optional (NULL = skip).

@@ -137,6 +137,7 @@ struct pm3gpu_ctx {
   DevBuf gp, gpb, gm, gv, gg;
   DevBuf gqmols, gatom, gao, gcoord, gX, gY, gZ[3], gH[3], gdH, gdZ, gT, gM, gidx, gXb, gTb, gMb, gdY, gpart, gguess, gdens;
   DevBuf gwt, gerr;  // inference: transposed hidden weights (tcgen05 B operands), kernel error flag
+  DevBuf d3buf;      // D3 correction: offsets, sets, coordination numbers, row energies, gradients
   int* h_gerr = nullptr;  // pinned copy of gerr, read after the stream's next synchronisation
 };
 
@@ -319,6 +320,12 @@ void plan_molecule(const pm3gpu_ctx* c, const int32_t* z, const double* xyz, int
   if (o->multiplicity < 1) {
     m.status = PM3GPU_INVALID_INPUT;
     m.msg = "multiplicity must be >= 1";
+    return;
+  }
+  if (o->variant != PM3GPU_VARIANT_PM3 && o->variant != PM3GPU_VARIANT_D3) {
+    m.status = (o->variant == PM3GPU_VARIANT_D3H4 || o->variant == PM3GPU_VARIANT_D3H4X) ? PM3GPU_UNSUPPORTED
+                                                                                          : PM3GPU_INVALID_INPUT;
+    m.msg = "method variant outside PM3 / PM3-D3 (the H4 and X corrections are not built)";
     return;
   }
   int nao = 0;
@@ -1082,6 +1089,8 @@ struct HostJobResult {
 // The run_pm3 flow over a batch (scf.rs:450-848): one persistent launch solves every
 // molecule and the stability-search rungs its first pass asks for; the host then selects
 // each molecule's state exactly as run_pm3 does and forms the epilogue.
+#include "d3.cuh"
+
 int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_z, const double* h_xyz,
               const int32_t* d_z, const double* d_xyz, const pm3gpu_options* opts, int per_mol, const Want& want,
               pm3gpu_result* results, double* charges, double* gradients, double* density, double* mo_energies,
@@ -1316,6 +1325,9 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
       std::memcpy(gradients + 3 * (size_t)p.atom0, gr.data() + 3 * (size_t)p.atom0, 24 * (size_t)p.natom);
     }
   }
+  // ---------------------------------------------------------------- post-SCF corrections
+  rc = apply_corrections(c, n_mol, h_offs, h_z, opts, per_mol, dz, dxyz, results, want.grad ? gradients : nullptr);
+  if (rc != PM3GPU_OK) return rc;
   cudaEventRecord(c->ev[3], c->stream);
   cudaEventRecord(c->ev[4], c->stream);
   cudaEventSynchronize(c->ev[4]);
@@ -1356,6 +1368,7 @@ void pm3gpu_default_options(pm3gpu_options* o) {  // scf.rs:259-287
   o->level_shift_ev = 0.0;
   o->damping = 0.0;
   o->scf_memory_mb = 512;
+  o->variant = PM3GPU_VARIANT_PM3;
 }
 
 int pm3gpu_supported_element(int z) { return supported(z) ? 1 : 0; }
@@ -1507,7 +1520,8 @@ void pm3gpu_context_destroy(pm3gpu_ctx* c) {
   for (DevBuf& b : c->tcbuf) b.release();
   for (DevBuf* b : {&c->gp, &c->gpb, &c->gm, &c->gv, &c->gg, &c->gqmols, &c->gatom, &c->gao, &c->gcoord, &c->gX, &c->gY,
                     &c->gZ[0], &c->gZ[1], &c->gZ[2], &c->gH[0], &c->gH[1], &c->gH[2], &c->gdH, &c->gdZ, &c->gT, &c->gM,
-                    &c->gidx, &c->gXb, &c->gTb, &c->gMb, &c->gdY, &c->gpart, &c->gguess, &c->gdens, &c->gwt, &c->gerr})
+                    &c->gidx, &c->gXb, &c->gTb, &c->gMb, &c->gdY, &c->gpart, &c->gguess, &c->gdens, &c->gwt, &c->gerr,
+                    &c->d3buf})
     b->release();
   if (c->h_gerr) cudaFreeHost(c->h_gerr);
   if (c->own) cudaStreamDestroy(c->own);
@@ -1603,6 +1617,31 @@ int pm3gpu_optimize_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const i
   pm3gpu_options d;
   pm3gpu_default_options(&d);
   return optimize_batch(c, n_mol, offs, z, xyz, opts ? opts : &d, o, out, gradients);
+}
+
+int pm3gpu_d3_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t* z, const double* xyz, int d3_set,
+                    double* energies, double* gradients) {
+  if (!c || n_mol < 0 || !offs || !z || !xyz || !energies) return fail(c, PM3GPU_INVALID_INPUT, "null argument");
+  if (d3_set != 1 && d3_set != 2) return fail(c, PM3GPU_INVALID_INPUT, "d3_set must be 1 (PM3-D3) or 2 (PM3-D3H4)");
+  if (offs[0] != 0) return fail(c, PM3GPU_INVALID_INPUT, "atom_offsets must start at 0");
+  for (int m = 0; m < n_mol; ++m)
+    if (offs[m + 1] < offs[m]) return fail(c, PM3GPU_INVALID_INPUT, "atom_offsets must be non-decreasing");
+  const int total = offs[n_mol];
+  for (long long k = 0; k < 3LL * total; ++k)
+    if (!std::isfinite(xyz[k])) return fail(c, PM3GPU_INVALID_INPUT, "non-finite coordinate");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->err.clear();
+  c->launches = 0;
+  std::fill(energies, energies + n_mol, 0.0);
+  if (gradients) std::fill(gradients, gradients + 3 * (size_t)total, 0.0);
+  if (n_mol == 0 || total == 0) return PM3GPU_OK;
+  CUDA_TRY(c, c->z.ensure(4 * (size_t)total));
+  CUDA_TRY(c, c->xyz.ensure(24 * (size_t)total));
+  CUDA_TRY(c, cudaMemcpyAsync(c->z.p, z, 4 * (size_t)total, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->xyz.p, xyz, 24 * (size_t)total, cudaMemcpyHostToDevice, c->stream));
+  std::vector<int32_t> set(n_mol, d3_set);
+  return d3_batch(c, n_mol, offs, set.data(), c->z.as<int32_t>(), c->xyz.as<double>(), energies, gradients);
 }
 
 int pm3gpu_numerical_hessian_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t* z,
@@ -2209,6 +2248,8 @@ int noalloc_run(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz,
     return fail(c, PM3GPU_INVALID_INPUT, "atom count outside 1..256 for the allocation-free path");
   if (o->guess == PM3GPU_GUESS_LEARNED)
     return fail(c, PM3GPU_INVALID_INPUT, "the learned guess is not available on the allocation-free path");
+  if (o->variant != PM3GPU_VARIANT_PM3)
+    return fail(c, PM3GPU_INVALID_INPUT, "post-SCF corrections are not available on the allocation-free path");
   MolPlan p;
   plan_molecule(c, z, xyz, n_atoms, o, p);
   result->nao = p.nao;

@@ -2,9 +2,10 @@
 
 Drop-in for ``pm3_rs.native`` of pm3-rs (python/pm3_rs/native.py:41-140 and
 src/python.rs:253-357): same functions, signatures, dictionary keys and units, and the same
-``ValueError`` on any failure (src/python.rs:22-24). ``method`` is limited to plain ``"pm3"``
-and ``field`` to ``None``: the post-SCF corrections and external fields are outside this
-library's path, and asking for them raises rather than being silently ignored.
+``ValueError`` on any failure (src/python.rs:22-24). ``method`` is ``"pm3"`` or ``"pm3-d3"`` (the
+D3 dispersion correction, added to the energy, heat of formation and gradient) and ``field`` is
+``None``: the H4 and X corrections and external fields are outside this library's path, and asking
+for them raises rather than being silently ignored.
 """
 from __future__ import annotations
 
@@ -30,12 +31,20 @@ def _parse_reference(reference: str) -> int:
     return _REFERENCES[key]
 
 
-def _check_method(method: str, field) -> None:
+# corrections::Variant::parse (src/corrections/mod.rs:180-191) -> PM3GPU_VARIANT_*
+_VARIANTS = {"pm3": 0, "pm3-d3": 1, "pm3-d3h4": 2, "pm3-d3h4x": 3}
+
+
+def _check_method(method: str, field) -> int:
+    """The method string's variant code; PM3 and PM3-D3 run here, the H4 family raises."""
     m = str(method).strip().lower().replace(" ", "-").replace("_", "-")
-    if m not in ("", "pm3"):
-        raise ValueError(f"method {method!r} is not available here: only plain 'pm3' runs on pm3gpu")
+    if m not in _VARIANTS:
+        raise ValueError(f"unknown method {method!r}: expected PM3, PM3-D3, PM3-D3H4 or PM3-D3H4X")
+    if _VARIANTS[m] > 1:
+        raise ValueError(f"method {method!r} is not available here: 'pm3' and 'pm3-d3' run on pm3gpu")
     if field is not None:
         raise ValueError("an external field is not available on pm3gpu")
+    return _VARIANTS[m]
 
 
 def _as_arrays(numbers, positions):
@@ -117,9 +126,9 @@ def single_point(numbers: Sequence[int], positions, charge: float = 0.0, multipl
     ``electronic_ev``, ``core_ev``, ``charges`` (Mulliken, e), ``dipole_debye`` ([x, y, z]),
     ``homo_ev``, ``lumo_ev``, ``converged`` and ``unrestricted``.
     """
-    _check_method(method, field)
+    variant = _check_method(method, field)
     z, xyz = _as_arrays(numbers, positions)
-    r = run(z, xyz, options(charge, multiplicity, reference))
+    r = run(z, xyz, options(charge, multiplicity, reference, variant=variant))
     return {
         "energy_hartree": r["total_ev"] * EV_TO_HARTREE,
         "energy_ev": r["total_ev"],
@@ -138,9 +147,9 @@ def single_point(numbers: Sequence[int], positions, charge: float = 0.0, multipl
 def gradient(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
              reference: str = "auto", method: str = "pm3", field=None) -> dict:
     """Energy and analytic gradient dE/dR (src/python.rs:299-357): Hartree/Bohr and eV/Angstrom."""
-    _check_method(method, field)
+    variant = _check_method(method, field)
     z, xyz = _as_arrays(numbers, positions)
-    r = run(z, xyz, options(charge, multiplicity, reference), want_gradient=True)
+    r = run(z, xyz, options(charge, multiplicity, reference, variant=variant), want_gradient=True)
     g = r["gradient"]
     return {
         "energy_hartree": r["total_ev"] * EV_TO_HARTREE,
@@ -257,10 +266,11 @@ def optimize(numbers: Sequence[int], positions, charge: float = 0.0, multiplicit
     eV/Angstrom (None keeps OptOptions' 1e-3 eV/Bohr). Same keys as the reference:
     ``positions_angstrom`` / ``positions``, ``energy_hartree``, ``energy_ev``,
     ``heat_of_formation_kcal``, ``converged``, ``iterations`` / ``steps``."""
-    _check_method(method, field)
+    variant = _check_method(method, field)
     z, xyz = _as_arrays(numbers, positions)
     gtol = 1.0e-3 if force_tol is None else float(force_tol) * PM3_A0
-    r = optimize_batch([0, len(z)], z, xyz, options(charge, multiplicity, reference), max_iter=max_steps, gtol=gtol)
+    r = optimize_batch([0, len(z)], z, xyz, options(charge, multiplicity, reference, variant=variant),
+                       max_iter=max_steps, gtol=gtol)
     if r["status"][0] != 0:
         raise ValueError(_lib.default_context().last_error() or f"pm3gpu status {int(r['status'][0])}")
     coords = (r["positions_bohr"] * PM3_A0).tolist()
@@ -301,11 +311,13 @@ def numerical_hessian_batch(offsets, z, xyz_bohr, opts=None, step: float = 1.0e-
 
 
 def numerical_hessian(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
-                      reference: str = "auto", step: float = 1.0e-3) -> np.ndarray:
+                      reference: str = "auto", step: float = 1.0e-3, method: str = "pm3") -> np.ndarray:
     """One molecule's gradient-difference Hessian (eV/Bohr^2), positions in Angstrom, ``step`` in
     Bohr (src/hessian.rs:268-319)."""
+    variant = _check_method(method, None)
     z, xyz = _as_arrays(numbers, positions)
-    r = numerical_hessian_batch([0, len(z)], z, xyz, options(charge, multiplicity, reference), step=step)
+    r = numerical_hessian_batch([0, len(z)], z, xyz, options(charge, multiplicity, reference, variant=variant),
+                                step=step)
     if r["status"][0] != 0:
         raise ValueError(_lib.default_context().last_error() or f"pm3gpu status {int(r['status'][0])}")
     return r["hessians"][0]
@@ -319,7 +331,7 @@ def hessian(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity
     which its own tests hold to 5e-3 eV/Bohr^2 of the CPHF one); ``cphf_max_iter`` caps CPHF
     iterations, which this path does not run."""
     _check_method(method, field)
-    h = numerical_hessian(numbers, positions, charge, multiplicity, reference, 1.0e-3)
+    h = numerical_hessian(numbers, positions, charge, multiplicity, reference, 1.0e-3, method)
     return {"hessian_hartree_per_bohr2": (h * EV_TO_HARTREE).tolist(), "ndof": int(h.shape[0])}
 
 
@@ -343,7 +355,7 @@ def frequencies(numbers: Sequence[int], positions, charge: float = 0.0, multipli
     from . import vibrations
 
     _check_method(method, field)
-    h = numerical_hessian(numbers, positions, charge, multiplicity, reference, 1.0e-3)
+    h = numerical_hessian(numbers, positions, charge, multiplicity, reference, 1.0e-3, method)
     masses = atomic_masses(numbers)
     vib = vibrations.vibrational_analysis(h, np.asarray(positions, dtype=np.float64).reshape(-1, 3), masses)
     return {
@@ -354,3 +366,25 @@ def frequencies(numbers: Sequence[int], positions, charge: float = 0.0, multipli
         "n_rigid": vib["n_rigid"],
         "rigid_residual_cm": vib["rigid_residual_cm"],
     }
+
+
+def d3_batch(offsets, z, xyz_bohr, d3_set: int = 1, want_gradient: bool = True, device: int = 0,
+             context: _lib.Context | None = None) -> dict:
+    """The D3 dispersion correction alone (pm3gpu_d3_batch; src/corrections/d3.rs:360-458) for many
+    molecules: ``energy_ev`` per molecule and ``gradient`` (eV/Bohr, packed like the input).
+    ``d3_set`` 1 = the PM3-D3 parameters, 2 = the PM3-D3H4 ones."""
+    ctx = context if context is not None else _lib.default_context(device)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+    z = np.ascontiguousarray(z, dtype=np.int32)
+    x = np.ascontiguousarray(np.asarray(xyz_bohr, dtype=np.float64).reshape(-1, 3))
+    n_mol = len(offsets) - 1
+    e = np.zeros(max(n_mol, 1))
+    g = np.zeros_like(x) if want_gradient else None
+    rc = ctx.lib.pm3gpu_d3_batch(ctx.ptr, n_mol, _ip(offsets), _ip(z), _dp(x), int(d3_set), _dp(e),
+                                 _dp(g) if g is not None else None)
+    if rc != 0:
+        raise ValueError(ctx.last_error() or f"pm3gpu status {rc}")
+    out = {"energy_ev": e[:n_mol].copy()}
+    if g is not None:
+        out["gradient"] = g
+    return out

@@ -94,3 +94,10 @@ def test_noalloc_rejects_molecule_beyond_scratch():
     z, xyz = workloads.organic(12, 101)
     x = np.asarray(xyz) * A2B
     _same(_call("noalloc", z, x, native.options()), _call("single_point", z, x, native.options()))
+
+
+def test_noalloc_has_no_post_scf_corrections():
+    """The allocation-free entry runs plain PM3 only: a PM3-D3 request is refused, not ignored."""
+    z, xyz = workloads.organic(8, 3)
+    rc, _, _, msg = _call("noalloc", z, np.asarray(xyz) * A2B, native.options(variant=1))
+    assert rc == _lib.INVALID_INPUT and "correction" in msg
