@@ -54,9 +54,11 @@ extern "C" {
 #define PM3GPU_STABILITY_OFF 0
 #define PM3GPU_STABILITY_AUTO 1
 #define PM3GPU_STABILITY_ALWAYS 2
-/* Method variants (corrections::Variant, src/corrections/mod.rs:165-191). PM3-D3 adds the Grimme
- * D3 dispersion energy (src/corrections/d3.rs) to total_ev and the heat of formation, and its
- * gradient to the SCF gradient. The D3H4 family is not built: PM3GPU_UNSUPPORTED. */
+/* Method variants (corrections::Variant, src/corrections/mod.rs:165-191). The variant's post-SCF
+ * correction (mod.rs:129-160) joins total_ev and the heat of formation, and its gradient the SCF
+ * gradient: PM3-D3 adds Grimme D3 dispersion (src/corrections/d3.rs, D3Params::pm3_d3); PM3-D3H4
+ * adds D3 with D3Params::pm3_d3h4, the H4 hydrogen-bond term and the H-H repulsion
+ * (src/corrections/h4.rs); PM3-D3H4X adds the halogen-bond term (src/corrections/hx.rs) too. */
 #define PM3GPU_VARIANT_PM3 0
 #define PM3GPU_VARIANT_D3 1
 #define PM3GPU_VARIANT_D3H4 2
@@ -262,6 +264,13 @@ int pm3gpu_numerical_hessian_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* at
 int pm3gpu_d3_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
                     const double* xyz_bohr, int d3_set, double* energies, double* gradients);
 
+/* The whole correction of a variant (PM3GPU_VARIANT_D3 / _D3H4 / _D3H4X) alone for many molecules:
+ * the CorrectionEnergies of src/corrections/mod.rs:193-235. parts[4 * n_mol] receives per molecule
+ * (D3, H4, H-H repulsion, X) in eV; gradients[3 * total atoms] (optional) the gradient of their sum
+ * in eV/Bohr. */
+int pm3gpu_corrections_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
+                             const double* xyz_bohr, int variant, double* parts, double* gradients);
+
 /* pm3gpu_batch with z / xyz_bohr / atom_offsets already resident in device memory
  * (device pointers); results, charges and gradients are host buffers as above. */
 int pm3gpu_batch_device_inputs(pm3gpu_ctx* ctx, int n_mol, const int32_t* d_atom_offsets,
@@ -312,9 +321,10 @@ int pm3gpu_last_launch_layout(pm3gpu_ctx* ctx, int* ctas_per_sm, int* smem_matri
 /* Molecules with at least `nao` basis functions are solved one at a time on the whole GPU
  * (grid-wide integral and Fock kernels, blocked eigensolver, the library's FP64 tensor-core GEMM for
  * the dense products) instead of one CTA each. Default and maximum 257: every molecule beyond one CTA's
- * 256 basis functions. Lower values send smaller molecules to that path too (one molecule at a
- * time, all SMs on it). Same run_pm3 semantics either way (no reference counterpart: the
- * reference has one CPU path). */
+ * 256 basis functions; by default a call with a single molecule also sends it there from 192 basis
+ * functions, where all SMs beat one CTA (setting a threshold replaces that rule). Lower values send
+ * smaller molecules to that path too (one molecule at a time, all SMs on it). Same run_pm3
+ * semantics either way (no reference counterpart: the reference has one CPU path). */
 int pm3gpu_set_large_threshold(pm3gpu_ctx* ctx, int nao);
 
 /* Autotuner (no counterpart in the reference). Measures, on the caller's sample of molecules

@@ -1724,8 +1724,8 @@ int oracle_single_point(int n_atoms, const int* z, const double* xyz_bohr, const
     set_err(errbuf, errlen, "multiplicity must be >= 1");
     return 1;
   }
-  if (O.variant != 0 && O.variant != 1) {
-    set_err(errbuf, errlen, "variant outside PM3 / PM3-D3");
+  if (O.variant < 0 || O.variant > 3) {
+    set_err(errbuf, errlen, "variant outside PM3 / PM3-D3 / PM3-D3H4 / PM3-D3H4X");
     return 1;
   }
   if (!build_molecule(n_atoms, z, xyz_bohr, m, err)) {
@@ -1823,9 +1823,13 @@ int oracle_single_point(int n_atoms, const int* z, const double* xyz_bohr, const
   double improvement = std::max(first_ev - state.electronic, 0.0);
   double core_ev = core_core_energy(m);
   double electronic = state.electronic;
-  // post-SCF classical correction of the method variant (scf.rs:740-743): D3 for PM3-D3
+  // post-SCF classical correction of the method variant (scf.rs:740-743)
   double correction_ev = 0.0;
-  if (O.variant == 1) oracle_d3(n_atoms, z, xyz_bohr, 1, &correction_ev, nullptr, nullptr);
+  if (O.variant != 0) {
+    double parts[4];
+    oracle_corrections(n_atoms, z, xyz_bohr, O.variant, parts, nullptr);
+    correction_ev = parts[0] + parts[1] + parts[2] + parts[3];
+  }
   double total = electronic + core_ev + correction_ev;
   double e_isol = 0.0, eheat = 0.0;
   for (int i = 0; i < m.natom; ++i) {
@@ -1907,10 +1911,10 @@ int oracle_single_point(int n_atoms, const int* z, const double* xyz_bohr, const
       Mat none;
       electronic_gradient(m, state.density, none, none, false, g);
     }
-    if (O.variant == 1) {  // add_correction_gradient (gradient.rs:324-357)
+    if (O.variant != 0) {  // add_correction_gradient (gradient.rs:324-357)
       std::vector<double> gd(g.size(), 0.0);
-      double ed = 0.0;
-      oracle_d3(n_atoms, z, xyz_bohr, 1, &ed, gd.data(), nullptr);
+      double parts[4];
+      oracle_corrections(n_atoms, z, xyz_bohr, O.variant, parts, gd.data());
       for (size_t k = 0; k < g.size(); ++k) g[k] += gd[k];
     }
     std::memcpy(gradient, g.data(), g.size() * sizeof(double));

@@ -18,7 +18,8 @@
 // d(f / r^n)/dr = f / r^(n+1) (alpha u f - n), and dC6/dcn follows from the quotient rule on the
 // weights. Every sum is in FP64 and runs in a fixed order, so the result is deterministic. The pair
 // loops touch each molecule's coordinates from L1; per atom the work is O(n) and the whole
-// correction is a few microseconds for the batches the SCF solves in milliseconds.
+// correction is a few microseconds for the batches the SCF solves in milliseconds. The host side
+// (buffers, launches, the variant's sum) is corrections.cuh.
 #pragma once
 #include "pm3_d3_table.h"
 
@@ -242,80 +243,4 @@ cudaError_t d3_ready(int device) {
   const cudaError_t e = cudaMemcpyToSymbol(d3k::g_tab, &host, sizeof(host));
   if (e == cudaSuccess) done[device] = 1;
   return e;
-}
-
-// D3 energies (eV) and gradients (eV/Bohr) of the molecules whose set[m] is 1 (PM3-D3 parameters)
-// or 2 (PM3-D3H4 parameters); dz / dxyz hold the batch's atoms on the device. energy[m] is written
-// for those molecules, grad (optional, 3 per atom) for their atoms. Synchronises the stream.
-int d3_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_set, const int32_t* dz,
-             const double* dxyz, double* energy, double* grad) {
-  const int total = h_offs[n_mol];
-  if (n_mol <= 0 || total <= 0) return PM3GPU_OK;
-  CUDA_TRY(c, d3_ready(c->device));
-  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const size_t o_offs = 0, o_set = up(4 * (size_t)(n_mol + 1)), o_cn = o_set + up(4 * (size_t)n_mol);
-  const size_t o_de = o_cn + up(8 * (size_t)total), o_e6 = o_de + up(8 * (size_t)total);
-  const size_t o_e8 = o_e6 + up(8 * (size_t)total), o_gd = o_e8 + up(8 * (size_t)total);
-  const size_t o_g = o_gd + up(24 * (size_t)total), o_en = o_g + up(24 * (size_t)total);
-  const size_t bytes = o_en + up(8 * (size_t)n_mol);
-  CUDA_TRY(c, c->d3buf.ensure(bytes));
-  char* base = c->d3buf.as<char>();
-  int32_t* d_offs = reinterpret_cast<int32_t*>(base + o_offs);
-  int32_t* d_set = reinterpret_cast<int32_t*>(base + o_set);
-  double* d_cn = reinterpret_cast<double*>(base + o_cn);
-  double* d_de = reinterpret_cast<double*>(base + o_de);
-  double* d_e6 = reinterpret_cast<double*>(base + o_e6);
-  double* d_e8 = reinterpret_cast<double*>(base + o_e8);
-  double* d_gd = reinterpret_cast<double*>(base + o_gd);
-  double* d_g = reinterpret_cast<double*>(base + o_g);
-  double* d_en = reinterpret_cast<double*>(base + o_en);
-  cudaStream_t s = c->stream;
-  CUDA_TRY(c, cudaMemcpyAsync(d_offs, h_offs, 4 * (size_t)(n_mol + 1), cudaMemcpyHostToDevice, s));
-  CUDA_TRY(c, cudaMemcpyAsync(d_set, h_set, 4 * (size_t)n_mol, cudaMemcpyHostToDevice, s));
-  const int tb = 128, nb = (total + tb - 1) / tb;
-  const int wg = grad ? 1 : 0;
-  d3k::cn_kernel<<<nb, tb, 0, s>>>(total, n_mol, d_offs, d_set, dz, dxyz, d_cn);
-  d3k::pair_kernel<<<nb, tb, 0, s>>>(total, n_mol, d_offs, d_set, dz, dxyz, d_cn, d_e6, d_e8, d_de, d_gd, wg);
-  if (grad) d3k::chain_kernel<<<nb, tb, 0, s>>>(total, n_mol, d_offs, d_set, dz, dxyz, d_de, d_gd, d_g);
-  d3k::energy_kernel<<<(n_mol + tb - 1) / tb, tb, 0, s>>>(n_mol, d_offs, d_set, d_e6, d_e8, d_en);
-  CUDA_TRY(c, cudaGetLastError());
-  c->launches += grad ? 4 : 3;
-  CUDA_TRY(c, cudaMemcpyAsync(energy, d_en, 8 * (size_t)n_mol, cudaMemcpyDeviceToHost, s));
-  if (grad) CUDA_TRY(c, cudaMemcpyAsync(grad, d_g, 24 * (size_t)total, cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(c, cudaStreamSynchronize(s));
-  return PM3GPU_OK;
-}
-
-// The post-SCF correction of each molecule's method variant (scf.rs:740-743, gradient.rs:240-262):
-// for PM3-D3 molecules that converged, the D3 energy joins total_ev and the heat of formation and
-// its gradient joins the SCF gradient.
-int apply_corrections(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_z, const pm3gpu_options* opts,
-                      int per_mol, const int32_t* dz, const double* dxyz, pm3gpu_result* results, double* gradients) {
-  std::vector<int32_t> set(n_mol, 0);
-  bool any = false;
-  for (int m = 0; m < n_mol; ++m) {
-    const pm3gpu_options* o = per_mol ? opts + m : opts;
-    if (results[m].status == PM3GPU_OK && o->variant == PM3GPU_VARIANT_D3 && h_offs[m + 1] > h_offs[m]) {
-      set[m] = 1;
-      any = true;
-    }
-  }
-  if (!any) return PM3GPU_OK;
-  std::vector<double> e(n_mol, 0.0), g(gradients ? 3 * (size_t)h_offs[n_mol] : 0, 0.0);
-  const int rc = d3_batch(c, n_mol, h_offs, set.data(), dz, dxyz, e.data(), gradients ? g.data() : nullptr);
-  if (rc != PM3GPU_OK) return rc;
-  for (int m = 0; m < n_mol; ++m) {
-    if (!set[m]) continue;
-    pm3gpu_result& R = results[m];
-    double e_isol = 0.0, eheat = 0.0;
-    for (int a = h_offs[m]; a < h_offs[m + 1]; ++a) {
-      e_isol += c->h_elem[h_z[a]].e_isol;
-      eheat += c->h_elem[h_z[a]].eheat_ev;
-    }
-    R.total_ev = R.electronic_ev + R.core_ev + e[m];
-    R.heat_of_formation_kcal = (R.total_ev - e_isol + eheat) * kEvToKcal;
-    if (gradients)
-      for (size_t k = 3 * (size_t)h_offs[m]; k < 3 * (size_t)h_offs[m + 1]; ++k) gradients[k] += g[k];
-  }
-  return PM3GPU_OK;
 }

@@ -109,7 +109,7 @@ EXPORTS = [
     "pm3gpu_set_stream", "pm3gpu_single_point", "pm3gpu_gradient", "pm3gpu_batch",
     "pm3gpu_batch_device_inputs", "pm3gpu_core_hamiltonian", "pm3gpu_fock", "pm3gpu_last_timings",
     "pm3gpu_last_kernel_launches", "pm3gpu_last_launch_layout", "pm3gpu_dgemm", "pm3gpu_default_opt_options",
-    "pm3gpu_optimize_batch", "pm3gpu_numerical_hessian_batch", "pm3gpu_d3_batch", "pm3gpu_last_transfer_bytes", "pm3gpu_last_phase_cycles",
+    "pm3gpu_optimize_batch", "pm3gpu_numerical_hessian_batch", "pm3gpu_d3_batch", "pm3gpu_corrections_batch", "pm3gpu_last_transfer_bytes", "pm3gpu_last_phase_cycles",
     "pm3gpu_single_point_noalloc", "pm3gpu_set_large_threshold", "pm3gpu_last_large_phase_ms",
     "pm3gpu_set_precision", "pm3gpu_last_large_trace", "pm3gpu_autotune", "pm3gpu_load_tuning",
     "pm3gpu_tuning_choice",
@@ -164,6 +164,7 @@ def load() -> ctypes.CDLL:
     L.pm3gpu_optimize_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, ctypes.POINTER(Options),
                                         ctypes.POINTER(OptOptions), ctypes.POINTER(OptResult), _D]
     L.pm3gpu_d3_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, ctypes.c_int, _D, _D]
+    L.pm3gpu_corrections_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, ctypes.c_int, _D, _D]
     L.pm3gpu_numerical_hessian_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _D, ctypes.POINTER(Options),
                                                  ctypes.c_double, _D, _I]
     L.pm3gpu_dgemm.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,

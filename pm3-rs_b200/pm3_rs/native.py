@@ -2,10 +2,11 @@
 
 Drop-in for ``pm3_rs.native`` of pm3-rs (python/pm3_rs/native.py:41-140 and
 src/python.rs:253-357): same functions, signatures, dictionary keys and units, and the same
-``ValueError`` on any failure (src/python.rs:22-24). ``method`` is ``"pm3"`` or ``"pm3-d3"`` (the
-D3 dispersion correction, added to the energy, heat of formation and gradient) and ``field`` is
-``None``: the H4 and X corrections and external fields are outside this library's path, and asking
-for them raises rather than being silently ignored.
+``ValueError`` on any failure (src/python.rs:22-24). ``method`` is one of ``"pm3"``, ``"pm3-d3"``,
+``"pm3-d3h4"`` and ``"pm3-d3h4x"`` (the post-SCF corrections of src/corrections/, added to the
+energy, heat of formation and gradient) and ``field`` is ``None``: external fields and the MMOK
+amide term are outside this library's path, and asking for them raises rather than being silently
+ignored.
 """
 from __future__ import annotations
 
@@ -32,16 +33,16 @@ def _parse_reference(reference: str) -> int:
 
 
 # corrections::Variant::parse (src/corrections/mod.rs:180-191) -> PM3GPU_VARIANT_*
-_VARIANTS = {"pm3": 0, "pm3-d3": 1, "pm3-d3h4": 2, "pm3-d3h4x": 3}
+_VARIANTS = {"": 0, "pm3": 0, "pm3-d3": 1, "pm3-d3h4": 2, "pm3-d3h4x": 3}
 
 
 def _check_method(method: str, field) -> int:
-    """The method string's variant code; PM3 and PM3-D3 run here, the H4 family raises."""
+    """The method string's variant code (PM3GPU_VARIANT_*), parsed as src/python.rs:48-65 does."""
     m = str(method).strip().lower().replace(" ", "-").replace("_", "-")
+    if m.endswith("+mmok"):
+        raise ValueError(f"method {method!r}: the MMOK amide correction is not available on pm3gpu")
     if m not in _VARIANTS:
         raise ValueError(f"unknown method {method!r}: expected PM3, PM3-D3, PM3-D3H4 or PM3-D3H4X")
-    if _VARIANTS[m] > 1:
-        raise ValueError(f"method {method!r} is not available here: 'pm3' and 'pm3-d3' run on pm3gpu")
     if field is not None:
         raise ValueError("an external field is not available on pm3gpu")
     return _VARIANTS[m]
@@ -385,6 +386,33 @@ def d3_batch(offsets, z, xyz_bohr, d3_set: int = 1, want_gradient: bool = True, 
     if rc != 0:
         raise ValueError(ctx.last_error() or f"pm3gpu status {rc}")
     out = {"energy_ev": e[:n_mol].copy()}
+    if g is not None:
+        out["gradient"] = g
+    return out
+
+
+def corrections_batch(offsets, z, xyz_bohr, method: str = "pm3-d3h4", want_gradient: bool = True, device: int = 0,
+                      context: _lib.Context | None = None) -> dict:
+    """The post-SCF correction of a method variant alone (pm3gpu_corrections_batch; the
+    CorrectionEnergies of src/corrections/mod.rs:193-235) for many molecules: ``d3_ev``, ``h4_ev``,
+    ``hh_ev``, ``hx_ev`` and ``total_ev`` per molecule, ``gradient`` (eV/Bohr) of the total."""
+    variant = _check_method(method, None)
+    if variant == 0:
+        raise ValueError("plain PM3 has no correction")
+    ctx = context if context is not None else _lib.default_context(device)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+    z = np.ascontiguousarray(z, dtype=np.int32)
+    x = np.ascontiguousarray(np.asarray(xyz_bohr, dtype=np.float64).reshape(-1, 3))
+    n_mol = len(offsets) - 1
+    parts = np.zeros((max(n_mol, 1), 4))
+    g = np.zeros_like(x) if want_gradient else None
+    rc = ctx.lib.pm3gpu_corrections_batch(ctx.ptr, n_mol, _ip(offsets), _ip(z), _dp(x), variant, _dp(parts),
+                                          _dp(g) if g is not None else None)
+    if rc != 0:
+        raise ValueError(ctx.last_error() or f"pm3gpu status {rc}")
+    p = parts[:n_mol]
+    out = {"d3_ev": p[:, 0].copy(), "h4_ev": p[:, 1].copy(), "hh_ev": p[:, 2].copy(), "hx_ev": p[:, 3].copy(),
+           "total_ev": p[:, 0] + p[:, 1] + p[:, 2] + p[:, 3]}
     if g is not None:
         out["gradient"] = g
     return out

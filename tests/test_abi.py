@@ -54,13 +54,14 @@ def test_supported_elements_and_basis_size():
 
 def test_struct_layouts_match_header():
     assert ctypes.sizeof(_lib.Options) == 8 + 4 + 4 + 8 + 8 + 4 + 4 + 8 + 4 * 4 + 8 + 8 + 8
+    assert _lib.Options.scf_memory_mb.offset == 80 and _lib.Options.variant.offset == 84
     # pm3gpu_result: 4 ints, 4 doubles, 3+1 doubles, 2 doubles, 2 ints, 4 ints, 1 double, 1 double
     assert ctypes.sizeof(_lib.Result) == 16 + 32 + 32 + 16 + 8 + 16 + 16
 
 
 def test_unsupported_method_and_field_raise_before_any_gpu_work():
     with pytest.raises(ValueError):
-        native.single_point([8, 1, 1], np.zeros((3, 3)), method="pm3-d3h4")
+        native.single_point([8, 1, 1], np.zeros((3, 3)), method="am1")
     with pytest.raises(ValueError):
         native.single_point([8, 1, 1], np.zeros((3, 3)), field=[0.0, 0.0, 0.01])
     with pytest.raises(ValueError):

@@ -1,4 +1,4 @@
-"""The CPU restatement of the reference's D3 dispersion (oracle/d3_oracle.cpp, the checker of the GPU
+"""The CPU restatement of the reference's D3 dispersion (oracle/corrections_oracle.cpp, the checker of the GPU
 library's D3 kernels) pinned to the reference's own D3 tests (src/corrections/d3.rs:462-539): the
 CN-interpolated C6 of H-H and O-O at isolated and bonded coordination numbers, the water-dimer
 coordination numbers, attractive dispersion and the size of methane's D3H4 dispersion; plus the
@@ -71,11 +71,15 @@ def test_pm3_d3_single_point_adds_the_dispersion_energy_and_gradient():
 
 
 def test_method_strings_parse_like_the_reference():
+    """corrections::Variant::parse (src/corrections/mod.rs:180-191, tests/api_surface.rs:224-240)."""
     assert native._check_method("pm3", None) == 0
     assert native._check_method("PM3-D3", None) == 1
     assert native._check_method("pm3_d3", None) == 1
-    for m in ("pm3-d3h4", "PM3 D3H4X"):
+    assert native._check_method("pm3-d3h4", None) == 2
+    assert native._check_method("PM3 D3H4X", None) == 3
+    assert native._check_method(" ", None) == 0
+    for bad in ("am1", "pm3-d3h4+mmok"):
         with pytest.raises(ValueError):
-            native._check_method(m, None)
+            native._check_method(bad, None)
     with pytest.raises(ValueError):
-        native._check_method("am1", None)
+        native._check_method("pm3", [0.0, 0.0, 0.01])

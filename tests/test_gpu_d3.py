@@ -1,6 +1,6 @@
 """The D3 dispersion correction on the device (pm3gpu_d3_batch and the PM3-D3 variant of the single
 point, batch and gradient) against the CPU restatement of the reference's d3.rs
-(oracle/d3_oracle.cpp), whose gradient comes from dual numbers rather than the kernels' analytic
+(oracle/corrections_oracle.cpp), whose gradient comes from dual numbers rather than the kernels' analytic
 derivatives.
 
 Bars: D3 energies within 1e-12 eV and gradients within 1e-12 eV/Bohr of the oracle (FP64 on both
@@ -97,8 +97,6 @@ def test_variants_mix_in_one_batch_and_through_the_python_api():
     assert d3 < plain
     e, _, _ = O.d3(zd, xd * A2B, 1)
     assert d3 - plain == pytest.approx(e, abs=1e-9)
-    with pytest.raises(ValueError):
-        native.single_point(zd, xd, method="pm3-d3h4")
 
 
 def test_pm3_d3_on_the_whole_gpu_path_matches_oracle():
