@@ -83,6 +83,8 @@ typedef struct {
   double damping;         /* 0 */
   int scf_memory_mb;      /* 512: accelerator-history budget (sets the DIIS depth) */
   int variant;            /* PM3GPU_VARIANT_* (Pm3Options::variant, src/scf.rs:184): 0 plain PM3 */
+  int mmok;               /* 0; 1 adds MOPAC's MMOK amide torsion term (Pm3Options::mmok, src/scf.rs:193,
+                             src/corrections/mmok.rs) on top of the variant's correction */
 } pm3gpu_options;
 
 /* Pm3Result scalar fields (src/scf.rs:353-396). Arrays are returned through caller buffers. */

@@ -394,18 +394,90 @@ S hx_energy(int n, const int* z, const S* pos) {
   return sum * S(kKcalToEv);
 }
 
+// ---------------------------------------------------------------- MMOK amide term (mmok.rs)
+constexpr double kAmideKEv = 7.185300 / 23.06054783061903;  // AMIDE_K_KCAL / EV_TO_KCAL (mmok.rs:39-42)
+
+// sin^2 of the p0-p1-p2-p3 torsion, polynomial form (mmok.rs:64-89)
+template <class S>
+S sin2_torsion(const S* p0, const S* p1, const S* p2, const S* p3) {
+  S b1[3], b2[3], b3[3], n1[3], n2[3], m[3];
+  for (int k = 0; k < 3; ++k) {
+    b1[k] = p1[k] - p0[k];
+    b2[k] = p2[k] - p1[k];
+    b3[k] = p3[k] - p2[k];
+  }
+  auto cross = [](const S* a, const S* b, S* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  auto dot = [](const S* a, const S* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+  cross(b1, b2, n1);
+  cross(b2, b3, n2);
+  cross(n1, n2, m);
+  const S num = s_powi(dot(m, b2), 2);
+  const S den = dot(n1, n1) * dot(n2, n2) * dot(b2, b2);
+  if (val(den) <= 1.0e-30) return S(0.0);
+  return num / den;
+}
+
+// amide_torsions (mmok.rs:97-125): (O, C, N, H) with C-N < 1.65, C=O < 1.35, N-H < 1.30 Angstrom
+void amide_torsions(int n, const int* z, const double* pos, std::vector<int>& out) {
+  auto bonded = [&](int i, int j, double mx) {
+    double d2 = 0.0;
+    for (int k = 0; k < 3; ++k) d2 += (pos[3 * i + k] - pos[3 * j + k]) * (pos[3 * i + k] - pos[3 * j + k]);
+    return d2 < mx * mx;
+  };
+  const double co = 1.35 / kA0, cn = 1.65 / kA0, nh = 1.30 / kA0;
+  out.clear();
+  for (int ni = 0; ni < n; ++ni) {
+    if (z[ni] != 7) continue;
+    for (int ci = 0; ci < n; ++ci) {
+      if (z[ci] != 6 || !bonded(ni, ci, cn)) continue;
+      for (int oi = 0; oi < n; ++oi) {
+        if (z[oi] != 8 || !bonded(ci, oi, co)) continue;
+        for (int hi = 0; hi < n; ++hi)
+          if (z[hi] == 1 && bonded(ni, hi, nh)) {
+            out.push_back(oi);
+            out.push_back(ci);
+            out.push_back(ni);
+            out.push_back(hi);
+          }
+      }
+    }
+  }
+}
+
+// amide_correction_g (mmok.rs:132-143): topology from the coordinate values
+template <class S>
+S mmok_energy(int n, const int* z, const S* pos) {
+  std::vector<double> v(3 * (size_t)n);
+  for (size_t k = 0; k < v.size(); ++k) v[k] = val(pos[k]);
+  std::vector<int> q;
+  amide_torsions(n, z, v.data(), q);
+  S e(0.0);
+  for (size_t t = 0; t < q.size(); t += 4)
+    e = e + sin2_torsion(pos + 3 * q[t], pos + 3 * q[t + 1], pos + 3 * q[t + 2], pos + 3 * q[t + 3]) * S(kAmideKEv);
+  return e;
+}
+
 // correction_energy_cluster_g (mod.rs:129-160) for a molecule: variant 1 = PM3-D3, 2 = PM3-D3H4,
 // 3 = PM3-D3H4X; parts[4] = (d3, h4, hh, hx)
+// correction_energy_with_mmok_g (mod.rs:78-91): variant 0 has no variant term; parts[5] =
+// (d3, h4, hh, hx, mmok)
 template <class S>
-S correction(int n, const int* z, const int* e, const S* pos, int variant, S* parts) {
-  for (int k = 0; k < 4; ++k) parts[k] = S(0.0);
-  parts[0] = energy(n, e, pos, params_of(variant == 1 ? 1 : 2));
+S correction(int n, const int* z, const int* e, const S* pos, int variant, int mmok, S* parts) {
+  for (int k = 0; k < 5; ++k) parts[k] = S(0.0);
+  if (variant >= 1) parts[0] = energy(n, e, pos, params_of(variant == 1 ? 1 : 2));
   if (variant >= 2) {
     parts[1] = h4_energy(n, z, pos);
     parts[2] = hh_energy(n, z, pos);
   }
   if (variant == 3) parts[3] = hx_energy(n, z, pos);
-  return parts[0] + parts[1] + parts[2] + parts[3];
+  const S base = parts[0] + parts[1] + parts[2] + parts[3];
+  if (!mmok) return base;
+  parts[4] = mmok_energy(n, z, pos);
+  return base + parts[4];
 }
 
 void elements(int n, const int* z, std::vector<int>& e) {
@@ -442,21 +514,21 @@ int oracle_d3(int n_atoms, const int* z, const double* xyz_bohr, int variant, do
   return 0;
 }
 
-int oracle_corrections(int n_atoms, const int* z, const double* xyz_bohr, int variant, double* parts_ev,
+int oracle_corrections(int n_atoms, const int* z, const double* xyz_bohr, int variant, int mmok, double* parts_ev,
                        double* gradient) {
-  if (n_atoms < 0 || (n_atoms > 0 && (!z || !xyz_bohr)) || !parts_ev || variant < 1 || variant > 3) return 1;
+  if (n_atoms < 0 || (n_atoms > 0 && (!z || !xyz_bohr)) || !parts_ev || variant < 0 || variant > 3) return 1;
   std::vector<int> e;
   elements(n_atoms, z, e);
-  double parts[4];
-  correction<double>(n_atoms, z, e.data(), xyz_bohr, variant, parts);
-  for (int k = 0; k < 4; ++k) parts_ev[k] = parts[k];
+  double parts[5];
+  correction<double>(n_atoms, z, e.data(), xyz_bohr, variant, mmok, parts);
+  for (int k = 0; k < 5; ++k) parts_ev[k] = parts[k];
   if (gradient) {
     std::vector<Dual> pos(3 * (size_t)n_atoms);
-    Dual dp[4];
+    Dual dp[5];
     for (int a = 0; a < n_atoms; ++a) {
       for (int k = 0; k < 3 * n_atoms; ++k) pos[k] = Dual(xyz_bohr[k]);
       for (int k = 0; k < 3; ++k) pos[3 * a + k].d[k] = 1.0;
-      const Dual ed = correction<Dual>(n_atoms, z, e.data(), pos.data(), variant, dp);
+      const Dual ed = correction<Dual>(n_atoms, z, e.data(), pos.data(), variant, mmok, dp);
       for (int k = 0; k < 3; ++k) gradient[3 * a + k] = ed.d[k];
     }
   }

@@ -39,6 +39,7 @@ class Options(ctypes.Structure):
         ("damping", ctypes.c_double),
         ("scf_memory_mb", ctypes.c_int),
         ("variant", ctypes.c_int),
+        ("mmok", ctypes.c_int),
     ]
 
 
@@ -106,7 +107,7 @@ def lib():
     L.oracle_reset_parameters.argtypes = []
     L.oracle_reset_parameters.restype = None
     L.oracle_d3.argtypes = [ctypes.c_int, _I, _D, ctypes.c_int, _D, _D, _D]
-    L.oracle_corrections.argtypes = [ctypes.c_int, _I, _D, ctypes.c_int, _D, _D]
+    L.oracle_corrections.argtypes = [ctypes.c_int, _I, _D, ctypes.c_int, ctypes.c_int, _D, _D]
     L.oracle_d3_c6.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]
     L.oracle_d3_c6.restype = ctypes.c_double
     try:
@@ -310,15 +311,17 @@ def d3_c6(zi, zj, cni, cnj) -> float:
     return lib().oracle_d3_c6(int(zi), int(zj), float(cni), float(cnj))
 
 
-def corrections(z, xyz_bohr, variant, want_gradient=True):
-    """The post-SCF correction of a method variant (1 PM3-D3, 2 PM3-D3H4, 3 PM3-D3H4X;
-    src/corrections/mod.rs:129-160): (dict of the D3 / H4 / H-H / X parts in eV, gradient of their
-    sum in eV/Bohr [n, 3] or None)."""
+def corrections(z, xyz_bohr, variant, want_gradient=True, mmok=False):
+    """The post-SCF correction of a method variant (0 none, 1 PM3-D3, 2 PM3-D3H4, 3 PM3-D3H4X;
+    src/corrections/mod.rs:78-160), with the MMOK amide term when ``mmok``: (dict of the D3 / H4 /
+    H-H / X parts, plus "mmok" when asked for, in eV; gradient of their sum in eV/Bohr [n, 3] or
+    None)."""
     z = np.ascontiguousarray(z, dtype=np.int32)
     xyz = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1, 3)
-    parts = np.zeros(4)
+    parts = np.zeros(5)
     g = np.zeros((len(z), 3)) if want_gradient else None
-    code = lib().oracle_corrections(len(z), _ip(z), _dp(xyz), int(variant), _dp(parts), _dp(g))
+    code = lib().oracle_corrections(len(z), _ip(z), _dp(xyz), int(variant), int(bool(mmok)), _dp(parts), _dp(g))
     if code != 0:
         raise OracleError(code, "corrections")
-    return dict(zip(("d3", "h4", "hh", "hx"), parts.tolist())), g
+    names = ("d3", "h4", "hh", "hx", "mmok") if mmok else ("d3", "h4", "hh", "hx")
+    return dict(zip(names, parts.tolist())), g

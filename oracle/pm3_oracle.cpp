@@ -1571,6 +1571,7 @@ void oracle_default_options(oracle_options* o) {  // scf.rs:259-287
   o->damping = 0.0;
   o->scf_memory_mb = 512;
   o->variant = 0;
+  o->mmok = 0;
 }
 
 void oracle_set_lapack(void* dsyevd, void* dgemm) {
@@ -1825,10 +1826,11 @@ int oracle_single_point(int n_atoms, const int* z, const double* xyz_bohr, const
   double electronic = state.electronic;
   // post-SCF classical correction of the method variant (scf.rs:740-743)
   double correction_ev = 0.0;
-  if (O.variant != 0) {
-    double parts[4];
-    oracle_corrections(n_atoms, z, xyz_bohr, O.variant, parts, nullptr);
+  if (O.variant != 0 || O.mmok) {
+    double parts[5];
+    oracle_corrections(n_atoms, z, xyz_bohr, O.variant, O.mmok, parts, nullptr);
     correction_ev = parts[0] + parts[1] + parts[2] + parts[3];
+    if (O.mmok) correction_ev += parts[4];
   }
   double total = electronic + core_ev + correction_ev;
   double e_isol = 0.0, eheat = 0.0;
@@ -1911,10 +1913,10 @@ int oracle_single_point(int n_atoms, const int* z, const double* xyz_bohr, const
       Mat none;
       electronic_gradient(m, state.density, none, none, false, g);
     }
-    if (O.variant != 0) {  // add_correction_gradient (gradient.rs:324-357)
+    if (O.variant != 0 || O.mmok) {  // add_correction_gradient (gradient.rs:324-357)
       std::vector<double> gd(g.size(), 0.0);
-      double parts[4];
-      oracle_corrections(n_atoms, z, xyz_bohr, O.variant, parts, gd.data());
+      double parts[5];
+      oracle_corrections(n_atoms, z, xyz_bohr, O.variant, O.mmok, parts, gd.data());
       for (size_t k = 0; k < g.size(); ++k) g[k] += gd[k];
     }
     std::memcpy(gradient, g.data(), g.size() * sizeof(double));

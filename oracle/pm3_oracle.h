@@ -30,6 +30,7 @@ typedef struct {
   double damping;
   int scf_memory_mb;
   int variant;       /* 0 PM3, 1 PM3-D3, 2 PM3-D3H4, 3 PM3-D3H4X (corrections::Variant, src/corrections/mod.rs:165-178) */
+  int mmok;          /* MOPAC's amide torsion term (Pm3Options::mmok, src/scf.rs:193) */
 } oracle_options;
 
 typedef struct {
@@ -56,10 +57,10 @@ int oracle_nao(int n_atoms, const int* z);
  * dual numbers as src/gradient.rs:324-357) and cn[n] (coordination numbers) are optional. */
 int oracle_d3(int n_atoms, const int* z, const double* xyz_bohr, int d3_set, double* energy_ev, double* gradient,
               double* cn);
-/* The post-SCF correction of a method variant (1 PM3-D3, 2 PM3-D3H4, 3 PM3-D3H4X;
- * src/corrections/mod.rs:129-160): parts_ev[4] = (D3, H4, H-H repulsion, X) in eV; gradient[3n]
- * (optional) of their sum in eV/Bohr, by dual numbers. */
-int oracle_corrections(int n_atoms, const int* z, const double* xyz_bohr, int variant, double* parts_ev,
+/* The post-SCF correction of a method variant (0 none, 1 PM3-D3, 2 PM3-D3H4, 3 PM3-D3H4X;
+ * src/corrections/mod.rs:78-160) with the MMOK amide term when mmok is set: parts_ev[5] = (D3, H4,
+ * H-H repulsion, X, MMOK) in eV; gradient[3n] (optional) of their sum in eV/Bohr, by dual numbers. */
+int oracle_corrections(int n_atoms, const int* z, const double* xyz_bohr, int variant, int mmok, double* parts_ev,
                        double* gradient);
 /* getc6 (d3.rs:212-236) for one element pair at the given coordination numbers. */
 double oracle_d3_c6(int zi, int zj, double cni, double cnj);

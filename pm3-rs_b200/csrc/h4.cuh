@@ -356,3 +356,113 @@ __global__ void __launch_bounds__(kThreads) h4_kernel(const int32_t* __restrict_
 }
 
 }  // namespace h4k
+
+// MOPAC's MMOK amide term (pm3-rs src/corrections/mmok.rs:97-143): for every (O, C, N, H) with
+// C-N < 1.65, C=O < 1.35 and N-H < 1.30 Angstrom, AMIDE_K sin^2 of the O-C-N-H torsion, in the
+// reference's polynomial form ((n1 x n2) . b2)^2 / (|n1|^2 |n2|^2 |b2|^2), zero where that
+// denominator is at most 1e-30. The gradient comes from forward-mode dual numbers carrying the 12
+// coordinates of the quadruple, one evaluation per term.
+namespace mmk {
+
+constexpr double kAmideK = 7.185300 / 23.06054783061903;  // eV
+
+struct D12 {
+  double v, d[12];
+};
+__device__ __forceinline__ D12 dsub(const D12& a, const D12& b) {
+  D12 r;
+  r.v = a.v - b.v;
+#pragma unroll
+  for (int k = 0; k < 12; ++k) r.d[k] = a.d[k] - b.d[k];
+  return r;
+}
+__device__ __forceinline__ D12 dadd(const D12& a, const D12& b) {
+  D12 r;
+  r.v = a.v + b.v;
+#pragma unroll
+  for (int k = 0; k < 12; ++k) r.d[k] = a.d[k] + b.d[k];
+  return r;
+}
+__device__ __forceinline__ D12 dmul(const D12& a, const D12& b) {
+  D12 r;
+  r.v = a.v * b.v;
+#pragma unroll
+  for (int k = 0; k < 12; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+  return r;
+}
+
+__device__ inline void sin2_torsion(const double* xyz, const int* at, double& s, double* g) {
+  D12 p[4][3];
+  for (int a = 0; a < 4; ++a)
+    for (int c = 0; c < 3; ++c) {
+      p[a][c].v = xyz[3 * at[a] + c];
+#pragma unroll
+      for (int k = 0; k < 12; ++k) p[a][c].d[k] = (k == 3 * a + c) ? 1.0 : 0.0;
+    }
+  D12 b1[3], b2[3], b3[3], n1[3], n2[3], m[3];
+  for (int c = 0; c < 3; ++c) {
+    b1[c] = dsub(p[1][c], p[0][c]);
+    b2[c] = dsub(p[2][c], p[1][c]);
+    b3[c] = dsub(p[3][c], p[2][c]);
+  }
+  auto cross = [](const D12* a, const D12* b, D12* o) {
+    o[0] = dsub(dmul(a[1], b[2]), dmul(a[2], b[1]));
+    o[1] = dsub(dmul(a[2], b[0]), dmul(a[0], b[2]));
+    o[2] = dsub(dmul(a[0], b[1]), dmul(a[1], b[0]));
+  };
+  auto dot = [](const D12* a, const D12* b) { return dadd(dadd(dmul(a[0], b[0]), dmul(a[1], b[1])), dmul(a[2], b[2])); };
+  cross(b1, b2, n1);
+  cross(b2, b3, n2);
+  cross(n1, n2, m);
+  const D12 t = dot(m, b2);
+  const D12 num = dmul(t, t);
+  const D12 den = dmul(dmul(dot(n1, n1), dot(n2, n2)), dot(b2, b2));
+  if (den.v <= 1.0e-30) {
+    s = 0.0;
+    for (int k = 0; k < 12; ++k) g[k] = 0.0;
+    return;
+  }
+  s = num.v / den.v;
+  for (int k = 0; k < 12; ++k) g[k] = (num.d[k] * den.v - num.v * den.d[k]) / (den.v * den.v);
+}
+
+__device__ __forceinline__ bool bonded(const double* xyz, int i, int j, double mx) {
+  double d2 = 0.0;
+  for (int k = 0; k < 3; ++k) d2 += (xyz[3 * i + k] - xyz[3 * j + k]) * (xyz[3 * i + k] - xyz[3 * j + k]);
+  return d2 < mx * mx;
+}
+
+// grid: one CTA per entry of mols; energy[m] (eV) written, grad[3 atom] accumulated (zeroed first)
+__global__ void __launch_bounds__(128) mmok_kernel(const int32_t* __restrict__ mols, const int32_t* __restrict__ offs,
+                                                   const int32_t* __restrict__ z, const double* __restrict__ xyz,
+                                                   double* __restrict__ energy, double* __restrict__ grad) {
+  __shared__ double red[4];
+  const int m = mols[blockIdx.x];
+  const int a0 = offs[m], a1 = offs[m + 1];
+  const double co = 1.35 / h4k::kA0, cn = 1.65 / h4k::kA0, nh = 1.30 / h4k::kA0;
+  double e = 0.0;
+  for (int ni = a0 + threadIdx.x; ni < a1; ni += blockDim.x) {
+    if (z[ni] != 7) continue;
+    for (int ci = a0; ci < a1; ++ci) {
+      if (z[ci] != 6 || !bonded(xyz, ni, ci, cn)) continue;
+      for (int oi = a0; oi < a1; ++oi) {
+        if (z[oi] != 8 || !bonded(xyz, ci, oi, co)) continue;
+        for (int hi = a0; hi < a1; ++hi) {
+          if (z[hi] != 1 || !bonded(xyz, ni, hi, nh)) continue;
+          const int at[4] = {oi, ci, ni, hi};
+          double s, g[12];
+          sin2_torsion(xyz, at, s, g);
+          e = e + s * kAmideK;
+          for (int a = 0; a < 4; ++a)
+            for (int c = 0; c < 3; ++c) atomicAdd(&grad[3 * at[a] + c], g[3 * a + c] * kAmideK);
+        }
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) energy[m] = red[0] + red[1] + red[2] + red[3];
+}
+
+}  // namespace mmk

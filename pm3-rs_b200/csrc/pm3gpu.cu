@@ -1378,6 +1378,7 @@ void pm3gpu_default_options(pm3gpu_options* o) {  // scf.rs:259-287
   o->damping = 0.0;
   o->scf_memory_mb = 512;
   o->variant = PM3GPU_VARIANT_PM3;
+  o->mmok = 0;
 }
 
 int pm3gpu_supported_element(int z) { return supported(z) ? 1 : 0; }
@@ -1650,10 +1651,10 @@ int pm3gpu_d3_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t
   CUDA_TRY(c, cudaMemcpyAsync(c->z.p, z, 4 * (size_t)total, cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaMemcpyAsync(c->xyz.p, xyz, 24 * (size_t)total, cudaMemcpyHostToDevice, c->stream));
   std::vector<int32_t> set(n_mol, d3_set), var(n_mol, 0);
-  std::vector<double> parts(4 * (size_t)n_mol, 0.0);
-  const int rc = corrections_batch(c, n_mol, offs, set.data(), var.data(), c->z.as<int32_t>(), c->xyz.as<double>(),
-                                   parts.data(), gradients);
-  for (int m = 0; m < n_mol; ++m) energies[m] = parts[4 * (size_t)m];
+  std::vector<double> parts(5 * (size_t)n_mol, 0.0);
+  const int rc = corrections_batch(c, n_mol, offs, set.data(), var.data(), nullptr, c->z.as<int32_t>(),
+                                   c->xyz.as<double>(), parts.data(), gradients);
+  for (int m = 0; m < n_mol; ++m) energies[m] = parts[5 * (size_t)m];
   return rc;
 }
 
@@ -1680,8 +1681,12 @@ int pm3gpu_corrections_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, cons
   CUDA_TRY(c, cudaMemcpyAsync(c->z.p, z, 4 * (size_t)total, cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaMemcpyAsync(c->xyz.p, xyz, 24 * (size_t)total, cudaMemcpyHostToDevice, c->stream));
   std::vector<int32_t> set(n_mol, variant == PM3GPU_VARIANT_D3 ? 1 : 2), var(n_mol, variant);
-  return corrections_batch(c, n_mol, offs, set.data(), var.data(), c->z.as<int32_t>(), c->xyz.as<double>(), parts,
-                           gradients);
+  std::vector<double> p5(5 * (size_t)n_mol, 0.0);
+  const int rc = corrections_batch(c, n_mol, offs, set.data(), var.data(), nullptr, c->z.as<int32_t>(),
+                                   c->xyz.as<double>(), p5.data(), gradients);
+  for (int m = 0; m < n_mol; ++m)
+    for (int k = 0; k < 4; ++k) parts[4 * (size_t)m + k] = p5[5 * (size_t)m + k];
+  return rc;
 }
 
 int pm3gpu_numerical_hessian_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t* z,
@@ -2289,7 +2294,7 @@ int noalloc_run(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz,
     return fail(c, PM3GPU_INVALID_INPUT, "atom count outside 1..256 for the allocation-free path");
   if (o->guess == PM3GPU_GUESS_LEARNED)
     return fail(c, PM3GPU_INVALID_INPUT, "the learned guess is not available on the allocation-free path");
-  if (o->variant != PM3GPU_VARIANT_PM3)
+  if (o->variant != PM3GPU_VARIANT_PM3 || o->mmok)
     return fail(c, PM3GPU_INVALID_INPUT, "post-SCF corrections are not available on the allocation-free path");
   MolPlan p;
   plan_molecule(c, z, xyz, n_atoms, o, p);

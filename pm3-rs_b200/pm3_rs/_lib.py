@@ -40,6 +40,7 @@ class Options(ctypes.Structure):
         ("damping", ctypes.c_double),
         ("scf_memory_mb", ctypes.c_int),
         ("variant", ctypes.c_int),
+        ("mmok", ctypes.c_int),
     ]
 
 

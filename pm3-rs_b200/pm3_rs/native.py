@@ -3,10 +3,10 @@
 Drop-in for ``pm3_rs.native`` of pm3-rs (python/pm3_rs/native.py:41-140 and
 src/python.rs:253-357): same functions, signatures, dictionary keys and units, and the same
 ``ValueError`` on any failure (src/python.rs:22-24). ``method`` is one of ``"pm3"``, ``"pm3-d3"``,
-``"pm3-d3h4"`` and ``"pm3-d3h4x"`` (the post-SCF corrections of src/corrections/, added to the
-energy, heat of formation and gradient) and ``field`` is ``None``: external fields and the MMOK
-amide term are outside this library's path, and asking for them raises rather than being silently
-ignored.
+``"pm3-d3h4"`` and ``"pm3-d3h4x"``, each optionally with ``"+mmok"`` (the post-SCF corrections of
+src/corrections/, added to the energy, heat of formation and gradient) and ``field`` is ``None``:
+external fields are outside this library's path, and asking for one raises rather than being
+silently ignored.
 """
 from __future__ import annotations
 
@@ -36,16 +36,19 @@ def _parse_reference(reference: str) -> int:
 _VARIANTS = {"": 0, "pm3": 0, "pm3-d3": 1, "pm3-d3h4": 2, "pm3-d3h4x": 3}
 
 
-def _check_method(method: str, field) -> int:
-    """The method string's variant code (PM3GPU_VARIANT_*), parsed as src/python.rs:48-65 does."""
+def _check_method(method: str, field) -> dict:
+    """The method string as option fields, parsed as src/python.rs:48-65 does: ``variant``
+    (PM3GPU_VARIANT_*) and ``mmok`` (a ``+mmok`` suffix: MOPAC's amide term)."""
     m = str(method).strip().lower().replace(" ", "-").replace("_", "-")
-    if m.endswith("+mmok"):
-        raise ValueError(f"method {method!r}: the MMOK amide correction is not available on pm3gpu")
+    mmok = m.endswith("+mmok")
+    if mmok:
+        m = m[:-len("+mmok")]
     if m not in _VARIANTS:
-        raise ValueError(f"unknown method {method!r}: expected PM3, PM3-D3, PM3-D3H4 or PM3-D3H4X")
+        raise ValueError(f"method must be 'pm3', 'pm3-d3', 'pm3-d3h4' or 'pm3-d3h4x', each optionally with a "
+                         f"'+mmok' suffix (got {method!r})")
     if field is not None:
         raise ValueError("an external field is not available on pm3gpu")
-    return _VARIANTS[m]
+    return {"variant": _VARIANTS[m], "mmok": int(mmok)}
 
 
 def _as_arrays(numbers, positions):
@@ -127,9 +130,9 @@ def single_point(numbers: Sequence[int], positions, charge: float = 0.0, multipl
     ``electronic_ev``, ``core_ev``, ``charges`` (Mulliken, e), ``dipole_debye`` ([x, y, z]),
     ``homo_ev``, ``lumo_ev``, ``converged`` and ``unrestricted``.
     """
-    variant = _check_method(method, field)
+    mo = _check_method(method, field)
     z, xyz = _as_arrays(numbers, positions)
-    r = run(z, xyz, options(charge, multiplicity, reference, variant=variant))
+    r = run(z, xyz, options(charge, multiplicity, reference, **mo))
     return {
         "energy_hartree": r["total_ev"] * EV_TO_HARTREE,
         "energy_ev": r["total_ev"],
@@ -148,9 +151,9 @@ def single_point(numbers: Sequence[int], positions, charge: float = 0.0, multipl
 def gradient(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
              reference: str = "auto", method: str = "pm3", field=None) -> dict:
     """Energy and analytic gradient dE/dR (src/python.rs:299-357): Hartree/Bohr and eV/Angstrom."""
-    variant = _check_method(method, field)
+    mo = _check_method(method, field)
     z, xyz = _as_arrays(numbers, positions)
-    r = run(z, xyz, options(charge, multiplicity, reference, variant=variant), want_gradient=True)
+    r = run(z, xyz, options(charge, multiplicity, reference, **mo), want_gradient=True)
     g = r["gradient"]
     return {
         "energy_hartree": r["total_ev"] * EV_TO_HARTREE,
@@ -267,10 +270,10 @@ def optimize(numbers: Sequence[int], positions, charge: float = 0.0, multiplicit
     eV/Angstrom (None keeps OptOptions' 1e-3 eV/Bohr). Same keys as the reference:
     ``positions_angstrom`` / ``positions``, ``energy_hartree``, ``energy_ev``,
     ``heat_of_formation_kcal``, ``converged``, ``iterations`` / ``steps``."""
-    variant = _check_method(method, field)
+    mo = _check_method(method, field)
     z, xyz = _as_arrays(numbers, positions)
     gtol = 1.0e-3 if force_tol is None else float(force_tol) * PM3_A0
-    r = optimize_batch([0, len(z)], z, xyz, options(charge, multiplicity, reference, variant=variant),
+    r = optimize_batch([0, len(z)], z, xyz, options(charge, multiplicity, reference, **mo),
                        max_iter=max_steps, gtol=gtol)
     if r["status"][0] != 0:
         raise ValueError(_lib.default_context().last_error() or f"pm3gpu status {int(r['status'][0])}")
@@ -315,9 +318,9 @@ def numerical_hessian(numbers: Sequence[int], positions, charge: float = 0.0, mu
                       reference: str = "auto", step: float = 1.0e-3, method: str = "pm3") -> np.ndarray:
     """One molecule's gradient-difference Hessian (eV/Bohr^2), positions in Angstrom, ``step`` in
     Bohr (src/hessian.rs:268-319)."""
-    variant = _check_method(method, None)
+    mo = _check_method(method, None)
     z, xyz = _as_arrays(numbers, positions)
-    r = numerical_hessian_batch([0, len(z)], z, xyz, options(charge, multiplicity, reference, variant=variant),
+    r = numerical_hessian_batch([0, len(z)], z, xyz, options(charge, multiplicity, reference, **mo),
                                 step=step)
     if r["status"][0] != 0:
         raise ValueError(_lib.default_context().last_error() or f"pm3gpu status {int(r['status'][0])}")
@@ -396,9 +399,10 @@ def corrections_batch(offsets, z, xyz_bohr, method: str = "pm3-d3h4", want_gradi
     """The post-SCF correction of a method variant alone (pm3gpu_corrections_batch; the
     CorrectionEnergies of src/corrections/mod.rs:193-235) for many molecules: ``d3_ev``, ``h4_ev``,
     ``hh_ev``, ``hx_ev`` and ``total_ev`` per molecule, ``gradient`` (eV/Bohr) of the total."""
-    variant = _check_method(method, None)
-    if variant == 0:
-        raise ValueError("plain PM3 has no correction")
+    mo = _check_method(method, None)
+    variant = mo["variant"]
+    if variant == 0 or mo["mmok"]:
+        raise ValueError("corrections_batch takes 'pm3-d3', 'pm3-d3h4' or 'pm3-d3h4x' (no '+mmok')")
     ctx = context if context is not None else _lib.default_context(device)
     offsets = np.ascontiguousarray(offsets, dtype=np.int32)
     z = np.ascontiguousarray(z, dtype=np.int32)

@@ -53,8 +53,9 @@ def test_supported_elements_and_basis_size():
 
 
 def test_struct_layouts_match_header():
-    assert ctypes.sizeof(_lib.Options) == 8 + 4 + 4 + 8 + 8 + 4 + 4 + 8 + 4 * 4 + 8 + 8 + 8
+    assert ctypes.sizeof(_lib.Options) == 8 + 4 + 4 + 8 + 8 + 4 + 4 + 8 + 4 * 4 + 8 + 8 + 4 + 4 + 4 + 4
     assert _lib.Options.scf_memory_mb.offset == 80 and _lib.Options.variant.offset == 84
+    assert _lib.Options.mmok.offset == 88
     # pm3gpu_result: 4 ints, 4 doubles, 3+1 doubles, 2 doubles, 2 ints, 4 ints, 1 double, 1 double
     assert ctypes.sizeof(_lib.Result) == 16 + 32 + 32 + 16 + 8 + 16 + 16
 

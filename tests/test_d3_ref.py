@@ -72,13 +72,14 @@ def test_pm3_d3_single_point_adds_the_dispersion_energy_and_gradient():
 
 def test_method_strings_parse_like_the_reference():
     """corrections::Variant::parse (src/corrections/mod.rs:180-191, tests/api_surface.rs:224-240)."""
-    assert native._check_method("pm3", None) == 0
-    assert native._check_method("PM3-D3", None) == 1
-    assert native._check_method("pm3_d3", None) == 1
-    assert native._check_method("pm3-d3h4", None) == 2
-    assert native._check_method("PM3 D3H4X", None) == 3
-    assert native._check_method(" ", None) == 0
-    for bad in ("am1", "pm3-d3h4+mmok"):
+    v = lambda m: native._check_method(m, None)["variant"]
+    assert v("pm3") == 0 and v(" ") == 0
+    assert v("PM3-D3") == 1 and v("pm3_d3") == 1
+    assert v("pm3-d3h4") == 2 and v("PM3 D3H4X") == 3
+    assert native._check_method("pm3-d3h4+mmok", None) == {"variant": 2, "mmok": 1}
+    assert native._check_method("pm3+mmok", None) == {"variant": 0, "mmok": 1}
+    assert native._check_method("pm3", None)["mmok"] == 0
+    for bad in ("am1", "pm3-d3+mmok+mmok"):
         with pytest.raises(ValueError):
             native._check_method(bad, None)
     with pytest.raises(ValueError):

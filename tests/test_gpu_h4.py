@@ -86,7 +86,7 @@ def test_corrections_on_a_large_water_box():
                                          (CHLOROMETHANE_WATER, "pm3-d3h4x")])
 def test_d3h4_single_points_and_gradients_match_oracle(geom, method):
     z, xyz = parse(geom)
-    variant = native._check_method(method, None)
+    variant = native._check_method(method, None)["variant"]
     got = native.run(z, xyz * A2B, native.options(variant=variant), want_gradient=True)
     ref = O.single_point(z, xyz * A2B, want_gradient=True, variant=variant)
     assert abs(got["heat_of_formation_kcal"] - ref["heat_of_formation_kcal"]) < HOF_TOL
