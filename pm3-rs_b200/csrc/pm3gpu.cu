@@ -140,7 +140,9 @@ struct pm3gpu_ctx {
   DevBuf gp, gpb, gm, gv, gg;
   DevBuf gqmols, gatom, gao, gcoord, gX, gY, gZ[3], gH[3], gdH, gdZ, gT, gM, gidx, gXb, gTb, gMb, gdY, gpart, gguess, gdens;
   DevBuf gwt, gerr;  // inference: transposed hidden weights (tcgen05 B operands), kernel error flag
-  DevBuf d3buf;      // D3 correction: offsets, sets, coordination numbers, row energies, gradients
+  DevBuf d3buf;      // post-SCF corrections: inputs, coordination numbers, row energies, scratch, gradients
+  void* h_corr = nullptr;  // pinned staging of the corrections' inputs and results
+  size_t h_corr_bytes = 0;
   int* h_gerr = nullptr;  // pinned copy of gerr, read after the stream's next synchronisation
 };
 
@@ -1122,6 +1124,16 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
     c->h2d += 28LL * total_atoms;
   }
   cudaEventRecord(c->ev[1], c->stream);
+  // post-SCF corrections (scf.rs:740-743) depend on the geometry alone: enqueue them ahead of the SCF
+  CorrPlan corr;
+  {
+    bool offs_ok = true;
+    for (int m = 0; m < n_mol; ++m) offs_ok &= h_offs[m + 1] >= h_offs[m];
+    if (offs_ok) {
+      const int rcc = corrections_for_batch(c, n_mol, h_offs, opts, per_mol, dz, dxyz, want.grad && gradients, corr);
+      if (rcc != PM3GPU_OK) return rcc;
+    }
+  }
   std::vector<MolPlan> plans(n_mol);
   std::vector<JobDesc> jobs, rjobs;
   Offsets tot;
@@ -1335,8 +1347,10 @@ int run_batch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const int32_t* h_
     }
   }
   // ---------------------------------------------------------------- post-SCF corrections
-  rc = apply_corrections(c, n_mol, h_offs, h_z, opts, per_mol, dz, dxyz, results, want.grad ? gradients : nullptr);
-  if (rc != PM3GPU_OK) return rc;
+  if (corr.any) {
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));  // long done: enqueued ahead of the SCF
+    apply_corrections(c, n_mol, h_offs, h_z, corr, results, want.grad ? gradients : nullptr);
+  }
   cudaEventRecord(c->ev[3], c->stream);
   cudaEventRecord(c->ev[4], c->stream);
   cudaEventSynchronize(c->ev[4]);
@@ -1461,6 +1475,7 @@ int pm3gpu_context_create(int device, pm3gpu_ctx** out) {
   c->device = device;
   auto bail = [&](cudaError_t e) {
     if (c->h_gerr) cudaFreeHost(c->h_gerr);
+  if (c->h_corr) cudaFreeHost(c->h_corr);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
     (void)e;

@@ -10,6 +10,9 @@
     python pm3-rs_b200/profile_cases.py mlp [--mols 512]
         learned-guess inference on `mols` organics with a random model (pm3gpu_guess_predict):
         three launches of the tcgen05 layer kernel over all atom and pair rows
+    python pm3-rs_b200/profile_cases.py corrections [--mols 4096] [--reps 1]
+        the PM3-D3H4 corrections alone on `mols` organics (pm3gpu_corrections_batch): the D3
+        coordination-number, pair, chain and sum kernels, then the H4 / H-H kernel, per repetition
 
 Each case prints what it ran and exits 0 on success. The profiles/ summaries name the exact command.
 """
@@ -97,9 +100,20 @@ def mlp(mols):
     print(f"mlp: {mols} molecules in {1e3 * (time.perf_counter() - t):.1f} ms (features, three layer launches)")
 
 
+def corrections(mols, reps):
+    offs, z, xyz = workloads.pack(workloads.organic_batch(mols, 5, 60, seed=1234))
+    x = xyz * A2B
+    t = time.perf_counter()
+    for _ in range(reps):
+        r = native.corrections_batch(offs, z, x, "pm3-d3h4")
+    ms = 1e3 * (time.perf_counter() - t) / reps
+    print(f"corrections: {mols} molecules, {len(z)} atoms, PM3-D3H4 in {ms:.2f} ms per call (host copies included); "
+          f"mean D3 {r['d3_ev'].mean():.4f} eV, H4 {r['h4_ev'].mean():.4f} eV")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["split-gemm", "water", "dgemm", "mlp"])
+    ap.add_argument("case", choices=["split-gemm", "water", "dgemm", "mlp", "corrections"])
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--waters", type=int, default=1000)
@@ -112,6 +126,8 @@ def main():
         dgemm(a.n, a.reps)
     elif a.case == "mlp":
         mlp(a.mols)
+    elif a.case == "corrections":
+        corrections(a.mols, a.reps)
     else:
         water(a.waters, a.iters)
 
