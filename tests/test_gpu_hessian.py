@@ -68,3 +68,35 @@ def test_a_failing_molecule_keeps_its_own_status():
     assert np.abs(got["hessians"][0] - got["hessians"][3]).max() < 1.0e-6
     with pytest.raises(ValueError):
         native.numerical_hessian_batch(offs, z, xyz * A2B, step=0.0)
+
+
+def test_open_shell_and_linear_molecules():
+    """A doublet radical (UHF gradients through the batched launch) against the oracle, and a
+    linear molecule, whose rigid subspace has rank five."""
+    z, xyz = parse(GOLDEN["methyl_mopac"][0])
+    got = native.numerical_hessian_batch(np.array([0, len(z)], np.int32), z, xyz * A2B,
+                                         native.options(multiplicity=2))
+    ref = hessian_ref.numerical_hessian(z, xyz * A2B, multiplicity=2)
+    assert got["status"][0] == 0
+    assert np.abs(got["hessians"][0] - ref).max() < HESSIAN_ATOL
+    hcn_z = [1, 6, 7]
+    hcn = [[0.0, 0.0, -1.07], [0.0, 0.0, 0.0], [0.0, 0.0, 1.16]]
+    f = native.frequencies(hcn_z, hcn)
+    assert f["n_rigid"] == 5 and np.count_nonzero(np.array(f["frequencies_cm"]) == 0.0) == 5
+
+
+def test_documented_example_block():
+    """The reference's documented example (tests/test_python_api.py:285-308): PM3-D3H4
+    optimisation, frequencies at the minimum, and a cation's gradient."""
+    numbers = [8, 1, 1]
+    positions = np.array([[0.00, 0.00, 0.00], [0.96, 0.00, 0.00], [-0.24, 0.93, 0.00]])
+    assert np.isfinite(native.single_point(numbers, positions)["heat_of_formation_kcal"])
+    opt = native.optimize(numbers, positions, method="pm3-d3h4")
+    assert opt["converged"]
+    freqs = native.frequencies(numbers, opt["positions_angstrom"], method="pm3-d3h4")
+    assert len(freqs["frequencies_cm"]) == 9
+    assert min(freqs["frequencies_cm"]) >= 0.0  # a minimum: no imaginary mode
+    nh4 = np.array([[0.0, 0.0, 0.0], [0.63, 0.63, 0.63], [-0.63, -0.63, 0.63], [-0.63, 0.63, -0.63],
+                    [0.63, -0.63, -0.63]])
+    g = native.gradient([7, 1, 1, 1, 1], nh4, charge=1, multiplicity=1)
+    assert np.asarray(g["gradient_hartree_per_bohr"]).shape == (5, 3)
