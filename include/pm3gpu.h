@@ -192,8 +192,9 @@ int pm3gpu_single_point(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const do
  * code), so make it before any stream capture begins. A device reset invalidates that address
  * with everything else on the device: create a new context after a reset (creating a context
  * makes the next call look the address up again).
- * The call always runs the one-CTA-per-molecule kernel: a molecule that
- * pm3gpu_set_large_threshold sends to the whole-GPU path returns PM3GPU_RESOURCE_LIMIT here, so
+ * The call always runs the one-CTA-per-molecule kernel: a molecule that pm3gpu_single_point sends
+ * to the whole-GPU path (pm3gpu_set_large_threshold, or 192+ basis functions when no threshold is
+ * set) returns PM3GPU_RESOURCE_LIMIT here, so
  * that the two entry points never run different algorithms on the same input. The caller clears nothing: each call resets
  * the queue counters and flags it needs at zero itself. All contexts of a process on one device
  * share the one array, so calls that overlap in time on that device (two contexts, or two

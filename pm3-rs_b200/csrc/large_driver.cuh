@@ -784,8 +784,14 @@ class LargeSolver {
       coop_g_ = (coop && occ > 0) ? std::min(occ, 2) * c_->sms : 0;
     }
     if ((long long)coop_g_ * large::kTile < n_) return 0;
+    // A small matrix has a few stripes and GEMV tiles (n = 204: 4 and 10), so most blocks of the
+    // full grid only wait at the two grid barriers of each column; 64 blocks (the fewest the kernel
+    // takes: blocks 0-63 each finish one component of W^T v, V^T v) shorten both barriers and the
+    // cross-block sums.
+    if (n_ <= kCoopSmallN) return std::min(coop_g_, 64);
     return coop_g_;
   }
+  static constexpr int kCoopSmallN = 512;  // at most 8 stripes of 64 rows
 
   // Enqueues the blocked reduction of A (no host synchronisation inside).
   int enqueue_tridiag(double* A, int& launches) {

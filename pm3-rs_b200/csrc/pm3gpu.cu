@@ -2318,12 +2318,15 @@ int noalloc_run(pm3gpu_ctx* c, int n_atoms, const int32_t* z, const double* xyz,
     c->err = p.msg;
     return p.status;
   }
-  if (p.large) {  // pm3gpu_single_point would run the whole-GPU algorithm, which needs allocations
-    char msg[200];
+  // pm3gpu_single_point would run the whole-GPU algorithm, which needs allocations: by the context's
+  // threshold, or (none set) by the lone-molecule rule of run_batch
+  const bool lone_whole = !c->large_set && p.nao >= kSingleWholeNao && o->guess != PM3GPU_GUESS_LEARNED;
+  if (p.large || lone_whole) {
+    char msg[220];
     std::snprintf(msg, sizeof msg,
-                  "molecule (nao=%d) is at or above the context's whole-GPU threshold (%d); the allocation-free "
-                  "path runs only the one-CTA-per-molecule kernel",
-                  p.nao, c->large_min);
+                  "molecule (nao=%d) is at or above the whole-GPU threshold (%d) of a single-molecule call; the "
+                  "allocation-free path runs only the one-CTA-per-molecule kernel",
+                  p.nao, p.large ? c->large_min : kSingleWholeNao);
     return fail(c, PM3GPU_RESOURCE_LIMIT, msg);
   }
   // the first pass and the stability rungs run_pm3 would try, in its order (scf.rs:599-715)
