@@ -100,3 +100,17 @@ def test_documented_example_block():
                     [0.63, -0.63, -0.63]])
     g = native.gradient([7, 1, 1, 1, 1], nh4, charge=1, multiplicity=1)
     assert np.asarray(g["gradient_hartree_per_bohr"]).shape == (5, 3)
+
+
+def test_hessian_with_corrections_matches_the_restated_reference():
+    """PM3-D3H4X on a hydrogen-bonded and a halogen-bonded pair: the corrections' gradients enter
+    every displaced evaluation on both sides."""
+    mols = [parse("O 0.0 0.0 0.0; H 0.96 0.0 0.0; H -0.24 0.93 0.0; O 2.9 0.0 0.0; H 3.2 0.9 0.0; H 3.2 -0.5 0.8"),
+            parse("C 0 0 0; Cl 1.78 0 0; H -0.36 1.03 0; H -0.36 -0.51 0.89; H -0.36 -0.51 -0.89; N 4.80 0 0;"
+                  " H 5.18 0.94 0; H 5.18 -0.47 0.81; H 5.18 -0.47 -0.81")]
+    offs, z, xyz = workloads.pack(mols)
+    got = native.numerical_hessian_batch(offs, z, xyz * A2B, native.options(variant=3))
+    for m, (zm, xm) in enumerate(mols):
+        ref = hessian_ref.numerical_hessian(zm, xm * A2B, variant=3)
+        assert got["status"][m] == 0
+        assert np.abs(got["hessians"][m] - ref).max() < HESSIAN_ATOL
