@@ -164,6 +164,9 @@ int pm3gpu_set_stream(pm3gpu_ctx* ctx, void* stream);
 
 /* One molecule: run_pm3. charges[n_atoms] required; density[nao*nao] (total density) and
  * mo_energies[nao] (alpha MO energies of the last iteration) may be NULL.
+ * Not exported from Pm3Result (src/scf.rs:353-396): mo_coeff and the beta set (mo_coeff_beta,
+ * mo_energies_beta, spin_density). The eigensolvers form only the occupied eigenvectors the density
+ * needs, so the virtual coefficients of the last iteration do not exist on the device.
  * Returns the molecule's status (also in result->status). */
 int pm3gpu_single_point(pm3gpu_ctx* ctx, int n_atoms, const int32_t* z, const double* xyz_bohr,
                         const pm3gpu_options* opts, pm3gpu_result* result, double* charges,
