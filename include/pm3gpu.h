@@ -266,14 +266,15 @@ int pm3gpu_numerical_hessian_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* at
 
 /* The D3 dispersion correction alone for many molecules (src/corrections/d3.rs:360-458): d3_set 1 =
  * D3Params::pm3_d3, 2 = D3Params::pm3_d3h4. energies[n_mol] in eV; gradients[3 * total atoms]
- * (optional) in eV/Bohr. Elements outside the D3 table contribute nothing, as in the reference. */
+ * (optional) in eV/Bohr. */
 int pm3gpu_d3_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
                     const double* xyz_bohr, int d3_set, double* energies, double* gradients);
 
 /* The whole correction of a variant (PM3GPU_VARIANT_D3 / _D3H4 / _D3H4X) alone for many molecules:
  * the CorrectionEnergies of src/corrections/mod.rs:193-235. parts[4 * n_mol] receives per molecule
  * (D3, H4, H-H repulsion, X) in eV; gradients[3 * total atoms] (optional) the gradient of their sum
- * in eV/Bohr. */
+ * in eV/Bohr. Both correction-only entries take the s/p elements (pm3gpu_supported_element) and
+ * return PM3GPU_UNSUPPORTED for any other. */
 int pm3gpu_corrections_batch(pm3gpu_ctx* ctx, int n_mol, const int32_t* atom_offsets, const int32_t* z,
                              const double* xyz_bohr, int variant, double* parts, double* gradients);
 

@@ -85,8 +85,8 @@ int corrections_launch(pm3gpu_ctx* c, int n_mol, const int32_t* h_offs, const in
   std::memcpy(hb + h_offs_at, h_offs, 4 * (M + 1));
   std::memcpy(hb + h_set_at, P.set.data(), 4 * M);
   std::memcpy(hb + h_var_at, h_var, 4 * M);
-  std::memcpy(hb + h_hm_at, hmols.data(), 4 * (size_t)nh);
-  std::memcpy(hb + h_mm_at, mmols.data(), 4 * (size_t)nm);
+  if (nh) std::memcpy(hb + h_hm_at, hmols.data(), 4 * (size_t)nh);
+  if (nm) std::memcpy(hb + h_mm_at, mmols.data(), 4 * (size_t)nm);
   // device buffers
   size_t o = 0;
   auto take = [&](size_t b) {

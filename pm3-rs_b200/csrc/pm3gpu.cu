@@ -1654,6 +1654,8 @@ int pm3gpu_d3_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, const int32_t
   const int total = offs[n_mol];
   for (long long k = 0; k < 3LL * total; ++k)
     if (!std::isfinite(xyz[k])) return fail(c, PM3GPU_INVALID_INPUT, "non-finite coordinate");
+  for (int a = 0; a < total; ++a)  // the device tables hold the s/p elements only
+    if (!supported(z[a])) return fail(c, PM3GPU_UNSUPPORTED, "unsupported element Z=" + std::to_string(z[a]));
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   c->err.clear();
@@ -1684,6 +1686,8 @@ int pm3gpu_corrections_batch(pm3gpu_ctx* c, int n_mol, const int32_t* offs, cons
   const int total = offs[n_mol];
   for (long long k = 0; k < 3LL * total; ++k)
     if (!std::isfinite(xyz[k])) return fail(c, PM3GPU_INVALID_INPUT, "non-finite coordinate");
+  for (int a = 0; a < total; ++a)  // the device tables (D3, covalent radii, X pairs) hold the s/p elements only
+    if (!supported(z[a])) return fail(c, PM3GPU_UNSUPPORTED, "unsupported element Z=" + std::to_string(z[a]));
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   c->err.clear();

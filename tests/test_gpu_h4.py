@@ -106,3 +106,15 @@ def test_method_strings_through_the_python_api():
     g4 = native.gradient(zc, xc, method="pm3-d3h4")
     assert gx["energy_ev"] > g4["energy_ev"]  # the halogen-bond term is repulsive here
     assert np.abs(np.asarray(gx["gradient_hartree_per_bohr"]) - np.asarray(g4["gradient_hartree_per_bohr"])).max() > 0
+
+
+def test_correction_entries_refuse_elements_outside_the_tables():
+    """The device tables hold the s/p elements; a bromine is refused rather than given numbers that
+    would differ from the reference's."""
+    offs = np.array([0, 2], np.int32)
+    z = np.array([35, 1], np.int32)
+    x = np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 2.7]])
+    with pytest.raises(ValueError, match="unsupported element"):
+        native.corrections_batch(offs, z, x, "pm3-d3h4x")
+    with pytest.raises(ValueError, match="unsupported element"):
+        native.d3_batch(offs, z, x, 1)
