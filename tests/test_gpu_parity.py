@@ -107,6 +107,11 @@ def test_single_point_matches_oracle(name):
     assert got["unrestricted"] == ref["unrestricted"]
     assert got["scf_paths_tried"] == ref["scf_paths_tried"]
     assert abs(got["homo_ev"] - ref["homo_ev"]) < 1e-6 and abs(got["lumo_ev"] - ref["lumo_ev"]) < 1e-6
+    # the Pm3Result arrays: every alpha MO energy of the last iteration (virtuals included, from the
+    # saved tridiagonal) and the total density
+    refd = O.single_point(z, xyz * A2B, want_density=True, charge=charge, multiplicity=mult)
+    assert np.abs(got["mo_energies"] - ref["mo_energies"]).max() < 1e-6
+    assert np.abs(got["density"] - refd["density"]).max() < 1e-6
 
 
 def test_python_drop_in_keys_and_units():
