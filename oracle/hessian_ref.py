@@ -41,3 +41,34 @@ def numerical_hessian(z, xyz_bohr, step=1.0e-3, **scf_opts):
             h[i, j] = v
             h[j, i] = v
     return h
+
+
+AU_DIPOLE_TO_DEBYE = 2.541746473  # constants.rs:64
+
+
+def fixed_origin_dipole(z, x, charge, res):
+    """The dipole about the coordinate origin (e Bohr) from a result's centre-of-mass dipole:
+    mu_0 = mu_COM + Q R_COM."""
+    m = np.array([O.element(int(v))["mass"] for v in z])
+    com = (m[:, None] * np.asarray(x).reshape(-1, 3)).sum(axis=0) / m.sum()
+    return np.asarray(res["dipole_debye"]) / AU_DIPOLE_TO_DEBYE + charge * com
+
+
+def dipole_derivatives(z, xyz_bohr, step=1.0e-3, charge=0.0, **scf_opts):
+    """d mu / d R (elementary charges, 3 x 3N) by central differences of the fixed-origin dipole
+    under the tightened SCF: the quantity the reference's analytic dipole_derivatives
+    (src/ir.rs:103-190) is checked against in its own tests (src/ir.rs:393-436)."""
+    x0 = np.asarray(xyz_bohr, dtype=np.float64).reshape(-1, 3)
+    nd = 3 * len(x0)
+    opts = tightened(**scf_opts)
+    out = np.zeros((3, nd))
+    for j in range(nd):
+        a, k = divmod(j, 3)
+        mus = []
+        for sign in (1.0, -1.0):
+            x = x0.copy()
+            x[a, k] += sign * step
+            r = O.single_point(z, x, charge=charge, **opts)
+            mus.append(fixed_origin_dipole(z, x, charge, r))
+        out[:, j] = (mus[0] - mus[1]) / (2.0 * step)
+    return out

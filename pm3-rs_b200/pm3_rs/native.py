@@ -420,3 +420,136 @@ def corrections_batch(offsets, z, xyz_bohr, method: str = "pm3-d3h4", want_gradi
     if g is not None:
         out["gradient"] = g
     return out
+
+
+AU_DIPOLE_TO_DEBYE = 2.541746473  # constants.rs:64
+DEBYE_TO_E_ANGSTROM = 0.2081943  # src/python.rs:2049
+# N_A |dmu/dQ|^2 / (12 eps0 c^2) with dmu/dQ in e / sqrt(amu), in km/mol (src/ir.rs:60-80)
+KM_PER_MOL_PER_E2_PER_AMU = (6.02214076e23 * (1.602176634e-19 ** 2 / 1.66053906660e-27)
+                             / (12.0 * 8.8541878128e-12 * 2.99792458e8 ** 2) / 1000.0)
+
+
+def _tightened(o: _lib.Options) -> _lib.Options:
+    """tighten_scf_for_hessian (src/hessian.rs:169-175) on a copy."""
+    t = _lib.Options.from_buffer_copy(o)
+    t.e_tol = min(t.e_tol, 1.0e-12)
+    t.p_tol = min(t.p_tol, 1.0e-11)
+    t.max_scf = max(t.max_scf, 500)
+    return t
+
+
+def dipole_derivatives_batch(offsets, z, xyz_bohr, opts=None, step: float = 1.0e-3, device: int = 0,
+                             context: _lib.Context | None = None) -> dict:
+    """d mu / d R (elementary charges, one 3 x 3N array per molecule) by central differences of the
+    dipole about a fixed origin, every displaced geometry of every molecule in one batched SCF
+    launch under the tightened SCF. The reference's dipole_derivatives (src/ir.rs:103-190) solves
+    three coupled-perturbed equations instead; its own tests hold that tensor to exactly this
+    difference (src/ir.rs:393-436). ``opts``: one Options or a list, one per molecule. The GPU
+    reports the dipole about the centre of mass; mu_0 = mu_COM + Q R_COM restores the fixed origin.
+    Returns ``derivatives`` and ``status`` (the first failing displacement's)."""
+    offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+    z = np.ascontiguousarray(z, dtype=np.int32)
+    x = np.ascontiguousarray(np.asarray(xyz_bohr, dtype=np.float64).reshape(-1, 3))
+    n_mol = len(offsets) - 1
+    base = opts if opts is not None else options()
+    per = list(base) if isinstance(base, (list, tuple)) else [base] * n_mol
+    masses = np.asarray(atomic_masses(z)) if len(z) else np.zeros(0)
+    geo_z, geo_x, geo_o, geo_off = [], [], [], [0]
+    for m in range(n_mol):
+        a0, a1 = int(offsets[m]), int(offsets[m + 1])
+        t = _tightened(per[m])
+        for j in range(3 * (a1 - a0)):
+            for sign in (1.0, -1.0):
+                xd = x[a0:a1].copy()
+                xd[j // 3, j % 3] += sign * step
+                geo_z.append(z[a0:a1])
+                geo_x.append(xd)
+                geo_o.append(t)
+                geo_off.append(geo_off[-1] + (a1 - a0))
+    out = [np.zeros((3, 3 * int(offsets[m + 1] - offsets[m]))) for m in range(n_mol)]
+    status = np.zeros(n_mol, dtype=np.int32)
+    if geo_o:
+        r = batch(np.array(geo_off, np.int32), np.concatenate(geo_z), np.concatenate(geo_x), geo_o,
+                  device=device, context=context)
+        g = 0
+        for m in range(n_mol):
+            a0, a1 = int(offsets[m]), int(offsets[m + 1])
+            mm = masses[a0:a1]
+            q = float(per[m].charge)
+            for j in range(3 * (a1 - a0)):
+                mu = []
+                for _ in range(2):
+                    if status[m] == 0 and r.status[g] != 0:
+                        status[m] = r.status[g]
+                    xd = geo_x[g]
+                    com = (mm[:, None] * xd).sum(axis=0) / mm.sum()
+                    mu.append(r.dipole_debye[g] / AU_DIPOLE_TO_DEBYE + q * com)
+                    g += 1
+                out[m][:, j] = (mu[0] - mu[1]) / (2.0 * step)
+    for m in range(n_mol):
+        if status[m] != 0:
+            out[m][:] = 0.0
+    return {"derivatives": out, "status": status}
+
+
+def dipole(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1, reference: str = "auto",
+           method: str = "pm3", field=None, operator: bool = False) -> dict:
+    """The dipole and its nuclear derivatives (src/python.rs:2016-2083): ``dipole_debye``,
+    ``dipole_e_angstrom``, ``centre_of_mass_angstrom`` (the origin of both) and ``derivatives_e``
+    (3 x 3N, fixed origin, elementary charges; from ``dipole_derivatives_batch``). The AO moment
+    matrices (``operator=True``) are not available here."""
+    if operator:
+        raise ValueError("the dipole operator matrices (operator=True) are not available on pm3gpu")
+    mo = _check_method(method, field)
+    z, xyz = _as_arrays(numbers, positions)
+    o = options(charge, multiplicity, reference, **mo)
+    r = run(z, xyz, o)
+    d = dipole_derivatives_batch([0, len(z)], z, xyz, o)
+    if d["status"][0] != 0:
+        raise ValueError(_lib.default_context().last_error() or f"pm3gpu status {int(d['status'][0])}")
+    m = np.asarray(atomic_masses(z))
+    com = (m[:, None] * xyz).sum(axis=0) / m.sum()
+    mu = [float(v) for v in r["dipole_debye"]]
+    return {
+        "dipole_debye": mu,
+        "dipole_e_angstrom": [v * DEBYE_TO_E_ANGSTROM for v in mu],
+        "centre_of_mass_angstrom": (com * PM3_A0).tolist(),
+        "derivatives_e": d["derivatives"][0].tolist(),
+    }
+
+
+def ir_spectrum(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+                reference: str = "auto", method: str = "pm3", field=None, cphf_max_iter=None) -> dict:
+    """Infrared spectrum (src/ir.rs:284-345, src/python.rs:1952-2003): ``frequencies_cm``,
+    ``intensities_km_per_mol`` (N_A |d mu / d Q|^2 / (12 eps0 c^2), the modes projected onto the
+    internal subspace first), ``dipole_derivatives_e`` (3 x 3N) and ``ndof``. Frequencies from the
+    gradient-difference Hessian (see ``hessian``), derivatives from ``dipole_derivatives_batch``;
+    ``cphf_max_iter`` caps CPHF iterations, which this path does not run."""
+    from . import vibrations
+
+    mo = _check_method(method, field)
+    z, xyz = _as_arrays(numbers, positions)
+    o = options(charge, multiplicity, reference, **mo)
+    r = numerical_hessian_batch([0, len(z)], z, xyz, o, step=1.0e-3)
+    if r["status"][0] != 0:
+        raise ValueError(_lib.default_context().last_error() or f"pm3gpu status {int(r['status'][0])}")
+    d = dipole_derivatives_batch([0, len(z)], z, xyz, o)
+    if d["status"][0] != 0:
+        raise ValueError(_lib.default_context().last_error() or f"pm3gpu status {int(d['status'][0])}")
+    masses = np.asarray(atomic_masses(z))
+    pos = np.asarray(positions, dtype=np.float64).reshape(-1, 3)
+    vib = vibrations.vibrational_analysis(r["hessians"][0], pos, masses)
+    basis = vibrations.rigid_body_basis(pos, masses)
+    modes = vib["modes"]
+    proj = modes - (np.stack(basis, axis=1) @ (np.stack(basis, axis=1).T @ modes) if basis else 0.0)
+    root = np.sqrt(np.repeat(masses, 3))
+    inv = np.where(root > 0.0, 1.0 / np.where(root > 0.0, root, 1.0), 0.0)
+    dmu = d["derivatives"][0]
+    dq = dmu @ (proj * inv[:, None])  # 3 x modes
+    inten = KM_PER_MOL_PER_E2_PER_AMU * (dq ** 2).sum(axis=0)
+    return {
+        "frequencies_cm": vib["frequencies_cm"],
+        "intensities_km_per_mol": inten.tolist(),
+        "dipole_derivatives_e": dmu.tolist(),
+        "ndof": len(vib["frequencies_cm"]),
+    }
