@@ -553,3 +553,20 @@ def ir_spectrum(numbers: Sequence[int], positions, charge: float = 0.0, multipli
         "dipole_derivatives_e": dmu.tolist(),
         "ndof": len(vib["frequencies_cm"]),
     }
+
+
+def orbitals(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+             reference: str = "auto", method: str = "pm3", field=None) -> dict:
+    """The reference's orbitals (src/python.rs:559-688) returns every MO coefficient of the last
+    iteration. The device eigensolvers form only the occupied eigenvectors the density needs, so
+    the coefficients do not exist here: this raises, naming what is available instead (all MO
+    energies through ``run(..., want_mo_energies=True)``, the density through ``want_density``)."""
+    raise ValueError("orbitals: MO coefficients are not exported by pm3gpu (the eigensolvers form only the "
+                     "occupied vectors); MO energies and the density come from run(..., want_mo_energies=True, "
+                     "want_density=True)")
+
+
+def molden(*args, **kwargs):
+    """The reference's Molden writer (src/python.rs:1021-1066) needs the MO coefficients; see
+    ``orbitals``."""
+    raise ValueError("molden: MO coefficients are not exported by pm3gpu; see orbitals()")

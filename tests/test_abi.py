@@ -87,3 +87,11 @@ def test_tuning_file_is_checked_without_a_device(tmp_path):
     assert lib.pm3gpu_load_tuning(None, str(empty).encode()) == _lib.INVALID_INPUT
     assert lib.pm3gpu_load_tuning(None, str(tmp_path / "missing.json").encode()) == _lib.INVALID_INPUT
     assert lib.pm3gpu_tuning_choice(None, 0, 100) == -1
+
+
+def test_entry_points_without_coefficients_raise_loudly():
+    """orbitals / molden need MO coefficients, which the library does not export: a ValueError
+    that says so, before any GPU work."""
+    for fn in (native.orbitals, native.molden):
+        with pytest.raises(ValueError, match="MO coefficients"):
+            fn([8, 1, 1], np.zeros((3, 3)))
