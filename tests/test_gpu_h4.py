@@ -118,3 +118,50 @@ def test_correction_entries_refuse_elements_outside_the_tables():
         native.corrections_batch(offs, z, x, "pm3-d3h4x")
     with pytest.raises(ValueError, match="unsupported element"):
         native.d3_batch(offs, z, x, 1)
+
+
+def test_d3h4_on_the_whole_gpu_path_and_from_device_inputs():
+    """The corrections join the whole-GPU path's results (threshold 1), and the batch entry whose
+    coordinates are already on the device (the corrections read the caller's arrays there)."""
+    import ctypes
+
+    import torch
+
+    from pm3_rs import _lib
+
+    z, xyz = workloads.water_cluster(12)
+    ctx = _lib.Context()
+    try:
+        assert ctx.lib.pm3gpu_set_large_threshold(ctx.ptr, 1) == 0
+        got = native.run(z, xyz * A2B, native.options(p_tol=1e-8, variant=2), want_gradient=True, context=ctx)
+    finally:
+        ctx.close()
+    ref = O.single_point(z, xyz * A2B, want_gradient=True, p_tol=1e-8, variant=2)
+    assert abs(got["heat_of_formation_kcal"] - ref["heat_of_formation_kcal"]) < HOF_TOL
+    assert np.abs(got["gradient"] - ref["gradient"]).max() < 10 * GRAD_TOL
+
+    mols = [parse(DIMER_API), parse(ACETIC_WATER), parse(CHLOROMETHANE_AMMONIA)]
+    offs, zz, xx = workloads.pack(mols)
+    host = native.batch(offs, zz, xx * A2B, native.options(variant=3), want_gradient=True)
+    dz = torch.tensor(np.asarray(zz, np.int32), device="cuda")
+    dx = torch.tensor(np.ascontiguousarray(xx * A2B), dtype=torch.float64, device="cuda")
+    doffs = torch.tensor(np.asarray(offs, np.int32), device="cuda")
+    ho = np.ascontiguousarray(offs, np.int32)
+    hz = np.ascontiguousarray(zz, np.int32)
+    res = (_lib.Result * len(mols))()
+    q = np.zeros(len(zz))
+    g = np.zeros((len(zz), 3))
+    c = _lib.default_context()
+    torch.cuda.synchronize()
+    I32, D = ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)
+    o = native.options(variant=3)
+    rc = c.lib.pm3gpu_batch_device_inputs(c.ptr, len(mols), ctypes.c_void_p(doffs.data_ptr()),
+                                          ctypes.c_void_p(dz.data_ptr()), ctypes.c_void_p(dx.data_ptr()),
+                                          ho.ctypes.data_as(I32), hz.ctypes.data_as(I32), ctypes.byref(o), res,
+                                          q.ctypes.data_as(D), g.ctypes.data_as(D))
+    assert rc == 0, c.last_error()
+    for m in range(len(mols)):
+        assert res[m].status == 0
+        assert abs(res[m].heat_of_formation_kcal - host.heat_of_formation_kcal[m]) < 1e-9
+    # the SCF and gradient kernels sum some atom terms with atomics: the two runs agree to rounding
+    assert np.abs(g - host.gradients).max() < 1e-8
